@@ -1,0 +1,1208 @@
+// Device code of the bounce loop: Owen-scrambled Sobol, ordered BVH traversal
+// (closest and any hit), hit-record reconstruction, the Disney BSDF, lights,
+// transparent shadows, the homogeneous medium and the per-path integrator.
+//
+// Built with -fmad=false and IEEE div/sqrt: every decision (hit/miss, leaf
+// order, lobe choice, RR gate) uses the same float operations, in the same
+// order, as 3d-ray's C# (paths in comments are relative to src/RayTracer/).
+// Transcendentals (cos, sin, pow, exp, log) are CUDA's own; they differ from
+// glibc by a few ulps, so paths agree bit-for-bit only up to the first
+// transcendental-dependent direction.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "scene_types.h"
+
+namespace rt {
+
+// ---------------------------------------------------------------------------
+// Owen-scrambled Sobol (Core/Sampling/OwenSobol.cs:48-210)
+// ---------------------------------------------------------------------------
+__constant__ uint32_t c_dim1_dirs[32] = {
+    0x80000000u, 0xc0000000u, 0xa0000000u, 0xf0000000u, 0x88000000u, 0xcc000000u, 0xaa000000u, 0xff000000u,
+    0x80800000u, 0xc0c00000u, 0xa0a00000u, 0xf0f00000u, 0x88880000u, 0xcccc0000u, 0xaaaa0000u, 0xffff0000u,
+    0x80008000u, 0xc000c000u, 0xa000a000u, 0xf000f000u, 0x88008800u, 0xcc00cc00u, 0xaa00aa00u, 0xff00ff00u,
+    0x80808080u, 0xc0c0c0c0u, 0xa0a0a0a0u, 0xf0f0f0f0u, 0x88888888u, 0xccccccccu, 0xaaaaaaaau, 0xffffffffu,
+};
+
+RT_D uint32_t hash_u32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+RT_D uint32_t lk_permute(uint32_t v, uint32_t seed) {
+    v += seed;
+    v ^= v * 0x6c50b47cu;
+    v ^= v * 0xb82f1e52u;
+    v ^= v * 0xc7afe638u;
+    v ^= v * 0x8d22f6e6u;
+    return v;
+}
+RT_D uint32_t owen_scramble(uint32_t v, uint32_t seed) { return __brev(lk_permute(__brev(v), seed)); }
+
+RT_D float sobol_sample(uint32_t index, uint32_t dim, uint32_t pixel_seed) {
+    uint32_t v;
+    if (dim == 0u) {
+        v = __brev(index);
+    } else if (dim == 1u) {
+        v = 0u;
+        uint32_t i = index;
+#pragma unroll 1
+        for (int k = 0; i != 0u; k++, i >>= 1)
+            if (i & 1u) v ^= c_dim1_dirs[k];
+    } else {
+        uint32_t shuffle = hash_u32(dim * 0x68bc21ebu + 0xc7afe638u);
+        v = __brev(owen_scramble(index, shuffle));
+    }
+    uint32_t scramble = hash_u32(pixel_seed ^ hash_u32(dim * 0xa511e9b3u + 0x736f6c34u));
+    v = owen_scramble(v, scramble);
+    return (float)(v >> 8) * (1.0f / 16777216.0f);
+}
+
+// The per-path dimension counter of Core/Sampling/Sampler.cs:75-118.
+struct Sampler {
+    uint32_t seed, index, dim;
+    RT_D float next() { return sobol_sample(index, dim++, seed); }
+};
+
+RT_D V3 random_unit_vector(Sampler& s) {   // Core/MathUtils.cs:104-112
+    float u = s.next();
+    float v = s.next();
+    float z = 1.0f - 2.0f * u;
+    float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    float phi = 2.0f * kPi * v;
+    float sn, cs;
+    sincosf(phi, &sn, &cs);
+    return v3(r * cs, r * sn, z);
+}
+
+// ---------------------------------------------------------------------------
+// Traversal
+// ---------------------------------------------------------------------------
+enum : int { HIT_NONE = 0, HIT_TRI = 1, HIT_QUAD = 2, HIT_SPHERE = 3 };
+
+struct Hit {
+    float t, u, v;
+    int kind;
+    int slot;   // stored triangle index, or entity id for quads and spheres
+};
+
+// Work counters of the counting build (algorithmic bytes of the roofline).
+struct Counters {
+    uint32_t nodes, tris, others, closest_rays, shadow_rays;
+};
+
+RT_D V3 ld3(const float4& f) { return v3(f.x, f.y, f.z); }
+
+RT_D bool box_hit(float4 lo, float4 hi, V3 o, V3 inv, float tmin, float tmax) {   // Core/AABB.cs:28-52
+    float t0x = (lo.x - o.x) * inv.x, t0y = (lo.y - o.y) * inv.y, t0z = (lo.z - o.z) * inv.z;
+    float t1x = (hi.x - o.x) * inv.x, t1y = (hi.y - o.y) * inv.y, t1z = (hi.z - o.z) * inv.z;
+    float te = fmaxf(tmin, fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))));
+    float tx = fminf(tmax, fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z))));
+    return tx >= te;
+}
+
+// Geometry/Triangle.cs:49-89 (Moller-Trumbore, |a| < 1e-7 reject, inclusive t range)
+RT_D bool tri_test(const float4* tris, int i, V3 o, V3 d, float tmin, float tmax, float& t, float& u, float& v) {
+    float4 a0 = __ldg(tris + 3 * i), a1 = __ldg(tris + 3 * i + 1), a2 = __ldg(tris + 3 * i + 2);
+    V3 v0 = ld3(a0), e1 = ld3(a1), e2 = ld3(a2);
+    V3 h = cross(d, e2);
+    float a = dot(e1, h);
+    if (fabsf(a) < 1e-7f) return false;
+    float f = 1.0f / a;
+    V3 s = o - v0;
+    u = f * dot(s, h);
+    if (u < 0.0f || u > 1.0f) return false;
+    V3 q = cross(s, e1);
+    v = f * dot(d, q);
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = f * dot(e2, q);
+    if (t < tmin || t > tmax) return false;
+    return true;
+}
+
+// Geometry/Quad.cs:42-86; front_only for the back-face-culled light proxy
+// (Geometry/BackFaceCulledHittable.cs).
+RT_D bool quad_test(const QuadData& q, V3 o, V3 d, float tmin, float tmax, bool front_only, float& t, float& a,
+                    float& b) {
+    float denom = dot(q.normal, d);
+    if (fabsf(denom) < 1e-8f) return false;
+    t = (q.d - dot(q.normal, o)) / denom;
+    if (t < tmin || t > tmax) return false;
+    V3 ip = o + t * d;
+    V3 ph = ip - q.q;
+    a = dot(q.w, cross(ph, q.v));
+    b = dot(q.w, cross(q.u, ph));
+    if (a < 0.0f || a > 1.0f || b < 0.0f || b > 1.0f) return false;
+    if (front_only && !(dot(d, q.normal) < 0.0f)) return false;
+    return true;
+}
+
+// Geometry/Sphere.cs:20-42
+RT_D bool sphere_test(const SphereData& s, V3 o, V3 d, float tmin, float tmax, float& t) {
+    V3 oc = o - s.c;
+    float a = length_sq(d);
+    float hb = dot(oc, d);
+    float c = length_sq(oc) - s.r * s.r;
+    float disc = hb * hb - a * c;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(disc);
+    float root = (-hb - sq) / a;
+    if (root < tmin || root > tmax) {
+        root = (-hb + sq) / a;
+        if (root < tmin || root > tmax) return false;
+    }
+    t = root;
+    return true;
+}
+
+// Tests one quad/sphere entity. Returns true on an accepted hit.
+RT_D bool entity_test(const SceneView& s, int e, V3 o, V3 d, float tmin, float tmax, Hit& h) {
+    Entity en = s.entities[e];
+    float t, a = 0.0f, b = 0.0f;
+    if (en.kind == ENT_QUAD) {
+        if (!quad_test(s.quads[en.index], o, d, tmin, tmax, (en.flags & ENT_BACKFACE_CULLED) != 0, t, a, b))
+            return false;
+        h = Hit{t, a, b, HIT_QUAD, e};
+        return true;
+    }
+    if (!sphere_test(s.spheres[en.index], o, d, tmin, tmax, t)) return false;
+    h = Hit{t, 0.0f, 0.0f, HIT_SPHERE, e};
+    return true;
+}
+
+// Ordered depth-first traversal reproducing HittableList -> BvhNode -> Mesh ->
+// BvhNode -> Triangle (Geometry/HittableList.cs:19-37, Acceleration/BvhNode.cs:157-206):
+// near child first by sign(dir[axis]), fat leaves scanned in order, a later
+// primitive at an equal t wins, the far child is tested against the closest t
+// found in the near subtree. ANY = true stops at the first accepted hit
+// (opaque shadow rays). Stack entries: node index (>= 0) or ~entity.
+// Returns false on stack overflow (err set).
+// root >= 0 restricts the walk to one mesh BVH (a light's own geometry).
+template <bool ANY, int STACK>
+__device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
+                                         Counters* cnt, int* err, int root = -1) {
+    V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
+    int stack[STACK];
+    int sp = 0;
+    float closest = tmax;
+    best.kind = HIT_NONE;
+    if (root >= 0) {
+        stack[sp++] = root;
+    } else if (s.top_root >= 0) {
+        stack[sp++] = s.top_root;
+    } else {
+        for (int i = s.num_top_items - 1; i >= 0; --i) stack[sp++] = ~s.top_items[i];
+    }
+    while (sp > 0) {
+        int e = stack[--sp];
+        int node;
+        if (e < 0) {
+            int ent = ~e;
+            Entity en = s.entities[ent];
+            if (en.kind != ENT_MESH) {
+                if (cnt) cnt->others++;
+                Hit h;
+                if (entity_test(s, ent, o, d, tmin, closest, h)) {
+                    best = h;
+                    closest = h.t;
+                    if (ANY) return true;
+                }
+                continue;
+            }
+            node = en.index;
+        } else {
+            node = e;
+        }
+        for (;;) {
+            const float4* np = reinterpret_cast<const float4*>(s.nodes + node);
+            float4 lo = __ldg(np), hi = __ldg(np + 1);
+            int a = __float_as_int(lo.w), b = __float_as_int(hi.w);
+            if (cnt) cnt->nodes++;
+            if (a >= 0) {
+                if (!box_hit(lo, hi, o, inv, tmin, closest)) break;
+                int right = b & 0x3FFFFFFF;
+                int axis = (int)((unsigned)b >> 30);
+                float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
+                int near_c = da >= 0.0f ? a : right;
+                int far_c = da >= 0.0f ? right : a;
+                if (sp >= STACK) {
+                    *err = RT_ERR_STACK;
+                    return false;
+                }
+                stack[sp++] = far_c;
+                node = near_c;
+                continue;
+            }
+            int kind = b >> 16;
+            int count = b & 0xFFFF;
+            int first = ~a;
+            if (kind != LEAF_LIST && !box_hit(lo, hi, o, inv, tmin, closest)) break;
+            if (kind == LEAF_ENTS) {
+                if (sp + count > STACK) {
+                    *err = RT_ERR_STACK;
+                    return false;
+                }
+                for (int i = count - 1; i >= 0; --i) stack[sp++] = ~s.top_items[first + i];
+                break;
+            }
+            for (int i = 0; i < count; i++) {
+                float t, u, v;
+                if (cnt) cnt->tris++;
+                if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, v)) {
+                    best = Hit{t, u, v, HIT_TRI, first + i};
+                    closest = t;
+                    if (ANY) return true;
+                }
+            }
+            break;
+        }
+    }
+    return true;
+}
+
+// Surface record of an accepted hit (Core/HitRecord.cs fields on the path).
+struct Surface {
+    V3 p, n, tangent, bitangent;
+    float t;
+    int front;
+    int material;
+    int entity;
+    int prim;
+};
+
+RT_D Surface make_surface(const SceneView& s, const Hit& h, V3 o, V3 d) {
+    Surface r;
+    r.t = h.t;
+    r.p = o + h.t * d;   // Ray.At
+    if (h.kind == HIT_TRI) {
+        const float4* tp = s.tris + 3 * h.slot;
+        float4 a0 = __ldg(tp), a1 = __ldg(tp + 1), a2 = __ldg(tp + 2);
+        V3 e1 = ld3(a1), e2 = ld3(a2);
+        V3 n = v3(a0.w, a1.w, a2.w);
+        r.front = dot(d, n) < 0.0f;   // HitRecord.SetFaceNormal
+        r.n = r.front ? n : -n;
+        r.tangent = length_sq(e1) > 0.0f ? normalize(e1) : v3(1.0f, 0.0f, 0.0f);
+        r.bitangent = length_sq(e2) > 0.0f ? normalize(e2) : v3(0.0f, 0.0f, 1.0f);
+        r.entity = s.tri_entity[h.slot];
+        r.prim = s.tri_local[h.slot];
+    } else if (h.kind == HIT_QUAD) {
+        Entity en = s.entities[h.slot];
+        const QuadData& q = s.quads[en.index];
+        r.front = dot(d, q.normal) < 0.0f;
+        r.n = r.front ? q.normal : -q.normal;
+        r.tangent = q.tangent;
+        r.bitangent = q.bitangent;
+        r.entity = h.slot;
+        r.prim = 0;
+    } else {
+        Entity en = s.entities[h.slot];
+        const SphereData& sp = s.spheres[en.index];
+        V3 outward = (r.p - sp.c) / sp.r;
+        r.front = dot(d, outward) < 0.0f;
+        r.n = r.front ? outward : -outward;
+        V3 td = cross(v3(0.0f, 1.0f, 0.0f), outward);
+        if (length_sq(td) < 1e-4f) td = v3(1.0f, 0.0f, 0.0f);
+        r.tangent = normalize(td);
+        r.bitangent = normalize(cross(outward, r.tangent));
+        r.entity = h.slot;
+        r.prim = 0;
+    }
+    r.material = s.entities[r.entity].material;
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Kulla-Conty LUT lookups (Materials/EnergyCompensationLut.cs:140-175)
+// ---------------------------------------------------------------------------
+RT_D float lut_e(const float* e, float mu, float alpha) {
+    mu = clampf(mu, 0.0f, 1.0f);
+    alpha = clampf(alpha, 0.001f, 1.0f);
+    float fmu = mu * 32.0f - 0.5f;
+    float fal = alpha * 32.0f - 0.5f;
+    int m0 = min(max((int)floorf(fmu), 0), 31);
+    int a0 = min(max((int)floorf(fal), 0), 31);
+    int m1 = min(m0 + 1, 31);
+    int a1 = min(a0 + 1, 31);
+    float tu = clampf(fmu - (float)m0, 0.0f, 1.0f);
+    float ta = clampf(fal - (float)a0, 0.0f, 1.0f);
+    float e00 = __ldg(e + m0 * 32 + a0), e01 = __ldg(e + m0 * 32 + a1);
+    float e10 = __ldg(e + m1 * 32 + a0), e11 = __ldg(e + m1 * 32 + a1);
+    float x0 = e00 + (e01 - e00) * ta;
+    float x1 = e10 + (e11 - e10) * ta;
+    return x0 + (x1 - x0) * tu;
+}
+
+// ---------------------------------------------------------------------------
+// Microfacet helpers (Materials/Microfacet.cs) and Charlie sheen
+// (Materials/SheenCharlie.cs)
+// ---------------------------------------------------------------------------
+RT_D void tangent_frame(V3 n, V3& t, V3& b) {   // Microfacet.cs:22-37
+    if (n.z < -0.999f) {
+        t = v3(0.0f, -1.0f, 0.0f);
+        b = v3(-1.0f, 0.0f, 0.0f);
+    } else {
+        float a = 1.0f / (1.0f + n.z);
+        float bb = -n.x * n.y * a;
+        t = v3(1.0f - n.x * n.x * a, bb, -n.x);
+        b = v3(bb, 1.0f - n.y * n.y * a, -n.y);
+    }
+}
+RT_D float d_ggx(V3 h, float ax, float ay) {   // :43-49
+    float hx = h.x / ax;
+    float hy = h.y / ay;
+    float d = hx * hx + hy * hy + h.z * h.z;
+    return 1.0f / fmaxf(kPi * ax * ay * d * d, 1e-20f);
+}
+RT_D float g1_ggx(V3 w, float ax, float ay) {   // :55-69
+    float c2 = w.z * w.z;
+    float lam;
+    if (c2 < 1e-14f) {
+        lam = 1e10f;
+    } else {
+        float num = (ax * w.x) * (ax * w.x) + (ay * w.y) * (ay * w.y);
+        lam = 0.5f * (-1.0f + sqrtf(1.0f + num / c2));
+    }
+    return 1.0f / (1.0f + lam);
+}
+RT_D float smith_g1(float ndx, float alpha) {   // :75-81
+    float a2 = alpha * alpha;
+    float n2 = ndx * ndx;
+    float denom = ndx + sqrtf(a2 + (1.0f - a2) * n2);
+    return 2.0f * ndx / fmaxf(denom, 1e-7f);
+}
+RT_D V3 sample_vndf(V3 vl, float ax, float ay, float u1, float u2) {   // :100-124
+    V3 vh = normalize(v3(ax * vl.x, ay * vl.y, vl.z));
+    float lsq = vh.x * vh.x + vh.y * vh.y;
+    V3 t1 = lsq > 0.0f ? v3(-vh.y, vh.x, 0.0f) / sqrtf(lsq) : v3(1.0f, 0.0f, 0.0f);
+    V3 t2 = cross(vh, t1);
+    float r = sqrtf(u1);
+    float phi = 2.0f * kPi * u2;
+    float sn, cs;
+    sincosf(phi, &sn, &cs);
+    float a1 = r * cs;
+    float a2 = r * sn;
+    float s = 0.5f * (1.0f + vh.z);
+    a2 = (1.0f - s) * sqrtf(fmaxf(0.0f, 1.0f - a1 * a1)) + s * a2;
+    V3 nh = a1 * t1 + a2 * t2 + sqrtf(fmaxf(0.0f, 1.0f - a1 * a1 - a2 * a2)) * vh;
+    return normalize(v3(ax * nh.x, ay * nh.y, fmaxf(0.0f, nh.z)));
+}
+RT_D float sheen_lambda_log(float c, bool smooth) {   // SheenCharlie.cs:40-65
+    float a, b, cc, d, e;
+    if (smooth) {
+        a = 25.3245f; b = 3.32435f; cc = 0.16801f; d = -1.27393f; e = -4.85967f;
+    } else {
+        a = 21.5473f; b = 3.82987f; cc = 0.19823f; d = -1.97760f; e = -4.32054f;
+    }
+    return a / (1.0f + b * powf(c, cc)) + d * c + e;
+}
+RT_D float sheen_lambda(float c, float alpha) {   // :71-85
+    c = clampf(c, 1e-4f, 1.0f);
+    if (alpha <= 0.25f - 0.05f) return expf(sheen_lambda_log(c, true));
+    if (alpha >= 0.25f + 0.05f) return expf(sheen_lambda_log(c, false));
+    float t = (alpha - (0.25f - 0.05f)) / (2.0f * 0.05f);
+    float lo = expf(sheen_lambda_log(c, true));
+    float hi = expf(sheen_lambda_log(c, false));
+    return lo + (hi - lo) * t;
+}
+RT_D float sheen_brdf(float ndv, float ndl, float ndh, float alpha) {   // :24-34, :92-121
+    float denom = 4.0f * fmaxf(ndv, 1e-6f) * fmaxf(ndl, 1e-6f);
+    float g = 1.0f / ((1.0f + sheen_lambda(ndv, alpha)) * (1.0f + sheen_lambda(ndl, alpha)));
+    float al = fmaxf(alpha, 0.04f);
+    float inv = 1.0f / al;
+    float c2 = ndh * ndh;
+    float s2 = fmaxf(1.0f - c2, 0.0f);
+    float sp = powf(s2, 0.5f * inv);
+    float D = (2.0f + inv) * sp / (2.0f * kPi);
+    return D * g / denom;
+}
+RT_D float schlick_weight(float c) {   // DisneyBsdf.cs:1994-1999
+    float x = clampf(1.0f - c, 0.0f, 1.0f);
+    float x2 = x * x;
+    return x2 * x2 * x;
+}
+RT_D V3 fresnel_schlick(float c, V3 f0) {   // :1963-1967 (thin film off)
+    float w = schlick_weight(c);
+    return f0 + (v3(1.0f) - f0) * w;
+}
+RT_D float fresnel_dielectric(float ci, float eta) {   // Core/MathUtils.cs:191-201
+    ci = clampf(ci, 0.0f, 1.0f);
+    float s2i = fmaxf(0.0f, 1.0f - ci * ci);
+    float s2t = eta * eta * s2i;
+    if (s2t >= 1.0f) return 1.0f;
+    float ct = sqrtf(1.0f - s2t);
+    float rpa = (ci - eta * ct) / (ci + eta * ct);
+    float rpe = (eta * ci - ct) / (eta * ci + ct);
+    return 0.5f * (rpa * rpa + rpe * rpe);
+}
+RT_D V3 refract(V3 uv, V3 n, float eta) {   // Core/MathUtils.cs:160-166
+    float ct = fminf(dot(-uv, n), 1.0f);
+    V3 perp = eta * (uv + ct * n);
+    V3 par = -sqrtf(fabsf(1.0f - length_sq(perp))) * n;
+    return perp + par;
+}
+
+// ---------------------------------------------------------------------------
+// Disney BSDF (Materials/DisneyBsdf.cs) on host-precomputed material constants
+// ---------------------------------------------------------------------------
+struct Frame {
+    V3 t, b, n;
+    RT_D V3 to_local(V3 w) const { return v3(dot(w, t), dot(w, b), dot(w, n)); }
+    RT_D V3 to_world(V3 w) const { return w.x * t + w.y * b + w.z * n; }
+};
+
+RT_D Frame shading_frame(const Surface& rec, const Material& m) {   // :1840-1877
+    V3 n = rec.n, t, b;
+    if (length_sq(rec.tangent) > 1e-10f && length_sq(rec.bitangent) > 1e-10f) {
+        t = rec.tangent - dot(rec.tangent, n) * n;
+        float tl = length_sq(t);
+        if (tl > 1e-10f) {
+            t = t / sqrtf(tl);
+            b = cross(n, t);
+        } else {
+            tangent_frame(n, t, b);
+        }
+    } else {
+        tangent_frame(n, t, b);
+    }
+    if (m.has_rotation) {
+        float c = m.rot_cos, s = m.rot_sin;
+        V3 tr = c * t + s * b;
+        V3 br = -s * t + c * b;
+        t = tr;
+        b = br;
+    }
+    return Frame{t, b, n};
+}
+
+RT_D V3 multiscatter_weight(const SceneView& s, const Material& m, float ndv, float ndl) {   // :1906-1926
+    float e_out = lut_e(s.lut_e, ndv, m.alpha_iso);
+    float e_in = lut_e(s.lut_e, ndl, m.alpha_iso);
+    float e_avg = m.e_avg;
+    float one_m = fmaxf(1.0f - e_avg, 1e-6f);
+    V3 f_avg = m.f0 + (v3(1.0f) - m.f0) * (1.0f / 21.0f);
+    V3 den = v3(1.0f) - f_avg * (1.0f - e_avg);
+    den = v3(fmaxf(den.x, 1e-6f), fmaxf(den.y, 1e-6f), fmaxf(den.z, 1e-6f));
+    V3 f_ms = f_avg * f_avg * e_avg / den;
+    return f_ms * ((1.0f - e_out) * (1.0f - e_in) / one_m);
+}
+
+// EvaluateDirect (:418-535): f(V,L) * max(N.L, 0), the NEE integrand.
+RT_D V3 bsdf_eval_direct(const SceneView& s, const Material& m, const Surface& rec, V3 L, V3 V, V3 N) {
+    float ndl = fmaxf(dot(N, L), 0.0f);
+    if (ndl <= 0.0f) return v3(0.0f);
+    float ndv = fmaxf(dot(N, V), 0.001f);
+    V3 H = normalize(L + V);
+    float ndh = fmaxf(dot(N, H), 0.0f);
+    float vdh = fmaxf(dot(V, H), 0.0f);
+    float ldh = fmaxf(dot(L, H), 0.0f);
+    V3 bc = m.base;
+    V3 diffuse = v3(0.0f);
+    if (m.diffuse_w > 0.0f) {
+        float fd90 = 0.5f + 2.0f * m.roughness * ldh * ldh;
+        float fi = schlick_weight(ndv), fo = schlick_weight(ndl);
+        float fd = (1.0f + (fd90 - 1.0f) * fi) * (1.0f + (fd90 - 1.0f) * fo);
+        diffuse = bc * fd * (m.diffuse_w * ndl / kPi);
+    }
+    V3 specular = v3(0.0f);
+    if (m.alpha > kDeltaAlpha) {
+        Frame fr = shading_frame(rec, m);
+        V3 vl = fr.to_local(V), ll = fr.to_local(L), hl = fr.to_local(H);
+        float D = d_ggx(hl, m.alpha_x, m.alpha_y);
+        float G = g1_ggx(vl, m.alpha_x, m.alpha_y) * g1_ggx(ll, m.alpha_x, m.alpha_y);
+        V3 F = fresnel_schlick(vdh, m.f0);
+        specular = D * G * F / fmaxf(4.0f * ndv, 1e-6f);
+    }
+    V3 clearcoat = v3(0.0f);
+    if (m.clearcoat > 0.0f && m.cc_alpha > kDeltaAlpha) {
+        V3 cn = rec.n;
+        float cndv = fmaxf(dot(cn, V), 0.001f);
+        float cndl = dot(cn, L);
+        if (cndl > 0.0f) {
+            float cndh = fmaxf(dot(cn, H), 0.0f);
+            float cvdh = fmaxf(dot(V, H), 0.0f);
+            float ca2 = m.cc_alpha * m.cc_alpha;
+            float cden = cndh * cndh * (ca2 - 1.0f) + 1.0f;
+            float cD = ca2 / (kPi * cden * cden);
+            float cG = smith_g1(cndv, m.cc_alpha) * smith_g1(cndl, m.cc_alpha);
+            float cF = m.cc_f0 + (1.0f - m.cc_f0) * schlick_weight(cvdh);
+            clearcoat = v3(m.clearcoat * 0.25f * cD * cG * cF / fmaxf(4.0f * cndv, 1e-6f));
+        }
+    }
+    V3 sheen = v3(0.0f);
+    if (m.sheen > 0.0f && m.diffuse_w > 0.0f) {
+        float sb = sheen_brdf(ndv, ndl, ndh, m.sheen_roughness);
+        sheen = m.sheen * sb * m.sheen_col * ndl;
+    }
+    V3 ms = multiscatter_weight(s, m, ndv, ndl) * (1.0f / kPi) * ndl;
+    return diffuse + sheen + specular + ms + clearcoat;
+}
+
+// Evaluate (:649-771): f(V, L) without the cosine.
+RT_D V3 bsdf_eval(const SceneView& s, const Material& m, const Surface& rec, V3 V, V3 L) {
+    V3 N = rec.n;
+    float ndl = dot(N, L);
+    float ndv = dot(N, V);
+    if (ndv <= 0.0f) return v3(0.0f);
+    V3 bc = m.base;
+    if (ndl <= 0.0f) {
+        if (m.diff_all <= 0.0f || m.diff_trans <= 0.0f) return v3(0.0f);
+        return bc * (m.diff_all * m.diff_trans / kPi);
+    }
+    V3 hraw = V + L;
+    float hl2 = length_sq(hraw);
+    if (hl2 < 1e-14f) return v3(0.0f);
+    V3 H = hraw / sqrtf(hl2);
+    float ndh = fmaxf(dot(N, H), 0.0f);
+    float vdh = fmaxf(dot(V, H), 0.0f);
+    float ldh = fmaxf(dot(L, H), 0.0f);
+    V3 diffuse = v3(0.0f);
+    if (m.diffuse_w > 0.0f) {
+        float fd90 = 0.5f + 2.0f * m.roughness * ldh * ldh;
+        float fi = schlick_weight(ndv), fo = schlick_weight(ndl);
+        float fd = (1.0f + (fd90 - 1.0f) * fi) * (1.0f + (fd90 - 1.0f) * fo);
+        diffuse = bc * fd * (m.diffuse_w / kPi);
+    }
+    V3 sheen = v3(0.0f);
+    if (m.sheen > 0.0f && m.diffuse_w > 0.0f) {
+        float sb = sheen_brdf(ndv, ndl, ndh, m.sheen_roughness);
+        sheen = m.sheen * sb * m.sheen_col;
+    }
+    Frame fr = shading_frame(rec, m);
+    V3 vl = fr.to_local(V), ll = fr.to_local(L), hl = fr.to_local(H);
+    float D = d_ggx(hl, m.alpha_x, m.alpha_y);
+    float G = g1_ggx(vl, m.alpha_x, m.alpha_y) * g1_ggx(ll, m.alpha_x, m.alpha_y);
+    V3 F = fresnel_schlick(vdh, m.f0);
+    V3 specular = D * G / fmaxf(4.0f * ndv * ndl, 1e-7f) * F;
+    V3 clearcoat = v3(0.0f);
+    if (m.clearcoat > 0.0f) {
+        V3 cn = rec.n;
+        float cndv = dot(cn, V), cndl = dot(cn, L);
+        if (cndv > 0.0f && cndl > 0.0f) {
+            float cndh = fmaxf(dot(cn, H), 0.0f);
+            float cvdh = fmaxf(dot(V, H), 0.0f);
+            float ca2 = m.cc_alpha * m.cc_alpha;
+            float cden = cndh * cndh * (ca2 - 1.0f) + 1.0f;
+            float cD = ca2 / (kPi * cden * cden);
+            float cG = smith_g1(cndv, m.cc_alpha) * smith_g1(cndl, m.cc_alpha);
+            float cF = m.cc_f0 + (1.0f - m.cc_f0) * schlick_weight(cvdh);
+            float cc = m.clearcoat * 0.25f * cD * cG * cF / fmaxf(4.0f * cndv * cndl, 1e-7f);
+            clearcoat = v3(cc);
+        }
+    }
+    V3 ms = multiscatter_weight(s, m, ndv, ndl) * (1.0f / kPi);
+    return diffuse + sheen + specular + ms + clearcoat;
+}
+
+// Pdf (:783-870): the one-sample mixture density of Sample.
+RT_D float bsdf_pdf(const Material& m, const Surface& rec, V3 V, V3 L) {
+    V3 N = rec.n;
+    float ndl = dot(N, L);
+    float ndv = dot(N, V);
+    if (ndv <= 0.0f) return 0.0f;
+    float cos_pdf = ndl > 0.0f ? ndl / kPi : 0.0f;
+    float dt_pdf = ndl < 0.0f ? -ndl / kPi : 0.0f;
+    float spec_pdf = 0.0f, cc_pdf = 0.0f;
+    V3 hraw = V + L;
+    float hl2 = length_sq(hraw);
+    if (hl2 >= 1e-14f) {
+        V3 H = hraw / sqrtf(hl2);
+        float ndh = dot(N, H);
+        if (ndh > 0.0f && m.alpha > kDeltaAlpha) {
+            float sndv = fmaxf(ndv, 1e-7f);
+            Frame fr = shading_frame(rec, m);
+            V3 vl = fr.to_local(V), hl = fr.to_local(H);
+            float D = d_ggx(hl, m.alpha_x, m.alpha_y);
+            float g1v = g1_ggx(vl, m.alpha_x, m.alpha_y);
+            spec_pdf = g1v * D / (4.0f * sndv);
+        }
+        if (m.cc_alpha > kDeltaAlpha) {
+            V3 cn = rec.n;
+            float cndv = dot(cn, V), cndh = dot(cn, H);
+            if (cndv > 0.0f && cndh > 0.0f) {
+                float sc = fmaxf(cndv, 1e-7f);
+                float ca2 = m.cc_alpha * m.cc_alpha;
+                float cden = cndh * cndh * (ca2 - 1.0f) + 1.0f;
+                float cD = ca2 / (kPi * cden * cden);
+                float cg1 = smith_g1(cndv, m.cc_alpha);
+                cc_pdf = cg1 * cD / (4.0f * sc);
+            }
+        }
+    }
+    return m.p_d * cos_pdf + m.p_sh * cos_pdf + m.p_ms * cos_pdf + m.p_s * spec_pdf + m.p_c * cc_pdf +
+           m.p_dt * dt_pdf;
+}
+
+enum : int { LOBE_DIFFUSE = 0, LOBE_SPECULAR, LOBE_TRANSMISSION, LOBE_SHEEN, LOBE_MULTISCATTER, LOBE_DIFFTRANS,
+             LOBE_CLEARCOAT };
+
+RT_D bool any_nonfinite(V3 a) { return !isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z); }
+
+// ScatterInternal (:1176-1248) with the lobe samplers (:1263-1709). ray_dir is
+// the incoming ray direction; V = normalize(-ray_dir).
+RT_D bool bsdf_scatter(const SceneView& s, const Material& m, const Surface& rec, V3 ray_dir, float relative_eta,
+                       Sampler& rng, V3& att, V3& dir, int& lobe) {
+    V3 bc = m.base;
+    V3 N = rec.n;
+    V3 V = normalize(-ray_dir);
+    float rnd = rng.next();
+    bool ok = true;
+    if (rnd < m.p_d) {   // ScatterDiffuse (:1263-1306)
+        lobe = LOBE_DIFFUSE;
+        V3 sd = N + random_unit_vector(rng);
+        if (near_zero(sd)) sd = N;
+        sd = normalize(sd);
+        dir = sd;
+        float ndv = fmaxf(dot(N, V), 0.001f);
+        float ndl = fmaxf(dot(N, sd), 0.001f);
+        V3 hraw = V + sd;
+        float hl2 = length_sq(hraw);
+        V3 H = hl2 > 1e-7f ? hraw / sqrtf(hl2) : N;
+        float ldh = fmaxf(dot(sd, H), 0.0f);
+        float fd90 = 0.5f + 2.0f * m.roughness * ldh * ldh;
+        float fi = schlick_weight(ndv), fo = schlick_weight(ndl);
+        float fd = (1.0f + (fd90 - 1.0f) * fi) * (1.0f + (fd90 - 1.0f) * fo);
+        att = bc * fd;
+        att = att * (1.0f - m.diff_trans);
+        att = att / fmaxf(m.p_d, 0.1f);
+    } else if ((rnd -= m.p_d) < m.p_s) {   // ScatterSpecular (:1399-1444)
+        lobe = LOBE_SPECULAR;
+        Frame fr = shading_frame(rec, m);
+        V3 vl = fr.to_local(V);
+        float u1 = rng.next();
+        float u2 = rng.next();
+        V3 hl = sample_vndf(vl, m.alpha_x, m.alpha_y, u1, u2);
+        V3 H = fr.to_world(hl);
+        V3 L = reflect(-V, H);
+        if (dot(L, N) <= 0.0f) {
+            att = v3(0.0f);
+            dir = N;
+            ok = false;
+        } else {
+            dir = L;
+            float vdh = fmaxf(dot(V, H), 1e-4f);
+            V3 fres = fresnel_schlick(vdh, m.f0);
+            float g1l = g1_ggx(fr.to_local(L), m.alpha_x, m.alpha_y);
+            att = fres * g1l;
+            att = att / fmaxf(m.p_s, 0.1f);
+        }
+    } else if ((rnd -= m.p_s) < m.p_t) {   // ScatterTransmission (:1473-1608)
+        lobe = LOBE_TRANSMISSION;
+        bool thin = m.thin_walled != 0;
+        float eta = thin ? (1.0f / m.ior) : (relative_eta > 0.0f ? relative_eta : (rec.front ? (1.0f / m.ior) : m.ior));
+        V3 unit = normalize(ray_dir);
+        Frame fr = shading_frame(rec, m);
+        bool rough = m.roughness > 0.01f;
+        V3 Ht;
+        if (rough) {
+            V3 vl = fr.to_local(V);
+            float u1 = rng.next();
+            float u2 = rng.next();
+            Ht = fr.to_world(sample_vndf(vl, m.alpha_x, m.alpha_y, u1, u2));
+        } else {
+            Ht = N;
+        }
+        if (dot(Ht, unit) > 0.0f) Ht = -Ht;
+        float ct = fminf(dot(-unit, Ht), 1.0f);
+        float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+        bool cannot = !thin && eta * st > 1.0f;
+        float frs = cannot ? 1.0f : fresnel_dielectric(ct, eta);
+        V3 d;
+        bool is_refl;
+        if (frs > rng.next()) {
+            d = reflect(unit, Ht);
+            is_refl = true;
+        } else if (thin) {
+            d = unit;
+            is_refl = false;
+        } else {
+            d = refract(unit, Ht, eta);
+            is_refl = false;
+        }
+        if (near_zero(d)) {
+            d = reflect(unit, N);
+            is_refl = true;
+        }
+        dir = normalize(d);
+        att = is_refl ? v3(1.0f) : m.trans_tint;
+        if (rough) {
+            V3 ll = fr.to_local(dir);
+            ll.z = fabsf(ll.z);
+            att = att * g1_ggx(ll, m.alpha_x, m.alpha_y);
+        }
+        att = att / fmaxf(m.p_t, 0.1f);
+    } else if ((rnd -= m.p_t) < m.p_sh) {   // ScatterSheen (:1354-1388)
+        lobe = LOBE_SHEEN;
+        V3 sd = N + random_unit_vector(rng);
+        if (near_zero(sd)) sd = N;
+        sd = normalize(sd);
+        dir = sd;
+        float ndv = fmaxf(dot(N, V), 1e-4f);
+        float ndl = fmaxf(dot(N, sd), 1e-4f);
+        V3 hraw = V + sd;
+        float hl2 = length_sq(hraw);
+        V3 H = hl2 > 1e-7f ? hraw / sqrtf(hl2) : N;
+        float ndh = fmaxf(dot(N, H), 0.0f);
+        float sb = sheen_brdf(ndv, ndl, ndh, m.sheen_roughness);
+        att = m.sheen * kPi * sb * m.sheen_col;
+        att = att / fmaxf(m.p_sh, 0.1f);
+    } else if ((rnd -= m.p_sh) < m.p_ms) {   // ScatterMultiscatter (:1688-1709)
+        lobe = LOBE_MULTISCATTER;
+        V3 sd = N + random_unit_vector(rng);
+        if (near_zero(sd)) sd = N;
+        sd = normalize(sd);
+        dir = sd;
+        float ndv = fmaxf(dot(N, V), 1e-3f);
+        float ndl = fmaxf(dot(N, sd), 1e-3f);
+        att = multiscatter_weight(s, m, ndv, ndl) / fmaxf(m.p_ms, 0.05f);
+    } else if ((rnd -= m.p_ms) < m.p_dt) {   // ScatterDiffTrans (:1321-1338)
+        lobe = LOBE_DIFFTRANS;
+        V3 sd = -N + random_unit_vector(rng);
+        if (near_zero(sd)) sd = -N;
+        sd = normalize(sd);
+        dir = sd;
+        att = bc * m.diff_trans;
+        att = att / fmaxf(m.p_dt, 0.05f);
+    } else {   // ScatterClearcoat (:1623-1678)
+        lobe = LOBE_CLEARCOAT;
+        V3 cn = rec.n;
+        V3 ct_, cb_;
+        tangent_frame(cn, ct_, cb_);
+        Frame fr{ct_, cb_, cn};
+        if (dot(cn, V) <= 0.0f) {
+            att = v3(0.0f);
+            dir = N;
+            ok = false;
+        } else {
+            V3 vl = fr.to_local(V);
+            float u1 = rng.next();
+            float u2 = rng.next();
+            V3 H = fr.to_world(sample_vndf(vl, m.cc_alpha, m.cc_alpha, u1, u2));
+            V3 L = reflect(-V, H);
+            if (dot(L, N) <= 0.0f || dot(L, cn) <= 0.0f) {
+                att = v3(0.0f);
+                dir = N;
+                ok = false;
+            } else {
+                dir = L;
+                float cndl = fmaxf(dot(cn, L), 1e-4f);
+                float cvdh = fmaxf(dot(V, H), 1e-4f);
+                float fres = m.cc_f0 + (1.0f - m.cc_f0) * schlick_weight(cvdh);
+                float g1l = smith_g1(cndl, m.cc_alpha);
+                att = v3(fres * g1l);
+                att = att / fmaxf(m.p_c, 0.1f);
+            }
+        }
+    }
+    if (any_nonfinite(att)) att = bc;
+    return ok;
+}
+
+struct BsdfSample {
+    V3 wo, f;
+    float pdf;
+    int is_delta;
+    int lobe;
+    int transition;            // 0 none, 1 enter, 2 exit
+    int has_next_absorption;
+    V3 next_absorption;
+};
+
+// Sample (:893-997). Returns false for a null sample.
+RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec, V3 V, float relative_eta,
+                      Sampler& rng, BsdfSample& out) {
+    V3 att, wo;
+    int lobe = -1;
+    out.transition = 0;
+    out.has_next_absorption = 0;
+    bool ok = bsdf_scatter(s, m, rec, -V, relative_eta, rng, att, wo, lobe);
+    out.lobe = lobe;
+    if (!ok) return false;
+    float ndwo = dot(rec.n, wo);
+    out.wo = wo;
+    if (lobe == LOBE_DIFFTRANS) {
+        V3 fb = bsdf_eval(s, m, rec, V, wo);
+        float pb = bsdf_pdf(m, rec, V, wo);
+        if (pb <= 0.0f) {
+            out.f = att;
+            out.pdf = 1.0f;
+            out.is_delta = 1;
+            return true;
+        }
+        out.f = fb;
+        out.pdf = pb;
+        out.is_delta = 0;
+        return true;
+    }
+    if (lobe == LOBE_TRANSMISSION) {
+        if (ndwo < 0.0f && !m.thin_walled) {
+            V3 sg = m.trans_sigma;
+            bool has_sigma = sg.x > 0.0f || sg.y > 0.0f || sg.z > 0.0f;
+            if (rec.front && has_sigma) {
+                out.has_next_absorption = 1;
+                out.next_absorption = sg;
+            } else if (!rec.front) {
+                out.has_next_absorption = 1;
+                out.next_absorption = v3(0.0f);
+            }
+            out.transition = rec.front ? 1 : 2;
+        }
+        out.f = att;
+        out.pdf = 1.0f;
+        out.is_delta = 1;
+        return true;
+    }
+    if (ndwo <= 0.0f) return false;
+    bool nd_spec = lobe == LOBE_SPECULAR && m.alpha <= kDeltaAlpha;
+    bool nd_coat = lobe == LOBE_CLEARCOAT && m.cc_alpha <= kDeltaAlpha;
+    if (nd_spec || nd_coat) {
+        out.f = att;
+        out.pdf = 1.0f;
+        out.is_delta = 1;
+        return true;
+    }
+    out.f = bsdf_eval(s, m, rec, V, wo);
+    out.pdf = bsdf_pdf(m, rec, V, wo);
+    out.is_delta = 0;
+    return true;
+}
+
+// ShadowTransmittance (:560-584) and ShadowAbsorption (:609-614).
+RT_D V3 bsdf_shadow_transmittance(const Material& m, V3 wi, const Surface& rec) {
+    if (m.type != 0) return v3(0.0f);   // Emissive: IMaterial default (opaque)
+    float st = m.spec_trans_raw;
+    if (st <= 0.0f) return v3(0.0f);
+    float eta = 1.0f / m.ior_raw;
+    float c = fminf(fabsf(dot(wi, rec.n)), 1.0f);
+    float fr = fresnel_dielectric(c, eta);
+    return st * (1.0f - fr) * m.trans_tint;
+}
+
+// ---------------------------------------------------------------------------
+// Lights (Lights/*.cs)
+// ---------------------------------------------------------------------------
+struct LightSample {
+    int occluded;     // early "in shadow" (no shadow ray needed)
+    int has_ray;      // a shadow ray must decide visibility
+    V3 color;         // contribution before the shadow transmittance
+    V3 dir;
+    float dist;
+    V3 ray_o;
+    float ray_tmax;
+};
+
+// Draws the light sample (all RNG draws happen here, before any shadow test):
+// GeometryLight.ComputeAreaSample (GeometryLight.cs:149-190),
+// AreaLight.IlluminateAndTestStratified (AreaLight.cs:129-178),
+// DirectionalLight.IlluminateAndTestStratified (DirectionalLight.cs:102-160).
+RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, int si, Sampler& rng) {
+    LightSample r;
+    r.occluded = 0;
+    r.has_ray = 0;
+    r.color = v3(0.0f);
+    r.dist = 0.0f;
+    if (l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH) {
+        V3 sp, ln;
+        float area;
+        if (l.type == LIGHT_GEOM_QUAD) {   // Quad.SampleStratified (Quad.cs:99-109)
+            const QuadData& q = s.quads[l.quad];
+            int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
+            float inv = 1.0f / (float)l.sqrt_samples;
+            float uu = ((float)su + rng.next()) * inv;
+            float vv = ((float)sv + rng.next()) * inv;
+            sp = q.q + uu * q.u + vv * q.v;
+            ln = q.normal;
+            area = q.area;
+        } else {   // Mesh.SampleStratified (Mesh.cs:151-178) + Triangle.Sample
+            int total = max(1, l.sqrt_samples * l.sqrt_samples);
+            float stratum = 1.0f / (float)total;
+            float jit = ((float)si + rng.next()) * stratum;
+            float target = clampf(jit, 0.0f, 0.9999999f) * l.rep_area;
+            int lo = 0, hi = l.mesh_count;   // lower_bound over the cumulative areas
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (s.light_tris[l.mesh_first + mid].cum_area < target) lo = mid + 1;
+                else hi = mid;
+            }
+            int idx = min(max(lo, 0), l.mesh_count - 1);
+            const LightTri& t = s.light_tris[l.mesh_first + idx];
+            float x1 = rng.next();
+            float x2 = rng.next();
+            float r1 = sqrtf(x1);
+            float u = 1.0f - r1;
+            float v = x2 * r1;
+            sp = t.v0 + u * t.e1 + v * t.e2;
+            ln = t.normal;
+            area = l.rep_area;
+        }
+        V3 tl = sp - p;
+        float d2 = length_sq(tl);
+        if (d2 < kEps * kEps) {
+            r.occluded = 1;
+            r.dir = v3(0.0f, 1.0f, 0.0f);
+            return r;
+        }
+        float dist = sqrtf(d2);
+        V3 dir = tl / dist;
+        r.dir = dir;
+        r.dist = dist;
+        float cl = fmaxf(0.0f, dot(-dir, ln));
+        if (cl <= 0.0f) {
+            r.occluded = 1;
+            return r;
+        }
+        V3 so = offset_origin(p, sn);
+        r.has_ray = 1;
+        r.ray_o = so;
+        r.ray_tmax = length(sp - so) - kEps;
+        float atten = area * cl / (d2 * (float)l.shadow_samples);
+        r.color = l.emission * atten;
+        return r;
+    }
+    if (l.type == LIGHT_AREA) {
+        int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
+        float ru = ((float)su + rng.next()) * l.inv_sqrt;
+        float rv = ((float)sv + rng.next()) * l.inv_sqrt;
+        V3 sp = l.corner + ru * l.u + rv * l.v;
+        V3 tl = sp - p;
+        float d2 = length_sq(tl);
+        if (d2 < kEps * kEps) {
+            r.occluded = 1;
+            r.dir = v3(0.0f, 1.0f, 0.0f);
+            return r;
+        }
+        float dist = sqrtf(d2);
+        V3 dir = tl / dist;
+        r.dir = dir;
+        r.dist = dist;
+        float cl = fmaxf(0.0f, dot(-dir, l.normal));
+        if (cl <= 0.0f) return r;   // not in shadow, zero colour
+        V3 so = offset_origin(p, sn);
+        r.has_ray = 1;
+        r.ray_o = so;
+        r.ray_tmax = length(sp - so) - kEps;
+        float ad2 = d2;
+        if (l.soft_radius > 0.0f) ad2 = fmaxf(ad2, l.soft_radius * l.soft_radius);
+        float atten = l.intensity * l.area * cl / (ad2 * (float)l.shadow_samples);
+        r.color = l.color * atten;
+        return r;
+    }
+    // Directional
+    V3 tl;
+    if (l.angular_radius > 0.0f) {
+        int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
+        float xi1 = ((float)su + rng.next()) * l.inv_sqrt;
+        float xi2 = ((float)sv + rng.next()) * l.inv_sqrt;
+        float ct = 1.0f - xi1 * (1.0f - l.cos_angular);
+        float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+        float phi = 2.0f * kPi * xi2;
+        float sn2, cs2;
+        sincosf(phi, &sn2, &cs2);
+        V3 w = -l.direction;
+        V3 loc = v3(st * cs2, st * sn2, ct);
+        V3 uu, vv;
+        tangent_frame(w, uu, vv);   // DirectionalLight.LocalToWorld (:192-213)
+        V3 res = loc.x * uu + loc.y * vv + loc.z * w;
+        float l2 = length_sq(res);
+        tl = l2 > 1e-8f ? res / sqrtf(l2) : w;
+    } else {
+        tl = -l.direction;
+    }
+    r.dir = tl;
+    r.dist = kInf;
+    r.has_ray = 1;
+    r.ray_o = offset_origin(p, sn);
+    r.ray_tmax = kInf;
+    float e = l.intensity / (float)l.shadow_samples;
+    r.color = l.color * e;
+    return r;
+}
+
+// ILight.PdfSolidAngle (GeometryLight.cs:254-279, AreaLight.cs:189-226,
+// DirectionalLight.cs:169-181).
+RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
+    if (l.type == LIGHT_GEOM_QUAD) {
+        const QuadData& q = s.quads[l.quad];
+        float t, a, b;
+        if (!quad_test(q, p, wi, kEps, kInf, false, t, a, b)) return 0.0f;
+        float cl = fabsf(dot(-wi, q.normal));   // |.| makes the face flip irrelevant
+        if (cl < 1e-6f) return 0.0f;
+        float d2 = t * t;
+        if (l.rep_area < 1e-12f) return 0.0f;
+        return d2 / (l.rep_area * cl);
+    }
+    if (l.type == LIGHT_GEOM_MESH) {   // ray cast against the emitter mesh alone
+        Hit h;
+        int err = 0;
+        traverse<false, 64>(s, p, wi, kEps, kInf, h, nullptr, &err, l.mesh_root);
+        if (err || h.kind == HIT_NONE) return 0.0f;
+        const float4* tp = s.tris + 3 * h.slot;
+        V3 n = v3(__ldg(tp).w, __ldg(tp + 1).w, __ldg(tp + 2).w);
+        float cl = fabsf(dot(-wi, n));
+        if (cl < 1e-6f) return 0.0f;
+        float d2 = h.t * h.t;
+        if (l.rep_area < 1e-12f) return 0.0f;
+        return d2 / (l.rep_area * cl);
+    }
+    if (l.type == LIGHT_AREA) {
+        float denom = dot(l.normal, wi);
+        if (fabsf(denom) < 1e-7f) return 0.0f;
+        float t = dot(l.corner - p, l.normal) / denom;
+        if (t <= kEps) return 0.0f;
+        V3 hp = p + t * wi;
+        V3 loc = hp - l.corner;
+        float uu = dot(l.u, l.u), vv = dot(l.v, l.v), uv = dot(l.u, l.v);
+        float det = uu * vv - uv * uv;
+        if (det < 1e-12f) return 0.0f;
+        float lu = dot(loc, l.u), lv = dot(loc, l.v);
+        float a = (lu * vv - lv * uv) / det;
+        float b = (lv * uu - lu * uv) / det;
+        if (a < 0.0f || a > 1.0f || b < 0.0f || b > 1.0f) return 0.0f;
+        float cl = fabsf(denom);
+        if (cl < 1e-6f) return 0.0f;
+        return (t * t) / (l.area * cl);
+    }
+    if (l.angular_radius <= 0.0f || l.solid_angle <= 0.0f) return 0.0f;
+    float wl = length(wi);
+    if (wl < kEps) return 0.0f;
+    float ct = dot(wi / wl, -l.direction);
+    if (ct < l.cos_angular) return 0.0f;
+    return 1.0f / l.solid_angle;
+}
+
+RT_D float mis_weight(float p, float q, int power) {   // Renderer.cs:1534-1543
+    if (power) {
+        float p2 = p * p, q2 = q * q;
+        return p2 / (p2 + q2 + 1e-30f);
+    }
+    return p / (p + q + 1e-30f);
+}
+
+// Geometry/ShadowRay.cs:59-157. Opaque scenes take the any-hit fast path: with
+// no transmissive material the walk returns 0 at the first hit, so "any hit in
+// [tmin, tmax]" decides it exactly.
+template <int STACK>
+__device__ __forceinline__ V3 shadow_transmittance(const SceneView& s, int opaque_scene, V3 o, V3 d, float tmin,
+                                                   float tmax, Counters* cnt, int* err) {
+    Hit h;
+    if (cnt) cnt->shadow_rays++;
+    if (opaque_scene) {
+        traverse<true, STACK>(s, o, d, tmin, tmax, h, cnt, err);
+        return h.kind == HIT_NONE ? v3(1.0f) : v3(0.0f);
+    }
+    V3 thr = v3(1.0f);
+    float remaining = tmax;
+    V3 sigma = v3(0.0f), entry = v3(0.0f);
+    bool in_med = false;
+    for (int i = 0; i < 8; i++) {
+        traverse<false, STACK>(s, o, d, tmin, remaining, h, cnt, err);
+        if (h.kind == HIT_NONE) return thr;
+        Surface rec = make_surface(s, h, o, d);
+        const Material& m = s.materials[rec.material];
+        if (in_med) {
+            float dd = length(rec.p - entry);
+            thr = v3(thr.x * expf(-sigma.x * dd), thr.y * expf(-sigma.y * dd), thr.z * expf(-sigma.z * dd));
+            in_med = false;
+            if (near_zero(thr)) return v3(0.0f);
+        }
+        V3 t = bsdf_shadow_transmittance(m, d, rec);
+        if (near_zero(t)) return v3(0.0f);
+        thr = thr * t;
+        if (near_zero(thr)) return v3(0.0f);
+        if (rec.front && m.type == 0) {
+            V3 sg = m.trans_sigma;
+            if (!near_zero(sg)) {
+                in_med = true;
+                entry = rec.p;
+                sigma = sg;
+            }
+        }
+        V3 on = dot(d, rec.n) >= 0.0f ? rec.n : -rec.n;
+        o = offset_origin(rec.p, on);
+        remaining -= rec.t + 2.0f * kEps;
+        if (remaining <= tmin) return thr;
+    }
+    return v3(0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Homogeneous medium + Henyey-Greenstein (Volumetrics/HomogeneousMedium.cs,
+// Volumetrics/HenyeyGreensteinPhase.cs)
+// ---------------------------------------------------------------------------
+RT_D V3 medium_tr(const SceneView& s, float t) {
+    float d = fminf(fmaxf(t, 0.0f), 1e30f);
+    return v3(expf(-s.sigma_t.x * d), expf(-s.sigma_t.y * d), expf(-s.sigma_t.z * d));
+}
+RT_D float hg_eval(float g, V3 wo, V3 wi) {
+    float mu = dot(wo, wi);
+    float den = 1.0f + g * g - 2.0f * g * mu;
+    return kInv4Pi * (1.0f - g * g) / (den * sqrtf(den));
+}
+RT_D V3 hg_sample(float g, V3 wo, Sampler& rng, float& pdf) {
+    float u1 = rng.next(), u2 = rng.next();
+    float ct;
+    if (fabsf(g) < 1e-3f) {
+        ct = 1.0f - 2.0f * u1;
+    } else {
+        float sqr = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
+        ct = (1.0f + g * g - sqr * sqr) / (2.0f * g);
+    }
+    float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+    float phi = 2.0f * kPi * u2;
+    float sn, cs;
+    sincosf(phi, &sn, &cs);
+    V3 w = wo;
+    V3 a = fabsf(w.x) > 0.9f ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    V3 v = normalize(cross(w, a));
+    V3 u = cross(w, v);
+    V3 wi = st * cs * u + st * sn * v + ct * w;
+    wi = normalize(wi);
+    pdf = hg_eval(g, wo, wi);
+    return wi;
+}
+RT_D bool medium_sample(const SceneView& s, float tmax, Sampler& rng, float& t, V3& beta) {
+    int ch = (int)(rng.next() * 3.0f);
+    if (ch > 2) ch = 2;
+    float st = ch == 0 ? s.sigma_t.x : (ch == 1 ? s.sigma_t.y : s.sigma_t.z);
+    if (st <= 0.0f) {
+        t = tmax;
+        beta = v3(1.0f);
+        return false;
+    }
+    float dist = -logf(1.0f - rng.next()) / st;
+    bool sc = dist < tmax;
+    t = sc ? dist : tmax;
+    V3 tr = medium_tr(s, t);
+    V3 dens = sc ? s.sigma_t * tr : tr;
+    float pdf = (dens.x + dens.y + dens.z) / 3.0f;
+    if (pdf < 1e-20f) pdf = 1.0f;
+    beta = sc ? (tr * s.sigma_s / pdf) : (tr / pdf);
+    return sc;
+}
+
+RT_D V3 sanitize(V3 c) {   // Renderer.cs:917-923
+    if (!isfinite(c.x)) c.x = 0.0f;
+    if (!isfinite(c.y)) c.y = 0.0f;
+    if (!isfinite(c.z)) c.z = 0.0f;
+    return vmax(c, v3(0.0f));
+}
+RT_D V3 clamp_lum(V3 c, float mx) {   // ClampRadiance / ClampRadianceIndirect (:931-972)
+    c = sanitize(c);
+    float lum = luminance(c);
+    if (lum > mx && lum > 0.0f) c = c * (mx / lum);
+    return c;
+}
+RT_D V3 beer_lambert(V3 rad, V3 sigma, float t) {   // Renderer.cs:1791-1800
+    if (sigma.x <= 0.0f && sigma.y <= 0.0f && sigma.z <= 0.0f) return rad;
+    if (isinf(t) && t > 0.0f) return v3(0.0f);
+    if (t <= 0.0f) return rad;
+    return rad * v3(sigma.x > 0.0f ? expf(-sigma.x * t) : 1.0f, sigma.y > 0.0f ? expf(-sigma.y * t) : 1.0f,
+                    sigma.z > 0.0f ? expf(-sigma.z * t) : 1.0f);
+}
+
+}  // namespace rt

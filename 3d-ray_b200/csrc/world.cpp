@@ -1,0 +1,712 @@
+// Host-side world assembly and the binned-SAH BVH build (see world.h).
+// Compiled with -ffp-contract=off: every float result here must equal what the
+// C# host computes for the same scene.
+#include "world.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <thread>
+
+namespace rt {
+
+namespace {
+
+struct Box {
+    V3 mn, mx;
+};
+inline Box surround(const Box& a, const Box& b) { return {vmin(a.mn, b.mn), vmax(a.mx, b.mx)}; }
+inline Box empty_box() { return {v3(kInf), v3(-kInf)}; }   // AABB.Empty (Core/AABB.cs:77)
+inline float surface_area(const Box& b) {                   // AABB.SurfaceArea (Core/AABB.cs:70-75)
+    V3 d = b.mx - b.mn;
+    if (d.x < 0.0f || d.y < 0.0f || d.z < 0.0f) return 0.0f;
+    return 2.0f * (d.x * d.y + d.x * d.z + d.y * d.z);
+}
+
+// One binned-SAH tree over `boxes`, built exactly like BvhNode's constructor
+// (fat leaves <= 4, 16 bins per axis, traversal cost 0.5, in-place partition,
+// median fallbacks). Nodes are emitted in pre-order into `out` with indices
+// local to `out`; `idx` ends in leaf order.
+struct SahBuilder {
+    static const int kMaxLeaf = 4;    // BvhNode.cs:53
+    static const int kBins = 16;      // BvhNode.cs:60
+    const std::vector<Box>& boxes;
+    std::vector<int>& idx;
+    std::vector<NodeF>& out;
+    std::vector<Box> nbox;            // node boxes (for the parent union)
+    int leaf_kind;
+    int max_depth = 0;                // interior nodes on the longest root-leaf path
+
+    SahBuilder(const std::vector<Box>& b, std::vector<int>& i, std::vector<NodeF>& o, int kind)
+        : boxes(b), idx(i), out(o), leaf_kind(kind) {}
+
+    static void set_node(NodeF& n, const Box& b, int a, int bb) {
+        n.lo[0] = b.mn.x; n.lo[1] = b.mn.y; n.lo[2] = b.mn.z;
+        n.hi[0] = b.mx.x; n.hi[1] = b.mx.y; n.hi[2] = b.mx.z;
+        std::memcpy(&n.lo[3], &a, 4);
+        std::memcpy(&n.hi[3], &bb, 4);
+    }
+
+    bool split(int start, int end, int& best_axis, int& mid) {   // BvhNode.cs:218-363
+        int span = end - start;
+        V3 cmin = v3(kInf), cmax = v3(-kInf);
+        for (int i = start; i < end; i++) {
+            const Box& b = boxes[idx[i]];
+            V3 c = (b.mn + b.mx) * 0.5f;
+            cmin = vmin(cmin, c);
+            cmax = vmax(cmax, c);
+        }
+        V3 ext = cmax - cmin;
+        float max_ext = fmaxf(ext.x, fmaxf(ext.y, ext.z));
+        if (max_ext <= 0.0f) {
+            best_axis = -1;
+            mid = start;
+            return false;
+        }
+        best_axis = -1;
+        int best_bin = -1;
+        float best_cost = kInf;
+        int cnt[kBins], pre_c[kBins], suf_c[kBins];
+        Box bb[kBins], pre_b[kBins], suf_b[kBins];
+        for (int ax = 0; ax < 3; ax++) {
+            float e = axis_of(ext, ax);
+            if (e <= 0.0f) continue;
+            float c0 = axis_of(cmin, ax);
+            float scale = (float)kBins / e;
+            for (int i = 0; i < kBins; i++) {
+                cnt[i] = 0;
+                bb[i] = empty_box();
+            }
+            for (int i = start; i < end; i++) {
+                const Box& b = boxes[idx[i]];
+                float c = axis_of((b.mn + b.mx) * 0.5f, ax);
+                int k = (int)((c - c0) * scale);
+                if (k < 0) k = 0;
+                else if (k >= kBins) k = kBins - 1;
+                cnt[k]++;
+                bb[k] = surround(bb[k], b);
+            }
+            int cum = 0;
+            Box cb = empty_box();
+            for (int i = 0; i < kBins; i++) {
+                cum += cnt[i];
+                cb = surround(cb, bb[i]);
+                pre_c[i] = cum;
+                pre_b[i] = cb;
+            }
+            cum = 0;
+            cb = empty_box();
+            for (int i = kBins - 1; i >= 0; i--) {
+                cum += cnt[i];
+                cb = surround(cb, bb[i]);
+                suf_c[i] = cum;
+                suf_b[i] = cb;
+            }
+            float parent = surface_area(pre_b[kBins - 1]);
+            if (parent <= 0.0f) continue;
+            for (int i = 0; i < kBins - 1; i++) {
+                int nl = pre_c[i], nr = suf_c[i + 1];
+                if (nl == 0 || nr == 0) continue;
+                float cost = 0.5f + (nl * surface_area(pre_b[i]) + nr * surface_area(suf_b[i + 1])) / parent;
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = ax;
+                    best_bin = i;
+                }
+            }
+        }
+        if (best_axis < 0) {
+            mid = start;
+            return false;
+        }
+        float amin = axis_of(cmin, best_axis);
+        float ascale = (float)kBins / axis_of(ext, best_axis);
+        int wp = start;
+        for (int i = start; i < end; i++) {
+            const Box& b = boxes[idx[i]];
+            float c = axis_of((b.mn + b.mx) * 0.5f, best_axis);
+            int k = (int)((c - amin) * ascale);
+            if (k < 0) k = 0;
+            else if (k >= kBins) k = kBins - 1;
+            if (k <= best_bin) {
+                std::swap(idx[i], idx[wp]);
+                wp++;
+            }
+        }
+        mid = wp;
+        if (mid == start || mid == end) mid = start + span / 2;
+        return true;
+    }
+
+    // Returns the node index (local to `out`) and its box.
+    int build(int start, int end, int depth, Box& box_out) {   // BvhNode.cs:91-152
+        int me = (int)out.size();
+        out.push_back(NodeF{});
+        int span = end - start;
+        if (span <= kMaxLeaf) {
+            Box b = boxes[idx[start]];
+            for (int i = 1; i < span; i++) b = surround(b, boxes[idx[start + i]]);
+            set_node(out[me], b, ~start, span | (leaf_kind << 16));
+            box_out = b;
+            max_depth = std::max(max_depth, depth);
+            return me;
+        }
+        int axis, mid;
+        if (!split(start, end, axis, mid)) {
+            axis = 0;
+            mid = start + span / 2;
+        }
+        Box lb, rb;
+        int l = build(start, mid, depth + 1, lb);
+        int r = build(mid, end, depth + 1, rb);
+        Box b = surround(lb, rb);
+        set_node(out[me], b, l, r | (axis << 30));
+        box_out = b;
+        return me;
+    }
+};
+
+inline Box tri_box(V3 a, V3 b, V3 c) {   // Triangle.BoundingBox (Geometry/Triangle.cs:144-149)
+    return {vmin(vmin(a, b), c) - v3(kEps), vmax(vmax(a, b), c) + v3(kEps)};
+}
+
+struct MeshBuild {
+    std::vector<NodeF> nodes;
+    std::vector<int> order;   // local triangle ids in leaf order
+    Box box;
+    int max_depth = 0;
+    bool is_list = false;
+};
+
+void build_mesh(const float* tv, int64_t count, MeshBuild& mb) {
+    std::vector<Box> boxes((size_t)count);
+    for (int64_t t = 0; t < count; t++) {
+        const float* p = tv + t * 9;
+        boxes[t] = tri_box(v3(p[0], p[1], p[2]), v3(p[3], p[4], p[5]), v3(p[6], p[7], p[8]));
+    }
+    mb.order.resize((size_t)count);
+    for (int64_t t = 0; t < count; t++) mb.order[t] = (int)t;
+    if (count > 4) {   // Mesh.cs:93-96: BvhNode above 4 triangles
+        SahBuilder sb(boxes, mb.order, mb.nodes, LEAF_TRIS);
+        sb.build(0, (int)count, 0, mb.box);
+        mb.max_depth = sb.max_depth;
+    } else {           // HittableList: flat scan, no box test
+        mb.is_list = true;
+        Box b = boxes[0];
+        for (int64_t t = 1; t < count; t++) b = surround(b, boxes[t]);
+        mb.box = b;
+        NodeF n{};
+        SahBuilder::set_node(n, b, ~0, (int)count | (LEAF_LIST << 16));
+        mb.nodes.push_back(n);
+    }
+}
+
+float light_power(const Light& l, const Box& bounds) {
+    if (l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH)   // GeometryLight.cs:116-120
+        return kPi * l.rep_area * luminance(l.emission);
+    if (l.type == LIGHT_AREA) return kPi * l.area * luminance(l.color) * l.intensity;   // AreaLight.cs:111
+    V3 ext = bounds.mx - bounds.mn;                                                     // DirectionalLight.cs:82-88
+    float radius = 0.5f * length(ext);
+    float cs = kPi * radius * radius;
+    return luminance(l.color) * l.intensity * cs;
+}
+
+// VNDF sampling (Materials/Microfacet.cs:100-124), host copy for the LUT build.
+V3 vndf_host(V3 vl, float ax, float ay, float u1, float u2) {
+    V3 vh = normalize(v3(ax * vl.x, ay * vl.y, vl.z));
+    float lsq = vh.x * vh.x + vh.y * vh.y;
+    V3 t1 = lsq > 0.0f ? v3(-vh.y, vh.x, 0.0f) / std::sqrt(lsq) : v3(1.0f, 0.0f, 0.0f);
+    V3 t2 = cross(vh, t1);
+    float r = std::sqrt(u1);
+    float phi = 2.0f * kPi * u2;
+    float a1 = r * std::cos(phi);
+    float a2 = r * std::sin(phi);
+    float s = 0.5f * (1.0f + vh.z);
+    a2 = (1.0f - s) * std::sqrt(std::fmax(0.0f, 1.0f - a1 * a1)) + s * a2;
+    V3 nh = a1 * t1 + a2 * t2 + std::sqrt(std::fmax(0.0f, 1.0f - a1 * a1 - a2 * a2)) * vh;
+    return normalize(v3(ax * nh.x, ay * nh.y, std::fmax(0.0f, nh.z)));
+}
+
+float g1_aniso_host(V3 w, float ax, float ay) {   // Microfacet.cs:55-69
+    float c2 = w.z * w.z;
+    float lam;
+    if (c2 < 1e-14f) {
+        lam = 1e10f;
+    } else {
+        float num = (ax * w.x) * (ax * w.x) + (ay * w.y) * (ay * w.y);
+        lam = 0.5f * (-1.0f + std::sqrt(1.0f + num / c2));
+    }
+    return 1.0f / (1.0f + lam);
+}
+
+float sample_eavg_host(const float* eavg, float alpha) {   // EnergyCompensationLut.cs:167-175
+    alpha = clampf(alpha, 0.001f, 1.0f);
+    float fal = alpha * 32.0f - 0.5f;
+    int a0 = std::min(std::max((int)std::floor(fal), 0), 31);
+    int a1 = std::min(a0 + 1, 31);
+    float ta = clampf(fal - (float)a0, 0.0f, 1.0f);
+    return eavg[a0] + (eavg[a1] - eavg[a0]) * ta;
+}
+
+}  // namespace
+
+void build_energy_lut(float* e, float* eavg) {   // EnergyCompensationLut.cs:48-134
+    const int kMu = 32, kAl = 32, kSpb = 2048;
+    for (int ai = 0; ai < kAl; ai++) {
+        float alpha = std::fmax(((float)ai + 0.5f) / (float)kAl, 0.001f);
+        for (int mi = 0; mi < kMu; mi++) {
+            float mu = ((float)mi + 0.5f) / (float)kMu;
+            uint32_t seed = ((uint32_t)mi * 0x9E3779B9u) ^ ((uint32_t)ai * 0xB5297A4Du) ^ 0xC2B2AE3Du;
+            float st = std::sqrt(std::fmax(0.0f, 1.0f - mu * mu));
+            V3 V = v3(st, 0.0f, mu);
+            double sum = 0.0;
+            uint32_t s = seed == 0 ? 1u : seed;
+            int hits = 0;
+            for (int k = 0; k < kSpb; k++) {
+                s ^= s << 13; s ^= s >> 17; s ^= s << 5;
+                float u1 = (float)(s & 0x00FFFFFFu) / (float)0x01000000u;
+                s ^= s << 13; s ^= s >> 17; s ^= s << 5;
+                float u2 = (float)(s & 0x00FFFFFFu) / (float)0x01000000u;
+                V3 H = vndf_host(V, alpha, alpha, u1, u2);
+                float vdh = dot(V, H);
+                V3 L = 2.0f * vdh * H - V;
+                if (L.z <= 0.0f) continue;
+                sum += (double)g1_aniso_host(L, alpha, alpha);
+                hits++;
+            }
+            double m = sum / (double)kSpb;
+            m = m < 0.0 ? 0.0 : (m > 1.0 ? 1.0 : m);
+            e[mi * kAl + ai] = hits == 0 ? 0.0f : (float)m;
+        }
+        float avg = 0.0f;
+        for (int mi = 0; mi < kMu; mi++) avg += 2.0f * e[mi * kAl + ai] * (((float)mi + 0.5f) / (float)kMu);
+        eavg[ai] = clampf(avg / (float)kMu, 0.0f, 1.0f);
+    }
+}
+
+Camera make_camera(const RtCameraDesc& c, float aspect) {   // Camera.cs:26-51
+    V3 from = v3(c.look_from[0], c.look_from[1], c.look_from[2]);
+    V3 at = v3(c.look_at[0], c.look_at[1], c.look_at[2]);
+    V3 vup = v3(c.vup[0], c.vup[1], c.vup[2]);
+    float theta = c.vfov_deg * kPi / 180.0f;
+    float h = std::tan(theta / 2.0f);
+    float vh = 2.0f * h;
+    float vw = aspect * vh;
+    V3 w = normalize(from - at);
+    if (length_sq(cross(w, vup)) < 1e-8f) vup = std::fabs(w.x) < 0.9f ? v3(1, 0, 0) : v3(0, 0, 1);
+    V3 u = normalize(cross(vup, w));
+    V3 v = cross(w, u);
+    float fd = c.focus_dist;
+    Camera cam;
+    cam.origin = from;
+    cam.horizontal = fd * vw * u;
+    cam.vertical = fd * vh * v;
+    cam.llc = from - cam.horizontal / 2.0f - cam.vertical / 2.0f - fd * w;
+    return cam;
+}
+
+Material make_material(const RtMaterialDesc& d, const float* eavg) {
+    Material m{};
+    m.type = d.type;
+    m.thin_walled = d.thin_walled;
+    m.has_tc = d.has_transmission_color;
+    m.base = v3(d.base_color[0], d.base_color[1], d.base_color[2]);
+    m.emission = m.base * std::fmax(d.intensity, 0.0f);   // Emissive: Albedo * Intensity
+    // ShadingParams (DisneyBsdf.cs:237-291)
+    m.metallic = clampf(d.metallic, 0.0f, 1.0f);
+    m.roughness = clampf(d.roughness, 0.0f, 1.0f);
+    m.specular = clampf(d.specular, 0.0f, 2.0f);
+    m.specular_tint = clampf(d.specular_tint, 0.0f, 1.0f);
+    m.sheen = clampf(d.sheen, 0.0f, 1.0f);
+    m.sheen_tint = clampf(d.sheen_tint, 0.0f, 1.0f);
+    m.sheen_roughness = clampf(d.sheen_roughness, 0.04f, 1.0f);
+    m.clearcoat = clampf(d.clearcoat, 0.0f, 1.0f);
+    m.clearcoat_gloss = clampf(d.clearcoat_gloss, 0.0f, 1.0f);
+    m.spec_trans = clampf(d.spec_trans, 0.0f, 1.0f);
+    m.ior = std::fmax(d.ior, 1.0001f);
+    m.anisotropic = clampf(d.anisotropic, 0.0f, 1.0f);
+    m.aniso_rotation = d.anisotropic_rotation - std::floor(d.anisotropic_rotation);
+    m.diff_trans = clampf(d.diff_trans, 0.0f, 1.0f);
+    m.alpha = std::fmax(m.roughness * m.roughness, 0.001f);
+    float aspect = std::sqrt(1.0f - 0.9f * m.anisotropic);
+    m.alpha_x = std::fmax(m.alpha / aspect, 0.001f);
+    m.alpha_y = std::fmax(m.alpha * aspect, 0.001f);
+    m.cc_alpha = d.coat_roughness >= 0.0f ? std::fmax(d.coat_roughness * d.coat_roughness, 0.001f)
+                                          : lerpf(0.1f, 0.001f, m.clearcoat_gloss);
+    float eta_c = std::fmax(d.coat_ior, 1.0001f);
+    float r0 = (eta_c - 1.0f) / (eta_c + 1.0f);
+    m.cc_f0 = r0 * r0;
+    m.has_rotation = m.aniso_rotation != 0.0f;
+    float ang = 2.0f * kPi * m.aniso_rotation;
+    m.rot_cos = std::cos(ang);
+    m.rot_sin = std::sin(ang);
+    m.spec_trans_raw = d.spec_trans;
+    m.ior_raw = std::fmax(d.ior, 1.0001f);
+    // ComputeF0 (:1943-1959)
+    V3 bc = m.base;
+    {
+        float r = (m.ior - 1.0f) / (m.ior + 1.0f);
+        float f0d = r * r;
+        float scaled = f0d * 2.0f * m.specular;
+        float lum = luminance(bc);
+        V3 tint = lum > 0.0f ? bc / lum : v3(1.0f);
+        V3 diel = lerp(v3(scaled), scaled * tint, m.specular_tint);
+        m.f0 = lerp(diel, bc, m.metallic);
+        m.sheen_col = lerp(v3(1.0f), tint, m.sheen_tint);
+    }
+    // ResolveTransmission (:1016-1049)
+    if (!d.has_transmission_color) {
+        m.trans_tint = v3(std::sqrt(std::fmax(bc.x, 0.0f)), std::sqrt(std::fmax(bc.y, 0.0f)),
+                          std::sqrt(std::fmax(bc.z, 0.0f)));
+        m.trans_sigma = v3(0.0f);
+    } else {
+        V3 tc = v3(d.transmission_color[0], d.transmission_color[1], d.transmission_color[2]);
+        float depth = std::fmax(d.transmission_depth, 0.0f);
+        if (depth <= 0.0f) {
+            m.trans_tint = tc;
+            m.trans_sigma = v3(0.0f);
+        } else {
+            V3 c = v3(std::fmax(tc.x, 1e-6f), std::fmax(tc.y, 1e-6f), std::fmax(tc.z, 1e-6f));
+            float inv = 1.0f / depth;
+            m.trans_sigma = v3(-std::log(c.x) * inv, -std::log(c.y) * inv, -std::log(c.z) * inv);
+            m.trans_tint = v3(1.0f);
+        }
+    }
+    // ComputeLobeWeights (:1104-1139) and the probabilities (LobeWeights :1094-1101)
+    float diffuse_all = (1.0f - m.metallic) * (1.0f - m.spec_trans);
+    float diffuse_w = diffuse_all * (1.0f - m.diff_trans);
+    float dt_w = diffuse_all * m.diff_trans;
+    float spec_f0;
+    if (m.metallic > 0.5f) {
+        spec_f0 = luminance(bc);
+    } else {
+        float r = (m.ior - 1.0f) / (m.ior + 1.0f);
+        spec_f0 = r * r * 2.0f * m.specular;
+    }
+    float spec_floor = 0.1f * (1.0f - m.spec_trans * 0.9f);
+    float spec_w = std::fmax(spec_floor, lerpf(spec_f0, 1.0f, m.metallic));
+    float trans_w = (1.0f - m.metallic) * m.spec_trans;
+    float clear_w = m.clearcoat * 0.04f;
+    float sheen_w = m.sheen * 0.25f * diffuse_all;
+    m.alpha_iso = std::sqrt(m.alpha_x * m.alpha_y);
+    m.e_avg = sample_eavg_host(eavg, m.alpha_iso);
+    float ms_w = spec_w * (1.0f - m.e_avg);
+    float sum = diffuse_w + spec_w + trans_w + clear_w + sheen_w + ms_w + dt_w;
+    float total = sum < 1e-6f ? 1.0f : sum;
+    m.p_d = diffuse_w / total;
+    m.p_s = spec_w / total;
+    m.p_t = trans_w / total;
+    m.p_c = clear_w / total;
+    m.p_sh = sheen_w / total;
+    m.p_ms = ms_w / total;
+    m.p_dt = dt_w / total;
+    m.diffuse_w = (1.0f - m.metallic) * (1.0f - m.spec_trans) * (1.0f - m.diff_trans);
+    m.diff_all = (1.0f - m.metallic) * (1.0f - m.spec_trans);
+    return m;
+}
+
+int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
+    if (!w || w->num_materials <= 0 || w->num_entities <= 0 || !w->materials || !w->entities) {
+        err = "world needs at least one material and one entity";
+        return RT_ERR_INVALID_ARG;
+    }
+    sc.lut_e.resize(1024);
+    sc.lut_eavg.resize(32);
+    build_energy_lut(sc.lut_e.data(), sc.lut_eavg.data());
+    for (int i = 0; i < w->num_materials; i++) {
+        const RtMaterialDesc& d = w->materials[i];
+        if (d.type != RT_MAT_DISNEY && d.type != RT_MAT_EMISSIVE) {
+            err = "material " + std::to_string(i) + ": only Disney and Emissive are on the GPU path";
+            return RT_ERR_UNSUPPORTED;
+        }
+        if (d.type == RT_MAT_DISNEY && d.thin_film_thickness > 0.0f) {
+            err = "material " + std::to_string(i) + ": thin-film iridescence is outside the GPU path";
+            return RT_ERR_UNSUPPORTED;
+        }
+        sc.materials.push_back(make_material(d, sc.lut_eavg.data()));
+    }
+    const int ne = w->num_entities;
+    // --- mesh BVHs (independent; built in parallel like BvhNode's Parallel.Invoke)
+    std::vector<MeshBuild> mb((size_t)ne);
+    std::vector<int> mesh_ids;
+    for (int e = 0; e < ne; e++) {
+        const RtEntityDesc& d = w->entities[e];
+        if (d.material < 0 || d.material >= w->num_materials) {
+            err = "entity " + std::to_string(e) + ": material index out of range";
+            return RT_ERR_INVALID_ARG;
+        }
+        if (d.kind == RT_ENT_MESH) {
+            if (d.count <= 0 || d.first < 0 || d.first + d.count > w->num_tris || !w->tri_verts) {
+                err = "entity " + std::to_string(e) + ": triangle range out of bounds";
+                return RT_ERR_INVALID_ARG;
+            }
+            mesh_ids.push_back(e);
+        } else if (d.kind != RT_ENT_QUAD && d.kind != RT_ENT_SPHERE) {
+            err = "entity " + std::to_string(e) + ": unsupported kind";
+            return RT_ERR_UNSUPPORTED;
+        }
+    }
+    {
+        std::atomic<size_t> next{0};
+        unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)mesh_ids.size()));
+        auto work = [&]() {
+            for (;;) {
+                size_t k = next.fetch_add(1);
+                if (k >= mesh_ids.size()) break;
+                int e = mesh_ids[k];
+                const RtEntityDesc& d = w->entities[e];
+                build_mesh(w->tri_verts + d.first * 9, d.count, mb[e]);
+            }
+        };
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+    }
+    // --- entities, quads, spheres and their boxes (world objects in YAML order)
+    std::vector<Box> ent_box((size_t)ne);
+    int max_blas_depth = 0;
+    for (int e = 0; e < ne; e++) {
+        const RtEntityDesc& d = w->entities[e];
+        Entity en{d.kind, d.material, (d.flags & RT_ENT_FLAG_BACKFACE_CULLED) ? ENT_BACKFACE_CULLED : 0, -1};
+        if (d.kind == RT_ENT_QUAD) {   // Quad.cs:26-40, BoundingBox :113-120
+            QuadData q{};
+            q.q = v3(d.p[0], d.p[1], d.p[2]);
+            q.u = v3(d.p[3], d.p[4], d.p[5]);
+            q.v = v3(d.p[6], d.p[7], d.p[8]);
+            V3 n = cross(q.u, q.v);
+            q.normal = normalize(n);
+            q.d = dot(q.normal, q.q);
+            q.w = n / dot(n, n);
+            q.tangent = normalize(q.u);
+            q.bitangent = normalize(q.v);
+            q.area = length(n);
+            Box b{q.q, q.q + q.u + q.v};
+            ent_box[e] = {vmin(b.mn, vmin(q.q + q.u, q.q + q.v)) - v3(0.0001f),
+                          vmax(b.mx, vmax(q.q + q.u, q.q + q.v)) + v3(0.0001f)};
+            en.index = (int)sc.quads.size();
+            sc.quads.push_back(q);
+        } else if (d.kind == RT_ENT_SPHERE) {   // Sphere.cs:271-275
+            SphereData s{v3(d.p[0], d.p[1], d.p[2]), d.p[3]};
+            V3 r = v3(s.r);
+            ent_box[e] = {s.c - r, s.c + r};
+            en.index = (int)sc.spheres.size();
+            sc.spheres.push_back(s);
+        } else {
+            ent_box[e] = mb[e].box;
+            max_blas_depth = std::max(max_blas_depth, mb[e].max_depth);
+        }
+        sc.entities.push_back(en);
+    }
+    // --- top level (SceneLoader.cs:460-485): BVH above 4 objects, else a flat list
+    sc.top_is_bvh = ne > 4;
+    int top_depth = 0;
+    if (sc.top_is_bvh) {
+        std::vector<int> order((size_t)ne);
+        for (int e = 0; e < ne; e++) order[e] = e;
+        SahBuilder sb(ent_box, order, sc.nodes, LEAF_ENTS);
+        Box root_box;
+        sc.top_root = sb.build(0, ne, 0, root_box);
+        top_depth = sb.max_depth;
+        sc.top_items = order;
+    } else {
+        sc.top_root = -1;
+        sc.top_items.resize((size_t)ne);
+        for (int e = 0; e < ne; e++) sc.top_items[e] = e;
+    }
+    // --- append mesh BVHs, relocating node and triangle indices
+    for (int e : mesh_ids) {
+        MeshBuild& m = mb[e];
+        int node_base = (int)sc.nodes.size();
+        int tri_base = (int)sc.tri_entity.size();
+        for (NodeF n : m.nodes) {
+            int a, b;
+            std::memcpy(&a, &n.lo[3], 4);
+            std::memcpy(&b, &n.hi[3], 4);
+            if (a >= 0) {
+                a += node_base;
+                int r = b & 0x3FFFFFFF;
+                b = (b & ~0x3FFFFFFF) | (r + node_base);
+            } else {
+                a = ~(~a + tri_base);
+            }
+            std::memcpy(&n.lo[3], &a, 4);
+            std::memcpy(&n.hi[3], &b, 4);
+            sc.nodes.push_back(n);
+        }
+        sc.entities[e].index = node_base;
+        const RtEntityDesc& d = w->entities[e];
+        for (int local : m.order) {
+            const float* p = w->tri_verts + (d.first + local) * 9;
+            V3 v0 = v3(p[0], p[1], p[2]), v1 = v3(p[3], p[4], p[5]), v2 = v3(p[6], p[7], p[8]);
+            V3 e1 = v1 - v0, e2 = v2 - v0;   // Triangle.cs:35-47
+            V3 cr = cross(e1, e2);
+            float cl = length(cr);
+            V3 n = cl > 0.0f ? cr / cl : v3(0.0f, 1.0f, 0.0f);
+            sc.tris.push_back(float4{v0.x, v0.y, v0.z, n.x});
+            sc.tris.push_back(float4{e1.x, e1.y, e1.z, n.y});
+            sc.tris.push_back(float4{e2.x, e2.y, e2.z, n.z});
+            sc.tri_entity.push_back(e);
+            sc.tri_local.push_back(local);
+        }
+    }
+    // Worst-case traversal stack: one far child per interior level of each
+    // tree, plus up to 3 pending entities of a top-level fat leaf.
+    sc.max_stack = top_depth + 4 + max_blas_depth + 1;
+    // --- explicit lights (SceneLoader.cs:446-458)
+    for (int i = 0; i < w->num_lights; i++) {
+        const RtLightDesc& d = w->lights[i];
+        Light l{};
+        l.quad = -1;
+        l.mesh_root = -1;
+        l.mesh_entity = -1;
+        l.emissive_material = -1;
+        l.color = v3(d.color[0], d.color[1], d.color[2]);
+        l.intensity = d.intensity;
+        if (d.type == RT_LIGHT_AREA) {   // AreaLight.cs:67-87
+            l.type = LIGHT_AREA;
+            l.corner = v3(d.corner[0], d.corner[1], d.corner[2]);
+            l.u = v3(d.u[0], d.u[1], d.u[2]);
+            l.v = v3(d.v[0], d.v[1], d.v[2]);
+            l.shadow_samples = std::max(1, d.shadow_samples);
+            l.soft_radius = std::fmax(0.0f, d.soft_radius);
+            V3 cr = cross(l.u, l.v);
+            l.area = length(cr);
+            l.normal = cr / l.area;
+            l.sqrt_samples = (int)std::ceil(std::sqrt((float)l.shadow_samples));
+            l.inv_sqrt = 1.0f / (float)l.sqrt_samples;
+            l.is_delta = 0;
+            l.emissive_material = d.proxy_material;
+            if (d.proxy_material >= w->num_materials) {
+                err = "area light proxy material out of range";
+                return RT_ERR_INVALID_ARG;
+            }
+        } else if (d.type == RT_LIGHT_DIRECTIONAL) {   // DirectionalLight.cs:55-72
+            l.type = LIGHT_DIRECTIONAL;
+            l.direction = normalize(v3(d.direction[0], d.direction[1], d.direction[2]));
+            l.angular_radius = std::fmax(0.0f, d.angular_radius_deg);
+            bool disc = l.angular_radius > 0.0f;
+            float rad = l.angular_radius * kPi / 180.0f;
+            l.cos_angular = disc ? std::cos(rad) : 1.0f;
+            l.solid_angle = disc ? 2.0f * kPi * (1.0f - l.cos_angular) : 0.0f;
+            l.shadow_samples = d.shadow_samples > 0 ? d.shadow_samples : (disc ? 4 : 1);
+            l.sqrt_samples = (int)std::ceil(std::sqrt((float)l.shadow_samples));
+            l.inv_sqrt = 1.0f / (float)l.sqrt_samples;
+            l.is_delta = disc ? 0 : 1;
+        } else {
+            err = "light " + std::to_string(i) + ": unsupported type";
+            return RT_ERR_UNSUPPORTED;
+        }
+        sc.lights.push_back(l);
+    }
+    // --- geometry lights from emissive, non-proxy entities (SceneLoader.cs:805-887)
+    int gls = std::max(1, w->geometry_light_samples);
+    for (int e = 0; e < ne; e++) {
+        const RtEntityDesc& d = w->entities[e];
+        const Material& m = sc.materials[d.material];
+        if (m.type != RT_MAT_EMISSIVE || w->materials[d.material].is_light_proxy) continue;
+        Light l{};
+        l.quad = -1;
+        l.mesh_root = -1;
+        l.mesh_entity = -1;
+        l.shadow_samples = gls;
+        l.sqrt_samples = (int)std::ceil(std::sqrt((float)gls));
+        l.inv_sqrt = 1.0f / (float)l.sqrt_samples;
+        l.is_delta = 0;
+        l.emissive_material = d.material;
+        l.emission = m.emission;
+        if (d.kind == RT_ENT_QUAD) {
+            l.type = LIGHT_GEOM_QUAD;
+            l.quad = sc.entities[e].index;
+            l.rep_area = sc.quads[l.quad].area;
+        } else if (d.kind == RT_ENT_MESH) {
+            l.type = LIGHT_GEOM_MESH;
+            l.mesh_root = sc.entities[e].index;
+            l.mesh_entity = e;
+            l.mesh_first = (int)sc.light_tris.size();
+            l.mesh_count = (int)d.count;
+            float sum = 0.0f;
+            for (int64_t t = 0; t < d.count; t++) {   // Mesh.cs:98-107, ComputeTriangleArea :195-203
+                const float* p = w->tri_verts + (d.first + t) * 9;
+                V3 v0 = v3(p[0], p[1], p[2]), v1 = v3(p[3], p[4], p[5]), v2 = v3(p[6], p[7], p[8]);
+                LightTri lt{};
+                lt.v0 = v0;
+                lt.e1 = v1 - v0;
+                lt.e2 = v2 - v0;
+                V3 cr = cross(lt.e1, lt.e2);
+                float cl = length(cr);
+                lt.normal = cl > 0.0f ? cr / cl : v3(0.0f, 1.0f, 0.0f);
+                float a = 0.5f * length(cross(v1 - v0, v2 - v0));
+                sum += a;
+                lt.cum_area = sum;
+                sc.light_tris.push_back(lt);
+            }
+            l.rep_area = sum;
+        } else {
+            err = "entity " + std::to_string(e) + ": emissive spheres (cone-sampled lights) are outside the GPU path";
+            return RT_ERR_UNSUPPORTED;
+        }
+        sc.lights.push_back(l);
+    }
+    // --- emitter -> light map (Renderer.cs:409-425)
+    sc.emitter_light.assign((size_t)w->num_materials, -1);
+    for (size_t i = 0; i < sc.lights.size(); i++)
+        if (sc.lights[i].type == LIGHT_GEOM_QUAD || sc.lights[i].type == LIGHT_GEOM_MESH)
+            sc.emitter_light[sc.lights[i].emissive_material] = (int)i;
+    for (size_t i = 0; i < sc.lights.size(); i++)
+        if (sc.lights[i].type == LIGHT_AREA && sc.lights[i].emissive_material >= 0)
+            sc.emitter_light[sc.lights[i].emissive_material] = (int)i;
+    // --- RR classifier (Renderer.cs:361-378; ComputeFiniteSceneBounds :475-500)
+    Box bounds;
+    {
+        bool any = false;
+        Box acc = empty_box();
+        if (sc.top_is_bvh) {
+            Box b{v3(sc.nodes[sc.top_root].lo[0], sc.nodes[sc.top_root].lo[1], sc.nodes[sc.top_root].lo[2]),
+                  v3(sc.nodes[sc.top_root].hi[0], sc.nodes[sc.top_root].hi[1], sc.nodes[sc.top_root].hi[2])};
+            V3 dd = b.mx - b.mn;
+            if (dd.x < 1.0e5f && dd.y < 1.0e5f && dd.z < 1.0e5f) {
+                acc = b;
+                any = true;
+            }
+        } else {
+            for (int e = 0; e < ne; e++) {
+                V3 dd = ent_box[e].mx - ent_box[e].mn;
+                if (dd.x < 1.0e5f && dd.y < 1.0e5f && dd.z < 1.0e5f) {
+                    acc = any ? surround(acc, ent_box[e]) : ent_box[e];
+                    any = true;
+                }
+            }
+        }
+        if (any) {
+            bounds = acc;
+        } else {
+            Box raw = ent_box[0];
+            for (int e = 1; e < ne; e++) raw = surround(raw, ent_box[e]);
+            bounds = {vmax(raw.mn, v3(-1.0e3f)), vmin(raw.mx, v3(1.0e3f))};
+        }
+    }
+    float flux = 0.0f;
+    for (const Light& l : sc.lights) flux += light_power(l, bounds);
+    V3 ext = bounds.mx - bounds.mn;
+    float radius = std::fmax(0.5f * length(ext), 1e-3f);
+    float area = 4.0f * kPi * radius * radius;
+    sc.mean_irradiance = flux / area;
+    bool indirect = sc.mean_irradiance < 0.5f;
+    sc.rr_min_bounces = indirect ? 6 : 3;
+    sc.rr_min_survival = indirect ? 0.40f : 0.10f;
+    // --- medium
+    if (w->medium.enabled) {
+        sc.has_medium = 1;
+        sc.sigma_a = vmax(v3(w->medium.sigma_a[0], w->medium.sigma_a[1], w->medium.sigma_a[2]), v3(0.0f));
+        sc.sigma_s = vmax(v3(w->medium.sigma_s[0], w->medium.sigma_s[1], w->medium.sigma_s[2]), v3(0.0f));
+        sc.sigma_t = sc.sigma_a + sc.sigma_s;
+        sc.hg_g = std::fmax(-0.999f, std::fmin(0.999f, w->medium.g));
+    }
+    sc.camera = w->camera;
+    return RT_OK;
+}
+
+}  // namespace rt

@@ -1,0 +1,55 @@
+// Host-side world assembly: what 3d-ray's .NET host does before the bounce
+// loop (SceneLoader world assembly + the binned-SAH build), producing the
+// flattened SoA the kernels read. Without .NET in this environment the SAH
+// build is restated here in C++ (Acceleration/BvhNode.cs:91-364); a .NET host
+// would instead read its own BvhNode tree out into the same arrays.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/rt3d.h"
+#include "scene_types.h"
+
+namespace rt {
+
+struct HostScene {
+    std::vector<NodeF> nodes;
+    std::vector<int> top_items;
+    std::vector<float4> tris;      // 3 per triangle
+    std::vector<int> tri_entity;
+    std::vector<int> tri_local;
+    std::vector<Entity> entities;
+    std::vector<QuadData> quads;
+    std::vector<SphereData> spheres;
+    std::vector<Material> materials;
+    std::vector<Light> lights;
+    std::vector<LightTri> light_tris;
+    std::vector<int> emitter_light;
+    std::vector<float> lut_e, lut_eavg;
+    RtCameraDesc camera{};
+    int top_root = -1;
+    int top_is_bvh = 0;
+    int max_stack = 0;
+    int rr_min_bounces = 3;
+    float rr_min_survival = 0.1f;
+    float mean_irradiance = 0.0f;
+    int has_medium = 0;
+    V3 sigma_a{}, sigma_s{}, sigma_t{};
+    float hg_g = 0.0f;
+};
+
+// Returns RT_OK or an RT_ERR_* code with a message in err.
+int build_world(const RtWorldDesc* w, HostScene& out, std::string& err);
+
+// Kulla-Conty E(mu, alpha) / E_avg(alpha) tables
+// (Materials/EnergyCompensationLut.cs:48-74), built with the host libm.
+void build_energy_lut(float* e1024, float* eavg32);
+
+// Pinhole camera basis (Camera/Camera.cs:26-51) for the given aspect ratio.
+Camera make_camera(const RtCameraDesc& c, float aspect);
+
+// Material constants (DisneyBsdf.cs:213-293, 1104-1139, 1943-1959, 1016-1049).
+Material make_material(const RtMaterialDesc& d, const float* lut_eavg);
+
+}  // namespace rt

@@ -1,0 +1,330 @@
+"""Benchmark of the B200 path-tracing core (one JSON line on rank 0).
+
+Workload: the reference's throughput configuration — 64 fBm-displaced
+icospheres (1 310 722 triangles) on a ground plane, area light + sun, Disney
+materials, 1920x1080, 256 spp, max depth 12 (synthetic, seeded). One step is
+one full frame render (530 841 600 camera samples). The scene (~95 MB of
+nodes and triangles) is resident in HBM before the timed region; L2 is
+flushed between steps by writing a 256 MiB buffer.
+
+  value  : Msamples/s over the K timed steps, device time from CUDA events on
+           the library's launching stream (max over ranks; whole-job total).
+  e2e    : the same metric through rt_render with a HOST film buffer: the
+           per-step render parameters go in, the 24.9 MB linear-HDR film comes
+           back to pinned host memory, both inside the timed region.
+  roofline: algorithmic bytes per sample (reference BVH2 traversal: 32 B per
+           node visit, 36 B per triangle test, 64 B per quad/sphere test,
+           96 B per path segment), counted on the GPU by the counting build
+           over a fixed pixel subsample, times samples per launch, divided by
+           the render kernel's average launch time, against measured HBM.
+  cpu_baseline: the oracle (C++ restatement of 3d-ray's C# loop) on all host
+           cores over a bounded pixel window of the same frame.
+
+Multi-GPU: rendering does not shard in the reference (one process, one
+frame); `--gpus N` runs N independent replicas, one full frame per rank per
+step ("scaling": "weak"), with only a barrier and a max-reduce of the timings.
+
+`--impl reference` times the reference's CPU path (the oracle port: 3d-ray's
+C# cannot run here) on the same configuration and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Msamples/s and time to relMSE 1e-3 on 1 B200: batched wavefront vs plain kernel"
+UNIT = "Msamples/s"
+W, H, SPP, DEPTH = 1920, 1080, 256, 12
+
+
+def load_package():
+    import importlib.util
+    if "rt3d_b200" in sys.modules:
+        return sys.modules["rt3d_b200"]
+    d = os.path.join(ROOT, "3d-ray_b200")
+    spec = importlib.util.spec_from_file_location("rt3d_b200", os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["rt3d_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return 0, 1, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return dist.get_rank(), world, dist
+
+
+def max_over_ranks(x: float, dist) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def build_world():
+    rt = load_package()
+    return rt, rt.scenes.throughput_scene()
+
+
+def cpu_baseline(rt, world, budget_s=12.0, rank=0):
+    """Times the oracle on a bounded pixel window of the same frame."""
+    from oracle import binding
+    binding.build()
+    osc = binding.OracleScene(rt.abi.PackedWorld(world))
+    cores = os.cpu_count() or 1
+    win_w, win_h = 64, 16
+    # Calibrate with a small window, then size the window for ~budget_s.
+    p = rt.abi.render_params(W, H, SPP, DEPTH, pixel_x0=W // 2 - win_w // 2, pixel_y0=H // 2 - win_h // 2,
+                             window_w=win_w, window_h=win_h)
+    t = time.perf_counter()
+    osc.render(p, threads=cores)
+    dt = time.perf_counter() - t
+    rate = win_w * win_h * SPP / dt
+    rows = int(max(16, min(H // 2, budget_s * rate / (win_w * 4 * SPP))))
+    win_w2, win_h2 = win_w * 4, rows
+    p = rt.abi.render_params(W, H, SPP, DEPTH, pixel_x0=W // 2 - win_w2 // 2, pixel_y0=H // 2 - win_h2 // 2,
+                             window_w=win_w2, window_h=win_h2)
+    t = time.perf_counter()
+    osc.render(p, threads=cores)
+    dt = time.perf_counter() - t
+    samples = win_w2 * win_h2 * SPP
+    osc.close()
+    return {"value": samples / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{win_w2}x{win_h2} centre pixels of the 1920x1080 frame at {SPP} spp, depth {DEPTH} "
+                      f"({samples} samples, {dt:.1f} s)"}
+
+
+def run_reference(args):
+    rank, world_size, dist = dist_setup(args.gpus)
+    if rank != 0:
+        barrier(dist)
+        return
+    rt, world = build_world()
+    per = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(rt, world, budget_s=8.0)
+        if i >= args.warmup:
+            per.append(b["value"])
+            base = b
+    v = float(np.mean(per))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "icospheres-64x20480 1920x1080 256spp depth12 (CPU sample window)",
+                       "triangles": world.num_tris},
+            "cpu_baseline": dict(base, value=v),
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    barrier(dist)
+
+
+def flush_l2(torch_mod, buf):
+    buf.fill_(1)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--kernel", default="megakernel", choices=["megakernel", "wavefront"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spp", type=int, default=SPP)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world_size, dist = dist_setup(args.gpus)
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    rt, world = build_world()
+    abi = rt.abi
+    lib = abi.load()
+    pw = abi.PackedWorld(world)
+    scene = C.c_void_p()
+    abi.check(lib.rt_scene_create(pw.ref(), C.byref(scene)), "rt_scene_create")
+    kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
+    spp = args.spp
+    params = abi.render_params(W, H, spp, DEPTH, kernel=kern)
+    film = torch.empty((3, H, W), dtype=torch.float32, device="cuda")
+    l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    st = abi.RtStats()
+
+    def step():
+        abi.check(lib.rt_render_device(scene, C.byref(params), C.c_void_p(film.data_ptr()), C.byref(st)),
+                  "rt_render_device")
+        return st.kernel_ms, st.kernel_launches
+
+    for _ in range(args.warmup):
+        step()
+        flush_l2(torch, l2)
+    torch.cuda.synchronize()
+    barrier(dist)
+    torch.cuda.synchronize()
+    times, launches = [], 0
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            ms, nl = step()
+            times.append(ms)
+            launches += nl
+            flush_l2(torch, l2)
+        torch.cuda.synchronize()
+    barrier(dist)
+    torch.cuda.synchronize()
+    total_ms = max_over_ranks(float(sum(times)), dist)
+    samples_per_step = W * H * spp
+    value = world_size * samples_per_step * args.steps / (total_ms / 1e3) / 1e6
+    ms_per_step = total_ms / args.steps
+
+    # e2e: public API with host buffers (film read back to pinned memory).
+    host_film = torch.empty((3, H, W), dtype=torch.float32).pin_memory()
+    e2e_times = []
+    st2 = abi.RtStats()
+    for i in range(args.steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        abi.check(lib.rt_render(scene, C.byref(params), C.c_void_p(host_film.data_ptr()), C.byref(st2)),
+                  "rt_render")
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_times.append(dt)
+    e2e_total = max_over_ranks(float(sum(e2e_times)), dist)
+    e2e_value = world_size * samples_per_step * args.steps / e2e_total / 1e6
+
+    # Roofline: algorithmic bytes per sample from the counting build on a
+    # fixed subsample (every 8th row and column block), scaled to the launch.
+    cp = abi.render_params(W, H, spp, DEPTH, kernel=abi.KERNEL_MEGAKERNEL, count_work=1)
+    work = {"node_visits": 0, "tri_tests": 0, "other_tests": 0, "closest_rays": 0, "shadow_rays": 0, "samples": 0}
+    stc = abi.RtStats()
+    for (x0, y0) in [(0, 0), (W // 2, H // 2), (W // 4, H // 3), (3 * W // 4, 2 * H // 3)]:
+        cp.pixel_x0, cp.pixel_y0, cp.window_w, cp.window_h = min(x0, W - 64), min(y0, H - 32), 64, 32
+        abi.check(lib.rt_render_device(scene, C.byref(cp), C.c_void_p(film.data_ptr()), C.byref(stc)), "count")
+        work["node_visits"] += stc.node_visits
+        work["tri_tests"] += stc.prim_tests
+        work["other_tests"] += stc.other_tests
+        work["closest_rays"] += stc.closest_rays
+        work["shadow_rays"] += stc.shadow_rays
+        work["samples"] += stc.samples
+    bytes_per_sample = (32 * work["node_visits"] + 36 * work["tri_tests"] + 64 * work["other_tests"]
+                        + 96 * work["closest_rays"]) / max(work["samples"], 1)
+    kernel_s = ms_per_step / 1e3
+    achieved = bytes_per_sample * samples_per_step / kernel_s / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "render_megakernel_icospheres.md")
+    if os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("traffic_bytes_per_full_launch:"):
+                traffic = float(line.split(":")[1])
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": f"icospheres-64x20480 ({world.num_tris} tris) {W}x{H} {spp}spp depth{DEPTH}",
+                       "kernel": args.kernel, "parallelism": f"replicas{world_size}",
+                       "l2": "flushed between steps (256 MiB write)", "spp": spp},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "algorithmic_bytes_per_sample": bytes_per_sample,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback",
+                         "work_per_sample": {k: v / max(work["samples"], 1) for k, v in work.items()
+                                             if k != "samples"}},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(params),
+                    "d2h_bytes_per_step": 3 * W * H * 4},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(rt, world)
+    lib.rt_scene_destroy(scene)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

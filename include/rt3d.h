@@ -1,0 +1,328 @@
+/*
+ * rt3d.h — C-ABI of the B200 path-tracing core for 3d-ray.
+ *
+ * The library replaces 3d-ray's per-pixel bounce loop (Sobol camera rays,
+ * closest-hit and shadow traversal of the host-built SAH BVH, Disney BSDF,
+ * NEE with MIS and Russian roulette, HDR film accumulation). Everything above
+ * that loop — YAML scene loading, the camera description, the CLI and the
+ * `Renderer` API — stays in the host. All entry points take plain pointers and
+ * sizes; no torch or .NET types cross this boundary.
+ *
+ * Conventions
+ *   - Every function returns 0 (RT_OK) or a negative RT_ERR_* code and never
+ *     aborts or traps. rt_last_error() returns a thread-local message.
+ *   - The caller owns every host pointer for the duration of a call; nothing
+ *     is retained after return. The library owns device memory behind the
+ *     opaque RtScene handle.
+ *   - Calls on one RtScene are serialised internally (one CUDA stream per
+ *     scene); distinct scenes may be used from different host threads.
+ *   - Films are planar linear-HDR fp32, channel-major: value (c, x, y) lives
+ *     at out[c*W*H + y*W + x], the layout of 3d-ray's FrameBuffer
+ *     (src/RayTracer/Rendering/FrameBuffer.cs:38).
+ *
+ * Reference seams (file:line in fiorenzobrioni/3d-ray):
+ *   rt_scene_build / rt_scene_create : SceneLoader.Load world assembly
+ *       (src/RayTracer/Scene/SceneLoader.cs:446-485, 805-887) and the SAH
+ *       build (src/RayTracer/Acceleration/BvhNode.cs:91-153)
+ *   rt_render          : Renderer.Render (src/RayTracer/Rendering/Renderer.cs:522-733)
+ *   rt_render_batch    : N independent Renderer.Render calls in one launch
+ *   rt_adjoint         : no counterpart (gradient of an image loss w.r.t.
+ *                        Disney parameters and emitter radiance)
+ *   rt_trace_closest   : IHittable.Hit on the world (Renderer.cs:1624-1647,
+ *                        HittableList.cs:19-37, BvhNode.cs:157-206)
+ *   rt_trace_any       : ShadowRay.Transmittance (Geometry/ShadowRay.cs:59-157)
+ *   rt_bsdf_batch      : DisneyBsdf.Sample/Evaluate/Pdf/EvaluateDirect
+ *                        (Materials/DisneyBsdf.cs:418-997)
+ *   rt_sobol_batch     : OwenSobol.Sample (Core/Sampling/OwenSobol.cs:48-89)
+ */
+#ifndef RT3D_H
+#define RT3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT3D_ABI_VERSION 1
+
+/* ---- status codes -------------------------------------------------------- */
+#define RT_OK                  0
+#define RT_ERR_INVALID_ARG    -1   /* null pointer, bad size, bad enum */
+#define RT_ERR_OOM            -2   /* device or host allocation failed */
+#define RT_ERR_CUDA           -3   /* a CUDA runtime call failed */
+#define RT_ERR_TIMEOUT        -4   /* a bounded device wait expired */
+#define RT_ERR_BOUNDS         -5   /* a checked kernel saw an out-of-range index */
+#define RT_ERR_UNSUPPORTED    -6   /* scene feature outside the GPU path */
+#define RT_ERR_STACK          -7   /* traversal stack bound exceeded */
+#define RT_ERR_NO_DEVICE      -8   /* no CUDA device / extension not usable */
+
+/* ---- scene description (what the host's loader produces) ---------------- */
+
+/* Material kinds (IMaterial implementations on the path). */
+#define RT_MAT_DISNEY   0   /* Materials/DisneyBsdf.cs */
+#define RT_MAT_EMISSIVE 1   /* Materials/Emissive.cs   */
+
+/* One material with constant parameters. Field meanings and defaults follow
+ * the DisneyBsdf constructor (Materials/DisneyBsdf.cs:172-215) and the
+ * Emissive constructor (Materials/Emissive.cs:43-53). */
+typedef struct RtMaterialDesc {
+    int32_t type;                 /* RT_MAT_* */
+    int32_t is_light_proxy;       /* Emissive backing an area light's proxy quad */
+    int32_t thin_walled;          /* DisneyBsdf.ThinWalled */
+    int32_t has_transmission_color;
+    float base_color[3];          /* Disney baseColor, or Emissive colour */
+    float intensity;              /* Emissive intensity (clamped >= 0 by the library) */
+    float metallic, roughness, specular, specular_tint;
+    float sheen, sheen_tint, sheen_roughness;
+    float clearcoat, clearcoat_gloss;
+    float spec_trans, ior;
+    float anisotropic, anisotropic_rotation;
+    float diff_trans;
+    float coat_ior, coat_roughness;   /* coat_roughness < 0 selects the clearcoat_gloss path */
+    float thin_film_thickness, thin_film_ior;
+    float transmission_color[3];
+    float transmission_depth;
+} RtMaterialDesc;
+
+/* Entity kinds (IHittable leaves the world list holds). */
+#define RT_ENT_QUAD   0   /* Geometry/Quad.cs          p[0..2]=Q, p[3..5]=U, p[6..8]=V */
+#define RT_ENT_SPHERE 1   /* Geometry/Sphere.cs        p[0..2]=centre, p[3]=radius     */
+#define RT_ENT_MESH   2   /* Geometry/Mesh.cs of flat Geometry/Triangle.cs,
+                             triangles [first, first+count) of tri_verts          */
+
+#define RT_ENT_FLAG_BACKFACE_CULLED 1  /* Geometry/BackFaceCulledHittable.cs wrapper */
+
+typedef struct RtEntityDesc {
+    int32_t kind;
+    int32_t material;
+    int32_t flags;
+    int32_t pad;
+    int64_t first;
+    int64_t count;
+    float p[12];
+} RtEntityDesc;
+
+#define RT_LIGHT_AREA        0   /* Lights/AreaLight.cs        */
+#define RT_LIGHT_DIRECTIONAL 1   /* Lights/DirectionalLight.cs */
+
+/* Explicit lights in YAML order. Geometry lights (Lights/GeometryLight.cs) are
+ * derived by the library from emissive, non-proxy entities in entity order and
+ * appended after these, as SceneLoader.ExtractGeometryLights does
+ * (Scene/SceneLoader.cs:516-522). */
+typedef struct RtLightDesc {
+    int32_t type;
+    int32_t shadow_samples;       /* <= 0: the light type's default */
+    int32_t proxy_material;       /* area light: material index of its proxy, or -1 */
+    int32_t pad;
+    float corner[3], u[3], v[3];  /* area light parallelogram */
+    float color[3];
+    float intensity;
+    float soft_radius;
+    float direction[3];           /* directional light travel direction */
+    float angular_radius_deg;     /* directional disc; 0 = delta light */
+} RtLightDesc;
+
+/* Camera/Camera.cs:26-51 (pinhole when aperture == 0). */
+typedef struct RtCameraDesc {
+    float look_from[3], look_at[3], vup[3];
+    float vfov_deg;
+    float aperture;
+    float focus_dist;
+} RtCameraDesc;
+
+/* Global homogeneous medium (Volumetrics/HomogeneousMedium.cs) with a
+ * Henyey-Greenstein phase (Volumetrics/HenyeyGreensteinPhase.cs). */
+typedef struct RtMediumDesc {
+    int32_t enabled;
+    int32_t pad;
+    float sigma_a[3];
+    float sigma_s[3];
+    float g;
+} RtMediumDesc;
+
+typedef struct RtWorldDesc {
+    const RtMaterialDesc* materials;  int32_t num_materials;
+    const RtEntityDesc*   entities;   int32_t num_entities;
+    const float*          tri_verts;  int64_t num_tris;   /* 9 floats: v0, v1, v2 */
+    const RtLightDesc*    lights;     int32_t num_lights;
+    int32_t geometry_light_samples;   /* ShadowSamples of derived geometry lights */
+    RtCameraDesc camera;
+    RtMediumDesc medium;
+} RtWorldDesc;
+
+/* ---- render parameters: the Renderer constructor (Renderer.cs:300-319) --- */
+
+#define RT_MIS_BALANCE 0
+#define RT_MIS_POWER   1
+#define RT_LIGHTS_ALL  0
+
+#define RT_KERNEL_MEGAKERNEL 0   /* one thread per sample, whole path in registers */
+#define RT_KERNEL_WAVEFRONT  1   /* raygen/extend/shade/occlude/resolve queues     */
+
+typedef struct RtRenderParams {
+    int32_t width, height;
+    int32_t spp;
+    int32_t max_depth;
+    int32_t spp_offset;             /* first Sobol sample index (progressive resume) */
+    int32_t rr_min_bounces;         /* < 0: the reference's scene classifier decides */
+    float   rr_min_survival;        /* used only when rr_min_bounces >= 0 */
+    float   max_sample_radiance;    /* <= 0: default 10 (Renderer.cs:202) */
+    float   indirect_clamp_factor;  /* < 0: default 0.25 (Renderer.cs:214) */
+    float   exposure_ev;
+    int32_t mis_heuristic;          /* RT_MIS_* */
+    int32_t light_strategy;         /* RT_LIGHTS_ALL only */
+    int32_t kernel;                 /* RT_KERNEL_* */
+    int32_t block_size;             /* 0: autotuned / default */
+    int32_t wavefront_size;         /* 0: autotuned / default (wavefront only) */
+    int32_t sort_materials;         /* wavefront: sort hits by material */
+    int32_t pixel_x0, pixel_y0;     /* render window (0,0,0,0 = full frame) */
+    int32_t window_w, window_h;
+    int32_t count_work;             /* 1: counting build, fills the work fields of RtStats */
+    int32_t pad;
+} RtRenderParams;
+
+/* Counters and timings of one call. */
+typedef struct RtStats {
+    double   kernel_ms;             /* device time of the render kernels (CUDA events) */
+    double   total_ms;              /* host wall time of the call */
+    uint64_t samples;               /* camera samples traced */
+    uint64_t closest_rays;          /* closest-hit rays */
+    uint64_t shadow_rays;           /* any-hit rays */
+    uint64_t node_visits;           /* BVH node box tests (count_work only) */
+    uint64_t prim_tests;            /* triangle tests (count_work only) */
+    uint64_t other_tests;           /* quad / sphere tests (count_work only) */
+    int32_t  kernel_launches;       /* kernels launched by the call */
+    int32_t  rr_min_bounces;        /* the RR knobs the call used */
+    float    rr_min_survival;
+    int32_t  pad;
+} RtStats;
+
+typedef struct RtScene RtScene;
+
+/* ---- version / errors ---------------------------------------------------- */
+int         rt_abi_version(void);
+const char* rt_last_error(void);
+/* Number of visible CUDA devices; < 0 on error. Loads no kernels. */
+int         rt_device_count(void);
+
+/* ---- scene lifetime ------------------------------------------------------ */
+/* Runs the host-side world assembly (SAH BVH build, flattening into SoA,
+ * geometry-light extraction, Kulla-Conty LUT build) and uploads the result to
+ * the current device. */
+int rt_scene_create(const RtWorldDesc* world, RtScene** out_scene);
+int rt_scene_destroy(RtScene* scene);
+
+/* Scene summary for tests and logs. */
+typedef struct RtSceneInfo {
+    int64_t num_nodes;            /* flattened BVH nodes (top level + all meshes) */
+    int64_t num_tris;
+    int32_t num_entities;
+    int32_t num_lights;           /* explicit + derived geometry lights */
+    int32_t top_is_bvh;           /* 0: the world is a flat list (<= 4 objects) */
+    int32_t max_stack_depth;      /* traversal stack entries the scene needs */
+    int32_t rr_min_bounces;       /* the reference's classifier result */
+    float   rr_min_survival;
+    float   mean_irradiance;      /* classifier input, Renderer.cs:361-372 */
+    int32_t pad;
+    int64_t device_bytes;
+} RtSceneInfo;
+int rt_scene_info(const RtScene* scene, RtSceneInfo* info);
+
+/* Copies the flattened BVH: nodes as 8 x int32 words each (bmin xyz as float
+ * bits, a, bmax xyz as float bits, b), and the item arrays. Any pointer may be
+ * null to skip that array. Used to compare against the oracle's build. */
+int rt_scene_export_bvh(const RtScene* scene, int32_t* nodes, int64_t max_nodes,
+                        int32_t* top_items, int64_t max_top_items,
+                        int32_t* tri_order, int64_t max_tris);
+
+/* Host-only world assembly without a device: runs the same build as
+ * rt_scene_create and returns the summary and the flattened BVH (same export
+ * layout as rt_scene_export_bvh). Lets a host without a GPU inspect the
+ * build; no device memory is touched. */
+int rt_world_inspect(const RtWorldDesc* world, RtSceneInfo* info, int32_t* nodes, int64_t max_nodes,
+                     int32_t* top_items, int64_t max_top_items, int32_t* tri_order, int64_t max_tris);
+
+/* ---- rendering ----------------------------------------------------------- */
+/* Renders into a caller-owned planar fp32 buffer of 3*W*H floats (host memory).
+ * The linear-HDR mean of the clamped per-sample radiance, before exposure. */
+int rt_render(RtScene* scene, const RtRenderParams* params, float* hdr_rgb_planar,
+              RtStats* stats);
+
+/* Same, with the film left in caller-owned DEVICE memory (3*W*H floats); no
+ * host copies. The call still synchronises before returning. */
+int rt_render_device(RtScene* scene, const RtRenderParams* params, float* d_hdr_rgb_planar,
+                     RtStats* stats);
+
+/* One request of a batch. */
+typedef struct RtRequest {
+    int32_t scene;                /* index into the scenes array */
+    int32_t width, height, spp, max_depth;
+    int32_t pad;
+    RtCameraDesc camera;          /* per-request camera (overrides the scene's) */
+} RtRequest;
+
+/* Renders n requests of uneven size in one persistent wavefront launch.
+ * outs[i] is a host buffer of 3*W_i*H_i floats. */
+int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
+                    const RtRequest* requests, int32_t n,
+                    const RtRenderParams* common, float* const* outs, RtStats* stats);
+
+/* ---- differentiation ----------------------------------------------------- */
+/* Parameters the adjoint differentiates, per material (Disney) and per emitter:
+ * base_color[3], roughness, metallic, specular, sheen, clearcoat, spec_trans,
+ * emission[3] — 12 floats per material, in material order. */
+#define RT_ADJ_PARAMS_PER_MATERIAL 12
+int rt_adjoint(RtScene* scene, const RtRenderParams* params,
+               const float* dL_dimage_planar, float* dL_dparams, RtStats* stats);
+/* Overwrites the differentiable parameters of the scene's materials
+ * (same 12-float layout as rt_adjoint's output). */
+int rt_scene_set_params(RtScene* scene, const float* params, int32_t num_materials);
+
+/* ---- test-only entry points --------------------------------------------- */
+/* Ray in: origin[3], dir[3] (8 floats per ray, last two ignored).
+ * Closest hit out per ray: t, u, v as float, entity id, local primitive id
+ * (int32 bits), and a hit flag: 6 words. */
+int rt_trace_closest(RtScene* scene, const float* rays, int64_t n, float tmin, float tmax,
+                     int32_t* hits);
+/* Shadow rays in: origin[3], dir[3], tmin, tmax. Out: transmittance rgb. */
+int rt_trace_any(RtScene* scene, const float* rays, int64_t n, float* transmittance);
+
+/* BSDF batch. Each record (RtBsdfQuery) carries the shading inputs; the
+ * results are the Sample outcome and Evaluate/Pdf/EvaluateDirect values. */
+typedef struct RtBsdfQuery {
+    int32_t material;
+    int32_t front_face;
+    uint32_t pixel_seed, sample_index;   /* Sobol stream for the sample draws */
+    uint32_t dim;                        /* first dimension the sample consumes */
+    int32_t pad;
+    float n[3], tangent[3], bitangent[3];
+    float v[3];                          /* view direction (toward the eye)     */
+    float l[3];                          /* direction for Evaluate/Pdf/Direct   */
+    float point[3];
+} RtBsdfQuery;
+typedef struct RtBsdfResult {
+    float f[3];  float pdf;              /* Evaluate(V, L), Pdf(V, L) */
+    float fd[3]; float pad0;             /* EvaluateDirect(L, V, N)   */
+    float wo[3]; float s_pdf;            /* Sample: direction, pdf    */
+    float s_f[3];
+    int32_t lobe;                        /* 0..6 (Diffuse..Clearcoat), -1 none */
+    int32_t is_delta;
+    int32_t has_sample;
+    uint32_t dims_used;
+    int32_t pad1;
+} RtBsdfResult;
+int rt_bsdf_batch(RtScene* scene, const RtBsdfQuery* q, int64_t n, RtBsdfResult* out);
+
+/* Owen-scrambled Sobol draws: out[i] = Sample(idx[i], dim[i], seed[i]). */
+int rt_sobol_batch(const uint32_t* sample_index, const uint32_t* dim, const uint32_t* pixel_seed,
+                   int64_t n, float* out);
+
+/* Kulla-Conty tables the scene uses: E (32x32, mu-major) then E_avg (32). */
+int rt_energy_lut(float* e_1024, float* eavg_32);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT3D_H */
