@@ -76,14 +76,17 @@ class RtRenderParams(C.Structure):
                 ("exposure_ev", C.c_float), ("mis_heuristic", C.c_int32), ("light_strategy", C.c_int32),
                 ("kernel", C.c_int32), ("block_size", C.c_int32), ("wavefront_size", C.c_int32),
                 ("sort_materials", C.c_int32), ("pixel_x0", C.c_int32), ("pixel_y0", C.c_int32),
-                ("window_w", C.c_int32), ("window_h", C.c_int32), ("count_work", C.c_int32), ("pad", C.c_int32)]
+                ("window_w", C.c_int32), ("window_h", C.c_int32), ("count_work", C.c_int32), ("profile_kernels", C.c_int32)]
 
 
 class RtStats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("samples", C.c_uint64),
                 ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("node_visits", C.c_uint64),
-                ("prim_tests", C.c_uint64), ("other_tests", C.c_uint64), ("kernel_launches", C.c_int32), ("rr_min_bounces", C.c_int32),
-                ("rr_min_survival", C.c_float), ("pad", C.c_int32)]
+                ("prim_tests", C.c_uint64), ("other_tests", C.c_uint64), ("shadow_node_visits", C.c_uint64),
+                ("shadow_prim_tests", C.c_uint64), ("shadow_other_tests", C.c_uint64), ("regen_ms", C.c_double),
+                ("extend_ms", C.c_double), ("shade_ms", C.c_double), ("occlude_ms", C.c_double),
+                ("sort_ms", C.c_double), ("iterations", C.c_int32), ("kernel_launches", C.c_int32),
+                ("rr_min_bounces", C.c_int32), ("rr_min_survival", C.c_float)]
 
 
 class RtSceneInfo(C.Structure):
@@ -205,6 +208,7 @@ def render_params(width, height, spp, max_depth, **kw) -> RtRenderParams:
     p.rr_min_survival = kw.pop("rr_min_survival", 0.0)
     p.max_sample_radiance = kw.pop("max_sample_radiance", 10.0)
     p.indirect_clamp_factor = kw.pop("indirect_clamp_factor", 0.25)
+    p.sort_materials = kw.pop("sort_materials", -1)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -242,12 +246,14 @@ def load(path: str | None = None):
         "rt_render_batch": (C.c_int, [P, C.c_int32, P, C.c_int32, C.POINTER(RtRenderParams), P,
                                       C.POINTER(RtStats)]),
         "rt_adjoint": (C.c_int, [P, C.POINTER(RtRenderParams), P, P, C.POINTER(RtStats)]),
+        "rt_autotune": (C.c_int, [P, C.POINTER(RtRenderParams), C.POINTER(RtRenderParams)]),
         "rt_scene_set_params": (C.c_int, [P, P, C.c_int32]),
         "rt_trace_closest": (C.c_int, [P, P, C.c_int64, C.c_float, C.c_float, P]),
         "rt_trace_any": (C.c_int, [P, P, C.c_int64, P]),
         "rt_bsdf_batch": (C.c_int, [P, P, C.c_int64, P]),
         "rt_sobol_batch": (C.c_int, [P, P, P, C.c_int64, P]),
         "rt_energy_lut": (C.c_int, [P, P]),
+        "rt_tonemap": (C.c_int, [P, C.c_int32, C.c_int32, C.c_float, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

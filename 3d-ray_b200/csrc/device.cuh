@@ -92,9 +92,14 @@ struct Hit {
     int slot;   // stored triangle index, or entity id for quads and spheres
 };
 
-// Work counters of the counting build (algorithmic bytes of the roofline).
+// Work counters of the counting build (algorithmic bytes of the roofline):
+// traversal work of closest-hit rays and of shadow rays kept apart.
+struct TravCounters {
+    uint32_t nodes, tris, others;
+};
 struct Counters {
-    uint32_t nodes, tris, others, closest_rays, shadow_rays;
+    TravCounters closest, shadow;
+    uint32_t closest_rays, shadow_rays;
 };
 
 RT_D V3 ld3(const float4& f) { return v3(f.x, f.y, f.z); }
@@ -186,7 +191,7 @@ RT_D bool entity_test(const SceneView& s, int e, V3 o, V3 d, float tmin, float t
 // root >= 0 restricts the walk to one mesh BVH (a light's own geometry).
 template <bool ANY, int STACK>
 __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
-                                         Counters* cnt, int* err, int root = -1) {
+                                         TravCounters* cnt, int* err, int root = -1) {
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
     int stack[STACK];
     int sp = 0;
@@ -1090,9 +1095,10 @@ template <int STACK>
 __device__ __forceinline__ V3 shadow_transmittance(const SceneView& s, int opaque_scene, V3 o, V3 d, float tmin,
                                                    float tmax, Counters* cnt, int* err) {
     Hit h;
+    TravCounters* tc = cnt ? &cnt->shadow : nullptr;
     if (cnt) cnt->shadow_rays++;
     if (opaque_scene) {
-        traverse<true, STACK>(s, o, d, tmin, tmax, h, cnt, err);
+        traverse<true, STACK>(s, o, d, tmin, tmax, h, tc, err);
         return h.kind == HIT_NONE ? v3(1.0f) : v3(0.0f);
     }
     V3 thr = v3(1.0f);
@@ -1100,7 +1106,7 @@ __device__ __forceinline__ V3 shadow_transmittance(const SceneView& s, int opaqu
     V3 sigma = v3(0.0f), entry = v3(0.0f);
     bool in_med = false;
     for (int i = 0; i < 8; i++) {
-        traverse<false, STACK>(s, o, d, tmin, remaining, h, cnt, err);
+        traverse<false, STACK>(s, o, d, tmin, remaining, h, tc, err);
         if (h.kind == HIT_NONE) return thr;
         Surface rec = make_surface(s, h, o, d);
         const Material& m = s.materials[rec.material];

@@ -75,76 +75,132 @@ RT_D V3 weight_emission(const SceneView& s, const RenderConst& rc, V3 raw, int m
     return raw;
 }
 
-// ComputeDirectLighting, strategy All (Renderer.cs:1894-2036). The BSDF
-// integrand and MIS weight are evaluated before the shadow ray, and the ray is
-// skipped when they are zero: the reference casts it first, which changes
-// nothing but the cost (all draws happen in the light sampler).
-template <int STACK>
-__device__ __forceinline__ V3 direct_lighting(const SceneView& s, const RenderConst& rc, const Surface& rec,
-                                              const Material& m, V3 view, Sampler& rng, Counters* cnt, int* err) {
-    V3 result = v3(0.0f);
+// Path state carried from vertex to vertex. The megakernel keeps it in
+// registers; the wavefront stores it in SoA arrays between kernels.
+struct PathState {
+    V3 o, d;          // current ray
+    V3 beta;          // path throughput used by RR and the dead-path test
+    V3 w;             // weight of the next vertex's terms (segment factors x attenuations)
+    V3 lp, la;        // first-vertex terms; deeper terms relative to att0
+    V3 pre, att0;     // first-vertex weight and attenuation (primary clamp)
+    V3 cur_abs;       // interior Beer-Lambert sigma_a of the current segment
+    V3 mask;          // channels still live in la (per-frame sanitize)
+    float prev_pdf;
+    int prev_delta;
+    int first;        // no scattering vertex yet
+    int clamp_mode;   // the first vertex was a surface
+    int depth;        // TraceRay depth of the next segment
+    Sampler rng;
+    IorStackD iors;
+
+    // Adds a term of the current vertex (already weighted) to lp or la.
+    RT_D void add(V3 x, int to_la) {
+        if (!to_la) {
+            lp = lp + x;
+            return;
+        }
+        if (!isfinite(x.x)) mask.x = 0.0f;
+        if (!isfinite(x.y)) mask.y = 0.0f;
+        if (!isfinite(x.z)) mask.z = 0.0f;
+        la = la + v3(mask.x != 0.0f ? x.x : 0.0f, mask.y != 0.0f ? x.y : 0.0f, mask.z != 0.0f ? x.z : 0.0f);
+    }
+};
+
+// Camera sample setup (Renderer.cs:615-653): pixel seed, 2 jitter draws,
+// pinhole ray (Camera.cs:127-139).
+RT_D void path_init(PathState& ps, const RenderConst& rc, int px, int py, uint32_t sample_index) {
+    uint32_t seed = ((uint32_t)px * 73856093u) ^ ((uint32_t)py * 19349663u);
+    ps.rng = Sampler{seed, sample_index, 0u};
+    float ju = ps.rng.next();
+    float jv = ps.rng.next();
+    float u = ((float)px + ju) / (float)rc.width;
+    float v = ((float)(rc.height - py - 1) + jv) / (float)rc.height;
+    V3 target = rc.cam.llc + u * rc.cam.horizontal + v * rc.cam.vertical;
+    ps.o = rc.cam.origin;
+    ps.d = target - rc.cam.origin;
+    ps.beta = v3(1.0f);
+    ps.w = v3(1.0f);
+    ps.lp = v3(0.0f);
+    ps.la = v3(0.0f);
+    ps.pre = v3(1.0f);
+    ps.att0 = v3(0.0f);
+    ps.cur_abs = v3(0.0f);
+    ps.mask = v3(1.0f);
+    ps.prev_pdf = 0.0f;
+    ps.prev_delta = 1;
+    ps.first = 1;
+    ps.clamp_mode = 0;
+    ps.depth = rc.max_depth;
+    ps.iors.n = 0;
+}
+
+// Entry test of TraceRay (Renderer.cs:1589-1603): depth and dead path.
+RT_D bool path_alive(const PathState& ps) { return ps.depth > 0 && max3(ps.beta) >= 1e-4f; }
+
+// The clamped sample radiance (ClampRadianceIndirect at the primary surface,
+// then ClampRadiance; Renderer.cs:670, 1380-1381).
+RT_D V3 path_resolve(const PathState& ps, const RenderConst& rc) {
+    V3 L = ps.lp;
+    if (ps.clamp_mode) L = L + ps.pre * clamp_lum(ps.att0 * sanitize(ps.la), rc.ind_max);
+    return clamp_lum(L, rc.max_rad);
+}
+
+// NEE at a surface vertex: ComputeDirectLighting, strategy All
+// (Renderer.cs:1894-2036). The BSDF integrand and the MIS weight are evaluated
+// before the shadow ray and the ray is dropped when they are zero (the
+// reference casts it first; only the cost differs: every draw happens in the
+// light sampler). Each unoccluded sample adds w * colour * brdf * Tr_medium,
+// times the vertex weight, through the sink.
+template <class Sink>
+RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, const Surface& rec,
+                      const Material& m, V3 view, Sink& sink) {
     float view_term = shadow_terminator(rec.n, rec.n, view);
+    int to_la = ps.clamp_mode;
     for (int li = 0; li < s.num_lights; li++) {
         const Light& l = s.lights[li];
-        V3 acc = v3(0.0f);
         for (int si = 0; si < l.shadow_samples; si++) {
-            LightSample ls = light_sample(s, l, rec.p, rec.n, si, rng);
-            if (ls.occluded) continue;
+            LightSample ls = light_sample(s, l, rec.p, rec.n, si, ps.rng);
+            if (ls.occluded || !ls.has_ray) continue;
             V3 brdf = bsdf_eval_direct(s, m, rec, ls.dir, view, rec.n);
             brdf = brdf * (view_term * shadow_terminator(rec.n, rec.n, ls.dir));
             if (is_zero(brdf)) continue;
-            V3 color = ls.color;
-            if (ls.has_ray) {
-                V3 tr = shadow_transmittance<STACK>(s, rc.opaque, ls.ray_o, ls.dir, kEps, ls.ray_tmax, cnt, err);
-                if (near_zero(tr)) continue;
-                color = color * tr;
-            }
             V3 tr_m = v3(1.0f);
             if (s.has_medium) tr_m = medium_tr(s, ls.dist >= kInf ? 1e30f : ls.dist);
-            float w = 1.0f;
+            float wgt = 1.0f;
             if (!l.is_delta) {
                 float pb = bsdf_pdf(m, rec, view, ls.dir);
                 if (pb > 0.0f) {
                     float pl = light_pdf(s, l, rec.p, ls.dir);
-                    w = (pl + pb > 0.0f) ? mis_weight(pl, pb, rc.mis_power) : 1.0f;
+                    wgt = (pl + pb > 0.0f) ? mis_weight(pl, pb, rc.mis_power) : 1.0f;
                 }
             }
-            acc = acc + w * color * brdf * tr_m;
+            V3 c = ps.w * (wgt * ls.color * brdf * tr_m);
+            sink.shadow(ps, ls.ray_o, ls.dir, ls.ray_tmax, c, to_la);
         }
-        result = result + acc;
     }
-    return result;
 }
 
-// ComputeDirectLightingMedium, strategy All (Renderer.cs:2162-2203)
-template <int STACK>
-__device__ __forceinline__ V3 direct_lighting_medium(const SceneView& s, const RenderConst& rc, V3 p, V3 wo,
-                                                     Sampler& rng, Counters* cnt, int* err) {
-    V3 result = v3(0.0f);
+// NEE at a medium scattering point: ComputeDirectLightingMedium, strategy All
+// (Renderer.cs:2162-2203).
+template <class Sink>
+RT_D void nee_medium(const SceneView& s, const RenderConst& rc, PathState& ps, V3 p, V3 wo, Sink& sink) {
+    int to_la = ps.clamp_mode;
     for (int li = 0; li < s.num_lights; li++) {
         const Light& l = s.lights[li];
-        V3 acc = v3(0.0f);
         for (int si = 0; si < l.shadow_samples; si++) {
-            LightSample ls = light_sample(s, l, p, v3(0.0f), si, rng);
-            if (ls.occluded) continue;
-            V3 color = ls.color;
-            if (ls.has_ray) {
-                V3 tr = shadow_transmittance<STACK>(s, rc.opaque, ls.ray_o, ls.dir, kEps, ls.ray_tmax, cnt, err);
-                if (near_zero(tr)) continue;
-                color = color * tr;
-            }
+            LightSample ls = light_sample(s, l, p, v3(0.0f), si, ps.rng);
+            if (ls.occluded || !ls.has_ray) continue;
             float ph = hg_eval(s.hg_g, wo, ls.dir);
             V3 tr_m = medium_tr(s, ls.dist >= kInf ? 1e30f : ls.dist);
-            float w = 1.0f;
+            float wgt = 1.0f;
             if (!l.is_delta && ph > 0.0f) {
                 float pl = light_pdf(s, l, p, ls.dir);
-                if (pl + ph > 0.0f) w = mis_weight(pl, ph, rc.mis_power);
+                if (pl + ph > 0.0f) wgt = mis_weight(pl, ph, rc.mis_power);
             }
-            acc = acc + w * color * ph * tr_m;
+            V3 c = ps.w * (wgt * ls.color * ph * tr_m);
+            sink.shadow(ps, ls.ray_o, ls.dir, ls.ray_tmax, c, to_la);
         }
-        result = result + acc;
     }
-    return result;
 }
 
 // Russian roulette on the projected throughput (Renderer.cs:1283-1294).
@@ -162,168 +218,154 @@ RT_D bool russian_roulette(const RenderConst& rc, int depth, V3& att, V3& next_b
     return true;
 }
 
-struct Accum {
-    V3 lp, la;       // first-vertex terms; deeper terms (relative to att0)
-    V3 mask;         // channels still live in la (per-frame sanitize)
-    int after;       // 1 once the first vertex has scattered
-    RT_D void add(V3 x) {
-        if (!after) {
-            lp = lp + x;
-            return;
+RT_D V3 bl_factor(V3 sigma, float t) { return beer_lambert(v3(1.0f), sigma, t); }
+
+// One vertex of TraceRay given the closest hit of the current ray: the
+// volumetric branch (Renderer.cs:1704-1782), ShadeSurface (:1008-1228) and
+// ShadeSampleBounce (:1235-1383). Returns true when the path continues with
+// ps.o/ps.d as the next ray (ps.depth already decremented).
+template <class Sink>
+__device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderConst& rc, PathState& ps, const Hit& h,
+                                             Sink& sink) {
+    bool hit = h.kind != HIT_NONE;
+    V3 beta_s = ps.beta;
+    if (s.has_medium) {
+        float tmax = hit ? h.t : 1e30f;
+        float tmed;
+        V3 mb;
+        bool sc = medium_sample(s, tmax, ps.rng, tmed, mb);
+        if (sc) {
+            V3 p = ps.o + ps.d * tmed;
+            ps.w = ps.w * bl_factor(ps.cur_abs, tmed) * mb;
+            nee_medium(s, rc, ps, p, ps.d, sink);
+            V3 mthr = ps.beta * mb;
+            int used = rc.max_depth - ps.depth;
+            float scale = 1.0f;
+            if (used >= rc.rr_min_bounces) {
+                float q = fmaxf(mthr.x, fmaxf(mthr.y, mthr.z));
+                q = fmaxf(q, rc.rr_min_survival);
+                q = fminf(q, 0.95f);
+                if (ps.rng.next() > q) return false;
+                scale = 1.0f / q;
+            }
+            float ppdf;
+            V3 wi = hg_sample(s.hg_g, ps.d, ps.rng, ppdf);
+            float pv = hg_eval(s.hg_g, ps.d, wi);
+            float pw = ppdf > 1e-20f ? pv / ppdf : 0.0f;
+            ps.beta = mthr * (pw * scale);
+            ps.w = ps.w * (pw * scale);
+            ps.o = p;
+            ps.d = wi;
+            ps.prev_pdf = ppdf;
+            ps.prev_delta = 0;
+            ps.first = 0;   // a medium first vertex: no primary clamp
+            ps.depth -= 1;
+            return path_alive(ps);
         }
-        if (!isfinite(x.x)) mask.x = 0.0f;
-        if (!isfinite(x.y)) mask.y = 0.0f;
-        if (!isfinite(x.z)) mask.z = 0.0f;
-        la = la + v3(mask.x != 0.0f ? x.x : 0.0f, mask.y != 0.0f ? x.y : 0.0f, mask.z != 0.0f ? x.z : 0.0f);
+        ps.w = ps.w * mb;
+        beta_s = ps.beta * mb;
+    }
+    if (!hit) return false;   // black flat sky: SampleSky returns 0
+    ps.w = ps.w * bl_factor(ps.cur_abs, h.t);
+    Surface rec = make_surface(s, h, ps.o, ps.d);
+    const Material& m = s.materials[rec.material];
+    int to_la = ps.clamp_mode;
+    if (m.type != 0) {   // Emissive: Emit (front face only), no NEE, no scatter
+        if (rec.front && (m.emission.x > 0.0f || m.emission.y > 0.0f || m.emission.z > 0.0f))
+            ps.add(ps.w * weight_emission(s, rc, m.emission, rec.material, ps.o, ps.d, ps.prev_pdf, ps.prev_delta),
+                   to_la);
+        return false;
+    }
+    V3 view = normalize(-ps.d);
+    float rel_eta = 0.0f;
+    bool dielectric = !m.thin_walled && m.spec_trans_raw > 0.0f;
+    if (dielectric) rel_eta = rec.front ? (ps.iors.top() / m.ior_raw) : (m.ior_raw / ps.iors.enclosing());
+    nee_surface(s, rc, ps, rec, m, view, sink);
+    BsdfSample bs;
+    V3 att, next_o, next_d, next_beta;
+    float next_pdf;
+    int next_delta;
+    if (bsdf_sample(s, m, rec, view, rel_eta, ps.rng, bs)) {   // ShadeSampleBounce
+        if (bs.is_delta) {
+            att = bs.f;
+        } else {
+            float a = fabsf(dot(rec.n, bs.wo));
+            if (a <= 0.0f || bs.pdf <= 0.0f) return false;
+            att = bs.f * a / bs.pdf;
+        }
+        next_beta = beta_s * att;
+        if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
+        V3 off = dot(bs.wo, rec.n) >= 0.0f ? rec.n : -rec.n;
+        next_o = offset_origin(rec.p, off);
+        next_d = bs.wo;
+        next_pdf = bs.is_delta ? 0.0f : bs.pdf;
+        next_delta = bs.is_delta;
+        if (bs.has_next_absorption) ps.cur_abs = bs.next_absorption;
+        if (rc.dielectrics && bs.transition == 1) ps.iors.push(dielectric ? m.ior_raw : ps.iors.top());
+        if (rc.dielectrics && bs.transition == 2) ps.iors.pop();
+    } else {   // Sample returned null: the legacy Scatter path (:1127-1225)
+        V3 sdir;
+        int lobe;
+        if (!bsdf_scatter(s, m, rec, ps.d, rel_eta, ps.rng, att, sdir, lobe)) return false;
+        next_beta = beta_s * att;
+        if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
+        next_o = rec.p;
+        next_d = sdir;
+        next_pdf = 0.0f;
+        next_delta = 0;
+        if (rc.dielectrics && dielectric && dot(sdir, rec.n) < 0.0f) {
+            if (rec.front) ps.iors.push(m.ior_raw);
+            else ps.iors.pop();
+        }
+    }
+    if (ps.first) {   // primary surface: deeper terms are clamped as one (:1380-1381)
+        ps.first = 0;
+        ps.clamp_mode = 1;
+        ps.pre = ps.w;
+        ps.att0 = att;
+        ps.w = v3(1.0f);
+    } else {
+        ps.w = ps.w * att;
+    }
+    ps.beta = next_beta;
+    ps.o = next_o;
+    ps.d = next_d;
+    ps.prev_pdf = next_pdf;
+    ps.prev_delta = next_delta;
+    ps.depth -= 1;
+    return path_alive(ps);
+}
+
+// Shadow sink of the megakernel: traces the shadow ray at once.
+template <int STACK>
+struct InlineShadows {
+    const SceneView* s;
+    int opaque;
+    Counters* cnt;
+    int* err;
+    RT_D void shadow(PathState& ps, V3 o, V3 d, float tmax, V3 c, int to_la) {
+        V3 tr = shadow_transmittance<STACK>(*s, opaque, o, d, kEps, tmax, cnt, err);
+        if (near_zero(tr)) return;
+        ps.add(c * tr, to_la);
     }
 };
 
-RT_D V3 bl_factor(V3 sigma, float t) { return beer_lambert(v3(1.0f), sigma, t); }
-
-// Traces one camera sample of pixel (px, py) and returns the clamped sample
-// radiance (ClampRadiance applied, Renderer.cs:670). cnt (counting builds
-// only) accumulates the traversal work.
+// Traces one camera sample of pixel (px, py) to the end and returns the
+// clamped sample radiance. cnt (counting builds only) accumulates the work.
 template <int STACK, bool COUNT>
 __device__ V3 trace_sample(const SceneView& s, const RenderConst& rc, int px, int py, uint32_t sample_index,
                            Counters* cnt, int* err) {
     if (!COUNT) cnt = nullptr;
-    uint32_t seed = ((uint32_t)px * 73856093u) ^ ((uint32_t)py * 19349663u);   // Renderer.cs:615
-    Sampler rng{seed, sample_index, 0u};
-    float ju = rng.next();
-    float jv = rng.next();
-    float u = ((float)px + ju) / (float)rc.width;
-    float v = ((float)(rc.height - py - 1) + jv) / (float)rc.height;
-    V3 target = rc.cam.llc + u * rc.cam.horizontal + v * rc.cam.vertical;   // Camera.cs:127-139
-    V3 o = rc.cam.origin;
-    V3 d = target - rc.cam.origin;
-    V3 beta = v3(1.0f);
-    float prev_pdf = 0.0f;
-    int prev_delta = 1;
-    V3 cur_abs = v3(0.0f);
-    IorStackD iors;
-    iors.n = 0;
-    Accum acc{v3(0.0f), v3(0.0f), v3(1.0f), 0};
-    V3 W = v3(1.0f), pre = v3(1.0f), att0 = v3(0.0f);
-    int clamp_mode = 0;
-    int first = 1;
-    for (int depth = rc.max_depth; depth > 0; --depth) {
-        if (max3(beta) < 1e-4f) break;   // dead path (Renderer.cs:1600-1603)
+    PathState ps;
+    path_init(ps, rc, px, py, sample_index);
+    InlineShadows<STACK> sink{&s, rc.opaque, cnt, err};
+    while (path_alive(ps)) {
         Hit h;
         if (COUNT) cnt->closest_rays++;
-        traverse<false, STACK>(s, o, d, kEps, kInf, h, cnt, err);
-        bool hit = h.kind != HIT_NONE;
-        V3 beta_s = beta;
-        if (s.has_medium) {   // volumetric branch (Renderer.cs:1704-1782)
-            float tmax = hit ? h.t : 1e30f;
-            float tmed;
-            V3 mb;
-            bool sc = medium_sample(s, tmax, rng, tmed, mb);
-            if (sc) {
-                V3 p = o + d * tmed;
-                W = W * bl_factor(cur_abs, tmed) * mb;
-                V3 lnee = direct_lighting_medium<STACK>(s, rc, p, d, rng, cnt, err);
-                acc.add(W * lnee);
-                V3 mthr = beta * mb;
-                int used = rc.max_depth - depth;
-                float scale = 1.0f;
-                if (used >= rc.rr_min_bounces) {
-                    float q = fmaxf(mthr.x, fmaxf(mthr.y, mthr.z));
-                    q = fmaxf(q, rc.rr_min_survival);
-                    q = fminf(q, 0.95f);
-                    if (rng.next() > q) break;
-                    scale = 1.0f / q;
-                }
-                float ppdf;
-                V3 wi = hg_sample(s.hg_g, d, rng, ppdf);
-                float pv = hg_eval(s.hg_g, d, wi);
-                float pw = ppdf > 1e-20f ? pv / ppdf : 0.0f;
-                beta = mthr * (pw * scale);
-                W = W * (pw * scale);
-                o = p;
-                d = wi;
-                prev_pdf = ppdf;
-                prev_delta = 0;
-                if (first) {
-                    first = 0;
-                    acc.after = 0;   // a medium first vertex: no primary clamp, keep summing into lp
-                }
-                continue;
-            }
-            W = W * mb;
-            beta_s = beta * mb;
-        }
-        if (!hit) break;   // black flat sky: SampleSky returns 0
-        W = W * bl_factor(cur_abs, h.t);
-        Surface rec = make_surface(s, h, o, d);
-        const Material& m = s.materials[rec.material];
-        if (m.type != 0) {   // Emissive: Emit (front face only), no NEE, no scatter
-            if (rec.front && (m.emission.x > 0.0f || m.emission.y > 0.0f || m.emission.z > 0.0f))
-                acc.add(W * weight_emission(s, rc, m.emission, rec.material, o, d, prev_pdf, prev_delta));
-            break;
-        }
-        V3 view = normalize(-d);
-        float rel_eta = 0.0f;
-        bool dielectric = !m.thin_walled && m.spec_trans_raw > 0.0f;
-        if (dielectric) rel_eta = rec.front ? (iors.top() / m.ior_raw) : (m.ior_raw / iors.enclosing());
-        V3 direct = direct_lighting<STACK>(s, rc, rec, m, view, rng, cnt, err);
-        acc.add(W * direct);
-        BsdfSample bs;
-        V3 att, next_o, next_d;
-        float next_pdf;
-        int next_delta;
-        V3 next_beta;
-        if (bsdf_sample(s, m, rec, view, rel_eta, rng, bs)) {   // ShadeSampleBounce (:1235-1383)
-            if (bs.is_delta) {
-                att = bs.f;
-            } else {
-                float a = fabsf(dot(rec.n, bs.wo));
-                if (a <= 0.0f || bs.pdf <= 0.0f) break;
-                att = bs.f * a / bs.pdf;
-            }
-            next_beta = beta_s * att;
-            if (!russian_roulette(rc, depth, att, next_beta, rng)) break;
-            V3 off = dot(bs.wo, rec.n) >= 0.0f ? rec.n : -rec.n;
-            next_o = offset_origin(rec.p, off);
-            next_d = bs.wo;
-            next_pdf = bs.is_delta ? 0.0f : bs.pdf;
-            next_delta = bs.is_delta;
-            if (bs.has_next_absorption) cur_abs = bs.next_absorption;
-            if (rc.dielectrics && bs.transition == 1) iors.push(dielectric ? m.ior_raw : iors.top());
-            if (rc.dielectrics && bs.transition == 2) iors.pop();
-        } else {   // Sample returned null: the legacy Scatter path (:1127-1225)
-            V3 sdir;
-            int lobe;
-            if (!bsdf_scatter(s, m, rec, d, rel_eta, rng, att, sdir, lobe)) break;
-            next_beta = beta_s * att;
-            if (!russian_roulette(rc, depth, att, next_beta, rng)) break;
-            next_o = rec.p;
-            next_d = sdir;
-            next_pdf = 0.0f;
-            next_delta = 0;
-            if (rc.dielectrics && dielectric && dot(sdir, rec.n) < 0.0f) {
-                if (rec.front) iors.push(m.ior_raw);
-                else iors.pop();
-            }
-        }
-        if (first) {   // primary surface: later terms are clamped as one (:1380-1381)
-            first = 0;
-            clamp_mode = 1;
-            pre = W;
-            att0 = att;
-            W = v3(1.0f);
-            acc.after = 1;
-        } else {
-            W = W * att;
-        }
-        beta = next_beta;
-        o = next_o;
-        d = next_d;
-        prev_pdf = next_pdf;
-        prev_delta = next_delta;
+        traverse<false, STACK>(s, ps.o, ps.d, kEps, kInf, h, COUNT ? &cnt->closest : nullptr, err);
+        if (!shade_vertex(s, rc, ps, h, sink)) break;
     }
-    V3 L = acc.lp;
-    if (clamp_mode) L = L + pre * clamp_lum(att0 * sanitize(acc.la), rc.ind_max);
-    return clamp_lum(L, rc.max_rad);
+    return path_resolve(ps, rc);
 }
 
 }  // namespace rt

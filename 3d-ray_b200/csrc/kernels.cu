@@ -10,6 +10,7 @@
 
 #include "../../include/rt3d.h"
 #include "integrator.cuh"
+#include "wavefront.cuh"
 #include "world.h"
 
 using rt::V3;
@@ -28,6 +29,18 @@ int fail(int code, const std::string& msg) {
         cudaError_t e_ = (x);                                                                  \
         if (e_ != cudaSuccess) return fail(RT_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
     } while (0)
+
+static_assert(sizeof(RtMaterialDesc) == 120, "ABI layout");
+static_assert(sizeof(RtEntityDesc) == 80, "ABI layout");
+static_assert(sizeof(RtLightDesc) == 88, "ABI layout");
+static_assert(sizeof(RtCameraDesc) == 48, "ABI layout");
+static_assert(sizeof(RtMediumDesc) == 36, "ABI layout");
+static_assert(sizeof(RtRenderParams) == 88, "ABI layout");
+static_assert(sizeof(RtStats) == 144, "ABI layout");
+static_assert(sizeof(RtBsdfQuery) == 96, "ABI layout");
+static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
+static_assert(sizeof(RtRequest) == 72, "ABI layout");
+static_assert(sizeof(RtSceneInfo) == 56, "ABI layout");
 
 constexpr int kStack = 64;       // traversal stack entries per thread
 constexpr int kBlock = 128;      // 16 x 8 pixel tiles
@@ -48,6 +61,8 @@ struct RtScene {
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     int* d_err = nullptr;
+    int tuned = 0;                 // rt_autotune ran: use the fields below
+    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0;
 };
 
 namespace {
@@ -95,15 +110,18 @@ __global__ void __launch_bounds__(kBlock) k_render_mega(rt::SceneView s, rt::Ren
     int sb = chunk * per_chunk;
     int se = min(sb + per_chunk, spp);
     V3 sum = rt::v3(0.0f);
-    rt::Counters cnt{0u, 0u, 0u, 0u, 0u};
+    rt::Counters cnt{{0u, 0u, 0u}, {0u, 0u, 0u}, 0u, 0u};
     for (int si = sb; si < se; si++)
         sum = sum + rt::trace_sample<STACK, COUNT>(s, rc, x0 + lx, y0 + ly, (uint32_t)(spp0 + si), &cnt, err);
     if (COUNT) {
-        atomicAdd(work + 0, (unsigned long long)cnt.nodes);
-        atomicAdd(work + 1, (unsigned long long)cnt.tris);
-        atomicAdd(work + 2, (unsigned long long)cnt.others);
+        atomicAdd(work + 0, (unsigned long long)cnt.closest.nodes);
+        atomicAdd(work + 1, (unsigned long long)cnt.closest.tris);
+        atomicAdd(work + 2, (unsigned long long)cnt.closest.others);
         atomicAdd(work + 3, (unsigned long long)cnt.closest_rays);
         atomicAdd(work + 4, (unsigned long long)cnt.shadow_rays);
+        atomicAdd(work + 5, (unsigned long long)cnt.shadow.nodes);
+        atomicAdd(work + 6, (unsigned long long)cnt.shadow.tris);
+        atomicAdd(work + 7, (unsigned long long)cnt.shadow.others);
     }
     size_t plane = (size_t)ww * wh;
     float* out = partial + (size_t)chunk * 3 * plane + (size_t)ly * ww + lx;
@@ -206,6 +224,20 @@ __global__ void k_bsdf(rt::SceneView s, const RtBsdfQuery* q, int64_t n, RtBsdfR
     out[i] = r;
 }
 
+// AcesToneMap (Renderer.cs:893-907) after the exposure gain, planar HDR in,
+// interleaved display RGB out.
+__global__ void k_tonemap(const float* hdr, int npix, float scale, float* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    for (int c = 0; c < 3; c++) {
+        float x = fmaxf(hdr[(size_t)c * npix + i] * scale, 0.0f);
+        float a = x * (2.51f * x + 0.03f);
+        float b = x * (2.43f * x + 0.59f) + 0.14f;
+        float m = rt::clampf(a / b, 0.0f, 1.0f);
+        out[(size_t)i * 3 + c] = powf(m, 1.0f / 2.2f);
+    }
+}
+
 __global__ void k_sobol(const uint32_t* idx, const uint32_t* dim, const uint32_t* seed, int64_t n, float* out) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -255,11 +287,14 @@ rt::RenderConst make_rc(const RtScene* sc, const RtRenderParams* p, const RtCame
 }
 
 // Renders into a device film (3*W*H, planar). Caller holds sc->mu.
+int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam, float* d_film, RtStats* st);
+
 int render_to_device(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam, float* d_film, RtStats* st) {
     auto t0 = std::chrono::steady_clock::now();
     int rc_ = validate_params(sc, p);
     if (rc_ != RT_OK) return rc_;
     CUDA_TRY(cudaSetDevice(sc->device));
+    if (p->kernel == RT_KERNEL_WAVEFRONT && !p->count_work) return wf_render_one(sc, p, cam, d_film, st);
     rt::RenderConst rc = make_rc(sc, p, cam);
     int ww = p->window_w > 0 ? p->window_w : p->width;
     int wh = p->window_h > 0 ? p->window_h : p->height;
@@ -311,10 +346,358 @@ int render_to_device(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& c
             st->other_tests = w[2];
             st->closest_rays = w[3];
             st->shadow_rays = w[4];
+            st->shadow_node_visits = w[5];
+            st->shadow_prim_tests = w[6];
+            st->shadow_other_tests = w[7];
         }
         st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     return RT_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Wavefront host driver
+// ---------------------------------------------------------------------------
+struct HostReq {
+    RtScene* scene;
+    rt::RenderConst rc;
+    int x0, y0, ww, wh, spp, spp0;
+    int W, H;
+    float* d_film;
+};
+
+struct WfWorkspace {
+    void* mem = nullptr;
+    size_t bytes = 0;
+    unsigned long long* pinned = nullptr;   // live / next / overflow read-back
+};
+std::mutex g_wf_mu;
+WfWorkspace g_wf_ws[16];
+
+struct Carve {
+    char* base;
+    size_t off = 0;
+    template <typename T>
+    T* take(size_t n) {
+        off = (off + 255) & ~(size_t)255;
+        T* p = reinterpret_cast<T*>(base + off);
+        off += n * sizeof(T);
+        return p;
+    }
+};
+
+// Autotuned (wavefront size, block size, sort) per scene set, kept for the
+// process lifetime; filled by rt_autotune or the defaults below.
+struct WfConfig {
+    int slots = 1 << 22;
+    int block = 256;
+    int sort = 1;
+    int profile = 0;   // per-kernel events instead of the graph
+};
+
+int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (reqs.empty()) return RT_OK;
+    std::lock_guard<std::mutex> lk(g_wf_mu);
+    RtScene* s0 = reqs[0].scene;
+    int dev = s0->device;
+    CUDA_TRY(cudaSetDevice(dev));
+    if (dev < 0 || dev >= 16) return fail(RT_ERR_INVALID_ARG, "device index out of range");
+    cudaStream_t stream = s0->stream;
+    // Distinct scenes of the batch, material key bases, limits.
+    std::vector<RtScene*> scenes;
+    std::vector<int> req_scene(reqs.size());
+    for (size_t r = 0; r < reqs.size(); r++) {
+        auto it = std::find(scenes.begin(), scenes.end(), reqs[r].scene);
+        if (it == scenes.end()) {
+            scenes.push_back(reqs[r].scene);
+            req_scene[r] = (int)scenes.size() - 1;
+        } else {
+            req_scene[r] = (int)(it - scenes.begin());
+        }
+        if (reqs[r].scene->device != dev) return fail(RT_ERR_INVALID_ARG, "batch scenes live on different devices");
+        if (reqs[r].scene->host.max_stack > kStack) return fail(RT_ERR_STACK, "scene stack bound exceeded");
+    }
+    std::vector<rt::SceneView> views;
+    std::vector<int> key_base;
+    int nkeys = 0, max_shadow = 1, opaque = 1, dielectrics = 0;
+    for (RtScene* sc : scenes) {
+        views.push_back(sc->view);
+        key_base.push_back(nkeys);
+        nkeys += (int)sc->host.materials.size();
+        int sh = 0;
+        for (const rt::Light& l : sc->host.lights) sh += l.shadow_samples;
+        max_shadow = std::max(max_shadow, sh);
+        opaque &= sc->opaque;
+        dielectrics |= sc->dielectrics;
+    }
+    int sort = cfg.sort && nkeys < 255;
+    int64_t total = 0;
+    std::vector<rt::WfRequest> wreq(reqs.size());
+    for (size_t r = 0; r < reqs.size(); r++) {
+        rt::WfRequest& q = wreq[r];
+        q.rc = reqs[r].rc;
+        q.rc.opaque = opaque;
+        q.rc.dielectrics = dielectrics;
+        q.scene = req_scene[r];
+        q.x0 = reqs[r].x0;
+        q.y0 = reqs[r].y0;
+        q.ww = reqs[r].ww;
+        q.wh = reqs[r].wh;
+        q.spp = reqs[r].spp;
+        q.spp0 = reqs[r].spp0;
+        q.begin = total;
+        q.count = (long long)q.ww * q.wh * q.spp;
+        total += q.count;
+        if (q.ww >= 65536 || q.wh >= 32768) return fail(RT_ERR_INVALID_ARG, "render window too large");
+    }
+    int nslots = (int)std::max<int64_t>(1024, std::min<int64_t>(cfg.slots, total));
+    nslots = (nslots + 255) / 256 * 256;
+    int64_t cap = (int64_t)nslots * max_shadow;
+    if (cap >= ((int64_t)1 << 31) || nslots >= (1 << 29)) return fail(RT_ERR_INVALID_ARG, "wavefront too large");
+    // Workspace layout.
+    size_t need = 0;
+    auto add = [&](size_t b) { need = ((need + 255) & ~(size_t)255) + b; };
+    add(views.size() * sizeof(rt::SceneView));
+    add(wreq.size() * sizeof(rt::WfRequest));
+    add(key_base.size() * sizeof(int));
+    add(sizeof(rt::WfCtl));
+    for (int k = 0; k < 9; k++) add((size_t)nslots * sizeof(float4));
+    add((size_t)nslots * sizeof(int));
+    add((size_t)nslots * sizeof(int));
+    if (dielectrics) {
+        add((size_t)nslots * sizeof(float4));
+        add((size_t)nslots * 8 * sizeof(float));
+    }
+    for (int k = 0; k < 3; k++) add((size_t)cap * sizeof(float4));
+    add(sizeof(int));
+    for (auto& q : wreq) add((size_t)3 * q.ww * q.wh * sizeof(float));
+    add(reqs.size() * sizeof(float*));
+    add(reqs.size() * sizeof(int) * 2);
+    need += 1024;
+    WfWorkspace& ws = g_wf_ws[dev];
+    if (ws.bytes < need) {
+        if (ws.mem) cudaFree(ws.mem);
+        ws.mem = nullptr;
+        ws.bytes = 0;
+        if (cudaMalloc(&ws.mem, need) != cudaSuccess) return fail(RT_ERR_OOM, "wavefront workspace allocation failed");
+        ws.bytes = need;
+    }
+    if (!ws.pinned && cudaMallocHost(&ws.pinned, 4 * sizeof(unsigned long long)) != cudaSuccess)
+        return fail(RT_ERR_OOM, "pinned read-back allocation failed");
+    Carve cv{static_cast<char*>(ws.mem)};
+    rt::WfArgs a{};
+    auto* d_views = cv.take<rt::SceneView>(views.size());
+    auto* d_reqs = cv.take<rt::WfRequest>(wreq.size());
+    auto* d_kb = cv.take<int>(key_base.size());
+    auto* d_ctl = cv.take<rt::WfCtl>(1);
+    a.P.o = cv.take<float4>(nslots);
+    a.P.d = cv.take<float4>(nslots);
+    a.P.beta = cv.take<float4>(nslots);
+    a.P.w = cv.take<float4>(nslots);
+    a.P.lp = cv.take<float4>(nslots);
+    a.P.la = cv.take<float4>(nslots);
+    a.P.pre = cv.take<float4>(nslots);
+    a.P.att0 = cv.take<float4>(nslots);
+    a.P.hit = cv.take<float4>(nslots);
+    a.P.order = cv.take<int>(nslots);
+    a.P.keys = cv.take<int>(nslots);
+    if (dielectrics) {
+        a.P.ab = cv.take<float4>(nslots);
+        a.P.ior = cv.take<float>((size_t)nslots * 8);
+    }
+    a.S.o = cv.take<float4>(cap);
+    a.S.d = cv.take<float4>(cap);
+    a.S.c = cv.take<float4>(cap);
+    a.S.count = cv.take<int>(1);
+    a.S.capacity = (int)cap;
+    std::vector<float*> films(reqs.size());
+    std::vector<int> fdims(2 * reqs.size());
+    for (size_t r = 0; r < reqs.size(); r++) {
+        wreq[r].accum = cv.take<float>((size_t)3 * wreq[r].ww * wreq[r].wh);
+        films[r] = reqs[r].d_film;
+        fdims[r] = reqs[r].W;
+        fdims[reqs.size() + r] = reqs[r].H;
+    }
+    auto* d_films = cv.take<float*>(reqs.size());
+    auto* d_fdims = cv.take<int>(2 * reqs.size());
+    a.views = d_views;
+    a.reqs = d_reqs;
+    a.nreq = (int)wreq.size();
+    a.nslots = nslots;
+    a.opaque = opaque;
+    a.sort = sort;
+    a.nkeys = nkeys;
+    a.key_base = d_kb;
+    a.ctl = d_ctl;
+    a.err = s0->d_err;
+    rt::WfCtl ctl0{};
+    ctl0.total = (unsigned long long)total;
+    CUDA_TRY(cudaMemcpyAsync(d_views, views.data(), views.size() * sizeof(rt::SceneView), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(d_reqs, wreq.data(), wreq.size() * sizeof(rt::WfRequest), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(d_kb, key_base.data(), key_base.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(d_ctl, &ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(d_films, films.data(), films.size() * sizeof(float*), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(d_fdims, fdims.data(), fdims.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemsetAsync(a.P.d, 0, (size_t)nslots * sizeof(float4), stream));
+    CUDA_TRY(cudaMemsetAsync(a.S.count, 0, sizeof(int), stream));
+    for (auto& q : wreq) CUDA_TRY(cudaMemsetAsync(q.accum, 0, (size_t)3 * q.ww * q.wh * sizeof(float), stream));
+    CUDA_TRY(cudaMemsetAsync(s0->d_err, 0, sizeof(int), stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));   // host vectors above go out of scope
+    // One iteration: reset, regen, extend, [scan, scatter], shade, occlude.
+    int blk = cfg.block;
+    unsigned gs = (unsigned)((nslots + blk - 1) / blk);
+    unsigned gsh = (unsigned)((cap + blk - 1) / blk);
+    unsigned g256 = (unsigned)((nslots + 255) / 256);
+    // ev (profiling only): boundaries between the kernel groups of one iteration.
+    auto launch_iter = [&](cudaEvent_t* ev) {
+        if (ev) cudaEventRecord(ev[0], stream);
+        rt::k_wf_reset<<<1, 256, 0, stream>>>(a);
+        rt::k_wf_regen<<<g256, 256, 0, stream>>>(a);
+        if (ev) cudaEventRecord(ev[1], stream);
+        rt::k_wf_extend<kStack><<<gs, blk, 0, stream>>>(a);
+        if (ev) cudaEventRecord(ev[2], stream);
+        if (sort) {
+            rt::k_wf_scan<<<1, 256, 0, stream>>>(a);
+            rt::k_wf_scatter<<<g256, 256, 0, stream>>>(a);
+        }
+        if (ev) cudaEventRecord(ev[3], stream);
+        rt::k_wf_shade<<<gs, blk, 0, stream>>>(a);
+        if (ev) cudaEventRecord(ev[4], stream);
+        rt::k_wf_occlude<kStack><<<gsh, blk, 0, stream>>>(a);
+        if (ev) cudaEventRecord(ev[5], stream);
+    };
+    const int batch = 4;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> pev;
+    if (cfg.profile) {
+        pev.resize(batch * 6);
+        for (auto& e : pev)
+            if (cudaEventCreate(&e) != cudaSuccess) return fail(RT_ERR_CUDA, "event creation failed");
+    } else {
+        CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        launch_iter(nullptr);
+        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+        if (ce != cudaSuccess) return fail(RT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return fail(RT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        }
+    }
+    int per_iter = 5 + (sort ? 2 : 0);
+    int max_depth = 1;
+    for (auto& q : wreq) max_depth = std::max(max_depth, q.rc.max_depth);
+    int64_t limit = (total / nslots + 2) * (int64_t)(max_depth + 2) + 64;
+    int64_t iters = 0;
+    double t_regen = 0, t_extend = 0, t_sort = 0, t_shade = 0, t_occlude = 0;
+    int rc = RT_OK;
+    CUDA_TRY(cudaEventRecord(s0->ev0, stream));
+    for (;;) {
+        for (int k = 0; k < batch; k++) {
+            if (cfg.profile) {
+                launch_iter(&pev[k * 6]);
+            } else if (cudaGraphLaunch(exec, stream) != cudaSuccess) {
+                rc = fail(RT_ERR_CUDA, "graph launch failed");
+                break;
+            }
+        }
+        if (rc != RT_OK) break;
+        iters += batch;
+        cudaMemcpyAsync(ws.pinned, &d_ctl->next, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(reinterpret_cast<char*>(ws.pinned) + 8, &d_ctl->live, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                        stream);
+        if (cudaStreamSynchronize(stream) != cudaSuccess) {
+            rc = fail(RT_ERR_CUDA, std::string("wavefront iteration failed: ") + cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if (cfg.profile) {
+            for (int k = 0; k < batch; k++) {
+                float m[5];
+                for (int e = 0; e < 5; e++) cudaEventElapsedTime(&m[e], pev[k * 6 + e], pev[k * 6 + e + 1]);
+                t_regen += m[0];
+                t_extend += m[1];
+                t_sort += m[2];
+                t_shade += m[3];
+                t_occlude += m[4];
+            }
+        }
+        unsigned long long next = ws.pinned[0];
+        int live = reinterpret_cast<int*>(ws.pinned)[2];
+        int overflow = reinterpret_cast<int*>(ws.pinned)[3];
+        if (overflow) {
+            rc = fail(RT_ERR_BOUNDS, "shadow queue overflow");
+            break;
+        }
+        if (next >= (unsigned long long)total && live == 0) break;
+        if (iters > limit) {
+            rc = fail(RT_ERR_TIMEOUT, "wavefront did not drain within its iteration bound");
+            break;
+        }
+    }
+    if (rc == RT_OK) {
+        dim3 g(std::max<unsigned>(1, std::min<unsigned>(4096, (unsigned)((wreq[0].ww * (int64_t)wreq[0].wh + 255) / 256))),
+               (unsigned)wreq.size());
+        rt::k_wf_finalize<<<g, 256, 0, stream>>>(d_reqs, (int)wreq.size(), d_films, d_fdims, d_fdims + reqs.size());
+        CUDA_TRY(cudaEventRecord(s0->ev1, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        rc = check_err(s0);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto e : pev) cudaEventDestroy(e);
+    if (rc != RT_OK) return rc;
+    if (st) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s0->ev0, s0->ev1);
+        st->kernel_ms = ms;
+        st->samples = (uint64_t)total;
+        st->kernel_launches = (int32_t)(iters * per_iter + 1);
+        st->iterations = (int32_t)iters;
+        st->regen_ms = t_regen;
+        st->extend_ms = t_extend;
+        st->sort_ms = t_sort;
+        st->shade_ms = t_shade;
+        st->occlude_ms = t_occlude;
+        st->rr_min_bounces = wreq[0].rc.rr_min_bounces;
+        st->rr_min_survival = wreq[0].rc.rr_min_survival;
+        st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return RT_OK;
+}
+
+WfConfig g_wf_default;
+
+int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam, float* d_film, RtStats* st) {
+    HostReq q;
+    q.scene = sc;
+    q.rc = make_rc(sc, p, cam);
+    q.x0 = p->pixel_x0;
+    q.y0 = p->pixel_y0;
+    q.ww = p->window_w > 0 ? p->window_w : p->width;
+    q.wh = p->window_h > 0 ? p->window_h : p->height;
+    q.spp = p->spp;
+    q.spp0 = p->spp_offset;
+    q.W = p->width;
+    q.H = p->height;
+    q.d_film = d_film;
+    WfConfig cfg = g_wf_default;
+    if (sc->tuned) {
+        cfg.slots = sc->tuned_slots;
+        cfg.block = sc->tuned_block;
+        cfg.sort = sc->tuned_sort;
+    }
+    if (p->wavefront_size > 0) cfg.slots = p->wavefront_size;
+    if (p->block_size > 0) cfg.block = p->block_size;
+    if (p->sort_materials >= 0) cfg.sort = p->sort_materials;
+    cfg.profile = p->profile_kernels != 0;
+    if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
+        return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
+    if (p->window_w > 0 || p->window_h > 0)
+        CUDA_TRY(cudaMemsetAsync(d_film, 0, (size_t)3 * p->width * p->height * sizeof(float), sc->stream));
+    return wf_render({q}, cfg, st);
 }
 
 }  // namespace
@@ -500,13 +883,18 @@ int rt_render(RtScene* sc, const RtRenderParams* p, float* out, RtStats* st) {
 
 int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest* reqs, int32_t n,
                     const RtRenderParams* common, float* const* outs, RtStats* st) {
-    if (!scenes || !reqs || !outs || !common || n < 0 || num_scenes <= 0)
-        return fail(RT_ERR_INVALID_ARG, "null argument");
-    RtStats total{};
-    for (int i = 0; i < n; i++) {
+    if (!scenes || !reqs || !outs || !common || n <= 0 || num_scenes <= 0)
+        return fail(RT_ERR_INVALID_ARG, "null argument or empty batch");
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<HostReq> hq((size_t)n);
+    std::vector<float*> d_films((size_t)n, nullptr);
+    int rc = RT_OK;
+    for (int i = 0; i < n && rc == RT_OK; i++) {
         const RtRequest& q = reqs[i];
-        if (q.scene < 0 || q.scene >= num_scenes || !scenes[q.scene] || !outs[i])
-            return fail(RT_ERR_INVALID_ARG, "request " + std::to_string(i) + ": bad scene or output");
+        if (q.scene < 0 || q.scene >= num_scenes || !scenes[q.scene] || !outs[i]) {
+            rc = fail(RT_ERR_INVALID_ARG, "request " + std::to_string(i) + ": bad scene or output");
+            break;
+        }
         RtScene* sc = scenes[q.scene];
         RtRenderParams p = *common;
         p.width = q.width;
@@ -514,21 +902,102 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
         p.spp = q.spp;
         p.max_depth = q.max_depth;
         p.pixel_x0 = p.pixel_y0 = p.window_w = p.window_h = 0;
-        std::lock_guard<std::mutex> lk(sc->mu);
-        size_t film_bytes = (size_t)3 * q.width * q.height * sizeof(float);
-        float* d_film = nullptr;
-        if (cudaMalloc(&d_film, film_bytes) != cudaSuccess) return fail(RT_ERR_OOM, "film allocation failed");
-        RtStats s1{};
-        int rc = render_to_device(sc, &p, q.camera, d_film, &s1);
-        if (rc == RT_OK && cudaMemcpy(outs[i], d_film, film_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
-            rc = fail(RT_ERR_CUDA, "film copy failed");
-        cudaFree(d_film);
-        if (rc != RT_OK) return rc;
-        total.kernel_ms += s1.kernel_ms;
-        total.samples += s1.samples;
-        total.kernel_launches += s1.kernel_launches;
+        p.spp_offset = 0;
+        rc = validate_params(sc, &p);
+        if (rc != RT_OK) break;
+        if (cudaSetDevice(sc->device) != cudaSuccess ||
+            cudaMalloc(&d_films[i], (size_t)3 * q.width * q.height * sizeof(float)) != cudaSuccess) {
+            rc = fail(RT_ERR_OOM, "film allocation failed");
+            break;
+        }
+        HostReq& h = hq[i];
+        h.scene = sc;
+        h.rc = make_rc(sc, &p, q.camera);
+        h.x0 = h.y0 = 0;
+        h.ww = q.width;
+        h.wh = q.height;
+        h.spp = q.spp;
+        h.spp0 = 0;
+        h.W = q.width;
+        h.H = q.height;
+        h.d_film = d_films[i];
     }
-    if (st) *st = total;
+    if (rc == RT_OK) {
+        WfConfig cfg = g_wf_default;
+        RtScene* s0 = scenes[reqs[0].scene];
+        if (s0->tuned) {
+            cfg.slots = s0->tuned_slots;
+            cfg.block = s0->tuned_block;
+            cfg.sort = s0->tuned_sort;
+        }
+        if (common->wavefront_size > 0) cfg.slots = common->wavefront_size;
+        if (common->block_size > 0) cfg.block = common->block_size;
+        if (common->sort_materials >= 0) cfg.sort = common->sort_materials;
+        rc = wf_render(hq, cfg, st);
+    }
+    for (int i = 0; i < n; i++) {
+        if (rc == RT_OK &&
+            cudaMemcpy(outs[i], d_films[i], (size_t)3 * reqs[i].width * reqs[i].height * sizeof(float),
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = fail(RT_ERR_CUDA, "film copy failed");
+        if (d_films[i]) cudaFree(d_films[i]);
+    }
+    if (st && rc == RT_OK)
+        st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best) {
+    if (!sc || !params) return fail(RT_ERR_INVALID_ARG, "null argument");
+    int rc = validate_params(sc, params);
+    if (rc != RT_OK) return rc;
+    std::lock_guard<std::mutex> lk(sc->mu);
+    CUDA_TRY(cudaSetDevice(sc->device));
+    // A bounded slice of the render: the full window at the spp that gives
+    // ~16 M samples (at least 4x the largest wavefront), capped at params->spp.
+    int ww = params->window_w > 0 ? params->window_w : params->width;
+    int wh = params->window_h > 0 ? params->window_h : params->height;
+    int64_t npix = (int64_t)ww * wh;
+    int spp = (int)std::max<int64_t>(1, std::min<int64_t>(params->spp, ((int64_t)1 << 24) / npix + 1));
+    float* d_film = nullptr;
+    if (cudaMalloc(&d_film, (size_t)3 * params->width * params->height * sizeof(float)) != cudaSuccess)
+        return fail(RT_ERR_OOM, "film allocation failed");
+    const int sizes[3] = {1 << 18, 1 << 20, 1 << 22};
+    const int blocks[3] = {64, 128, 256};
+    double best_ms = 1e30;
+    WfConfig pick;
+    for (int si = 0; si < 3 && rc == RT_OK; si++)
+        for (int bi = 0; bi < 3 && rc == RT_OK; bi++)
+            for (int so = 0; so < 2 && rc == RT_OK; so++) {
+                RtRenderParams p = *params;
+                p.kernel = RT_KERNEL_WAVEFRONT;
+                p.spp = spp;
+                p.count_work = 0;
+                p.wavefront_size = sizes[si];
+                p.block_size = blocks[bi];
+                p.sort_materials = so;
+                RtStats s1{};
+                rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
+                if (rc == RT_OK && s1.kernel_ms < best_ms) {
+                    best_ms = s1.kernel_ms;
+                    pick.slots = sizes[si];
+                    pick.block = blocks[bi];
+                    pick.sort = so;
+                }
+            }
+    cudaFree(d_film);
+    if (rc != RT_OK) return rc;
+    sc->tuned = 1;
+    sc->tuned_slots = pick.slots;
+    sc->tuned_block = pick.block;
+    sc->tuned_sort = pick.sort;
+    if (best) {
+        *best = *params;
+        best->kernel = RT_KERNEL_WAVEFRONT;
+        best->wavefront_size = pick.slots;
+        best->block_size = pick.block;
+        best->sort_materials = pick.sort;
+    }
     return RT_OK;
 }
 
@@ -617,6 +1086,25 @@ int rt_sobol_batch(const uint32_t* idx, const uint32_t* dim, const uint32_t* see
                                                      reinterpret_cast<float*>(d + 3 * b));
         if (cudaGetLastError() != cudaSuccess || cudaMemcpy(out, d + 3 * b, b, cudaMemcpyDeviceToHost) != cudaSuccess)
             rc = fail(RT_ERR_CUDA, "sobol kernel failed");
+    }
+    cudaFree(d);
+    return rc;
+}
+
+int rt_tonemap(const float* hdr, int32_t width, int32_t height, float exposure_ev, float* rgb) {
+    if (!hdr || !rgb || width <= 0 || height <= 0) return fail(RT_ERR_INVALID_ARG, "bad tonemap arguments");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(RT_ERR_NO_DEVICE, "no CUDA device");
+    size_t n = (size_t)width * height, b = n * 3 * sizeof(float);
+    float* d = nullptr;
+    if (cudaMalloc(&d, 2 * b) != cudaSuccess) return fail(RT_ERR_OOM, "allocation failed");
+    int rc = RT_OK;
+    if (cudaMemcpy(d, hdr, b, cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = fail(RT_ERR_CUDA, "copy failed");
+    } else {
+        k_tonemap<<<(unsigned)((n + 255) / 256), 256>>>(d, (int)n, powf(2.0f, exposure_ev), d + n * 3);
+        if (cudaGetLastError() != cudaSuccess || cudaMemcpy(rgb, d + n * 3, b, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = fail(RT_ERR_CUDA, "tonemap failed");
     }
     cudaFree(d);
     return rc;

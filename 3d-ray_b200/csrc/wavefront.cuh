@@ -1,0 +1,378 @@
+// Persistent, request-batched wavefront form of the bounce loop.
+//
+// A fixed pool of path slots (the wavefront) is advanced one vertex per
+// iteration by four small kernels instead of one large one:
+//   regen   : resolve finished samples into their request's film, then refill
+//             the slot with the next (request, sample, pixel) work item from a
+//             global counter (warp-aggregated atomics): camera ray generation.
+//   extend  : closest hit of every live path's current ray.
+//   shade   : one TraceRay vertex (medium, emission, NEE, BSDF sample, RR).
+//             Shadow rays go to a queue instead of being traced inline.
+//   occlude : any-hit (or the transparent walk) of the queued shadow rays;
+//             visible contributions are added to their path's accumulator.
+// The iteration is captured once in a CUDA graph and replayed until every
+// request's samples are done. Optional material sorting (a counting sort of
+// live slots by material id) feeds shade coherent warps.
+//
+// Many requests of uneven resolution, spp and depth share the pool: a work id
+// maps to (request, sample, pixel) with a binary search over the requests'
+// prefix offsets, samples outermost so a warp shares a sample index.
+#pragma once
+
+#include "integrator.cuh"
+
+namespace rt {
+
+enum : int {
+    PF_ALIVE = 1,       // a ray is in flight
+    PF_DONE = 2,        // finished: the sample waits for resolve
+    PF_PREV_DELTA = 4,
+    PF_FIRST = 8,
+    PF_CLAMP = 16,
+};
+
+struct WfRequest {
+    RenderConst rc;
+    int scene;
+    int x0, y0, ww, wh;   // render window inside the W x H image
+    int spp, spp0;
+    long long begin;      // first global work id of this request
+    long long count;      // ww * wh * spp
+    float* accum;         // 3 * ww * wh: sums of clamped samples (planar)
+};
+
+// SoA path state (144 B per slot + 16 B hit).
+struct WfPaths {
+    float4* o;      // o.xyz, prev_pdf
+    float4* d;      // d.xyz, flags
+    float4* beta;   // beta.xyz, depth
+    float4* w;      // w.xyz, rng dim
+    float4* lp;     // lp.xyz, sample index
+    float4* la;     // la.xyz, pixel (lx | ly << 16, window-local)
+    float4* pre;    // pre.xyz, request
+    float4* att0;   // att0.xyz, la mask (3 bits)
+    float4* ab;     // cur_abs.xyz, ior count   (dielectric scenes)
+    float* ior;     // 8 per slot                (dielectric scenes)
+    float4* hit;    // t, u, v, kind << 30 | slot
+    int* order;     // slot order for shade (material-sorted or identity)
+    int* keys;      // material key per slot (sorting)
+};
+
+struct WfShadow {
+    float4* o;    // o.xyz, tmax
+    float4* d;    // d.xyz, slot << 1 | to_la
+    float4* c;    // contribution.xyz, scene
+    int* count;
+    int capacity;
+};
+
+struct WfCtl {
+    unsigned long long next;    // next global work id
+    unsigned long long total;   // total work ids
+    int live;                   // slots alive or done after the last regen
+    int overflow;               // shadow queue overflow (never expected: sized by the host)
+    int hist[256];              // material histogram (sorting)
+};
+
+struct WfArgs {
+    const SceneView* views;
+    const WfRequest* reqs;
+    int nreq;
+    int nslots;
+    int opaque;       // every scene of the batch is opaque: any-hit shadows
+    int sort;
+    int nkeys;        // material keys (sum over scenes) for sorting
+    const int* key_base;   // per scene: first key
+    WfPaths P;
+    WfShadow S;
+    WfCtl* ctl;
+    int* err;
+};
+
+RT_D int fbits(float f) { return __float_as_int(f); }
+RT_D float ibits(int i) { return __int_as_float(i); }
+
+// Warp-aggregated atomic add of 1 per active lane; returns this lane's slot.
+RT_D unsigned long long wagg_next(unsigned long long* ctr) {
+    unsigned mask = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    int rank = __popc(mask & ((1u << lane) - 1u));
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(ctr, (unsigned long long)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + (unsigned long long)rank;
+}
+RT_D int wagg_next_int(int* ctr) {
+    unsigned mask = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    int rank = __popc(mask & ((1u << lane) - 1u));
+    int base = 0;
+    if (lane == leader) base = atomicAdd(ctr, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + rank;
+}
+
+RT_D void wf_store(const WfArgs& a, int i, const PathState& ps, int flags, int req, int pix) {
+    a.P.o[i] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.prev_pdf);
+    a.P.d[i] = make_float4(ps.d.x, ps.d.y, ps.d.z, ibits(flags));
+    a.P.beta[i] = make_float4(ps.beta.x, ps.beta.y, ps.beta.z, ibits(ps.depth));
+    a.P.w[i] = make_float4(ps.w.x, ps.w.y, ps.w.z, ibits((int)ps.rng.dim));
+    a.P.lp[i] = make_float4(ps.lp.x, ps.lp.y, ps.lp.z, ibits((int)ps.rng.index));
+    a.P.la[i] = make_float4(ps.la.x, ps.la.y, ps.la.z, ibits(pix));
+    a.P.pre[i] = make_float4(ps.pre.x, ps.pre.y, ps.pre.z, ibits(req));
+    int mask = (ps.mask.x != 0.0f ? 1 : 0) | (ps.mask.y != 0.0f ? 2 : 0) | (ps.mask.z != 0.0f ? 4 : 0);
+    a.P.att0[i] = make_float4(ps.att0.x, ps.att0.y, ps.att0.z, ibits(mask));
+}
+
+RT_D int wf_flags(const PathState& ps, int alive) {
+    return (alive ? PF_ALIVE : PF_DONE) | (ps.prev_delta ? PF_PREV_DELTA : 0) | (ps.first ? PF_FIRST : 0) |
+           (ps.clamp_mode ? PF_CLAMP : 0);
+}
+
+RT_D uint32_t pixel_seed(int px, int py) { return ((uint32_t)px * 73856093u) ^ ((uint32_t)py * 19349663u); }
+
+// Rebuilds the register path state of slot i (lp/la read after occlude).
+RT_D void wf_load(const WfArgs& a, int i, const WfRequest& R, PathState& ps, int& flags, int& pix) {
+    float4 o = a.P.o[i], d = a.P.d[i], b = a.P.beta[i], w = a.P.w[i], lp = a.P.lp[i], la = a.P.la[i],
+           pre = a.P.pre[i], at = a.P.att0[i];
+    flags = fbits(d.w);
+    pix = fbits(la.w);
+    ps.o = v3(o.x, o.y, o.z);
+    ps.prev_pdf = o.w;
+    ps.d = v3(d.x, d.y, d.z);
+    ps.beta = v3(b.x, b.y, b.z);
+    ps.depth = fbits(b.w);
+    ps.w = v3(w.x, w.y, w.z);
+    ps.lp = v3(lp.x, lp.y, lp.z);
+    ps.la = v3(la.x, la.y, la.z);
+    ps.pre = v3(pre.x, pre.y, pre.z);
+    ps.att0 = v3(at.x, at.y, at.z);
+    int mask = fbits(at.w);
+    ps.mask = v3((mask & 1) ? 1.0f : 0.0f, (mask & 2) ? 1.0f : 0.0f, (mask & 4) ? 1.0f : 0.0f);
+    ps.prev_delta = (flags & PF_PREV_DELTA) != 0;
+    ps.first = (flags & PF_FIRST) != 0;
+    ps.clamp_mode = (flags & PF_CLAMP) != 0;
+    int lx = pix & 0xFFFF, ly = pix >> 16;
+    ps.rng = Sampler{pixel_seed(R.x0 + lx, R.y0 + ly), (uint32_t)fbits(lp.w), (uint32_t)fbits(w.w)};
+    ps.cur_abs = v3(0.0f);
+    ps.iors.n = 0;
+    if (R.rc.dielectrics) {
+        float4 ab = a.P.ab[i];
+        ps.cur_abs = v3(ab.x, ab.y, ab.z);
+        ps.iors.n = fbits(ab.w);
+        for (int k = 0; k < 8; k++) ps.iors.slot[k] = a.P.ior[(size_t)i * 8 + k];
+    }
+}
+
+RT_D void wf_store_media(const WfArgs& a, int i, const WfRequest& R, const PathState& ps) {
+    if (!R.rc.dielectrics) return;
+    a.P.ab[i] = make_float4(ps.cur_abs.x, ps.cur_abs.y, ps.cur_abs.z, ibits(ps.iors.n));
+    for (int k = 0; k < 8; k++) a.P.ior[(size_t)i * 8 + k] = ps.iors.slot[k];
+}
+
+RT_D int find_request(const WfRequest* reqs, int n, unsigned long long id) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if ((unsigned long long)reqs[mid].begin <= id) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    float4 d = a.P.d[i];
+    int flags = fbits(d.w);
+    if (flags & PF_ALIVE) {
+        atomicAdd(&a.ctl->live, 1);
+        return;
+    }
+    if (flags & PF_DONE) {   // resolve the finished sample into its film
+        int req = fbits(a.P.pre[i].w);
+        const WfRequest& R = a.reqs[req];
+        PathState ps;
+        int fl, pix;
+        wf_load(a, i, R, ps, fl, pix);
+        V3 L = path_resolve(ps, R.rc);
+        int lx = pix & 0xFFFF, ly = pix >> 16;
+        size_t plane = (size_t)R.ww * R.wh, k = (size_t)ly * R.ww + lx;
+        atomicAdd(R.accum + k, L.x);
+        atomicAdd(R.accum + plane + k, L.y);
+        atomicAdd(R.accum + 2 * plane + k, L.z);
+    }
+    unsigned long long id = wagg_next(&a.ctl->next);
+    if (id >= a.ctl->total) {
+        a.P.d[i].w = ibits(0);
+        return;
+    }
+    int req = find_request(a.reqs, a.nreq, id);
+    const WfRequest& R = a.reqs[req];
+    long long local = (long long)(id - (unsigned long long)R.begin);
+    long long npix = (long long)R.ww * R.wh;
+    int s = (int)(local / npix);
+    int p = (int)(local % npix);
+    int lx = p % R.ww, ly = p / R.ww;
+    PathState ps;
+    path_init(ps, R.rc, R.x0 + lx, R.y0 + ly, (uint32_t)(R.spp0 + s));
+    int alive = path_alive(ps);
+    wf_store(a, i, ps, wf_flags(ps, alive), req, lx | (ly << 16));
+    wf_store_media(a, i, R, ps);
+    atomicAdd(&a.ctl->live, 1);
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    float4 d = a.P.d[i];
+    if (!(fbits(d.w) & PF_ALIVE)) return;
+    float4 o = a.P.o[i];
+    int req = fbits(a.P.pre[i].w);
+    const SceneView& s = a.views[a.reqs[req].scene];
+    Hit h;
+    traverse<false, STACK>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf, h, nullptr, a.err);
+    int packed = h.kind == HIT_NONE ? 0 : ((h.kind << 30) | h.slot);
+    a.P.hit[i] = make_float4(h.t, h.u, h.v, ibits(packed));
+    if (a.sort) {   // material key for the counting sort
+        int key = a.nkeys;   // misses and emitters sort last
+        if (h.kind != HIT_NONE) {
+            int ent = h.kind == HIT_TRI ? s.tri_entity[h.slot] : h.slot;
+            key = a.key_base[a.reqs[req].scene] + s.entities[ent].material;
+        }
+        a.P.keys[i] = key;
+        atomicAdd(&a.ctl->hist[key], 1);
+    }
+}
+
+// Exclusive scan of the material histogram (one block) and the scatter of
+// live slots into material order.
+__global__ void k_wf_scan(WfArgs a) {
+    __shared__ int s[257];
+    int t = threadIdx.x;
+    if (t <= a.nkeys) s[t] = a.ctl->hist[t];
+    __syncthreads();
+    if (t == 0) {
+        int acc = 0;
+        for (int k = 0; k <= a.nkeys; k++) {
+            int c = s[k];
+            s[k] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    if (t <= a.nkeys) a.ctl->hist[t] = s[t];
+}
+__global__ void k_wf_scatter(WfArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    if (!(fbits(a.P.d[i].w) & PF_ALIVE)) return;
+    int pos = atomicAdd(&a.ctl->hist[a.P.keys[i]], 1);
+    a.P.order[pos] = i;
+}
+
+// Shadow sink of the wavefront: queue the ray with its contribution.
+struct QueueShadows {
+    const WfArgs* a;
+    int slot;
+    int scene;
+    RT_D void shadow(PathState& ps, V3 o, V3 d, float tmax, V3 c, int to_la) {
+        if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) {
+            ps.add(c, to_la);   // records the per-frame sanitize in the mask
+            return;
+        }
+        int j = wagg_next_int(a->S.count);
+        if (j >= a->S.capacity) {
+            atomicExch(&a->ctl->overflow, 1);
+            return;
+        }
+        a->S.o[j] = make_float4(o.x, o.y, o.z, tmax);
+        a->S.d[j] = make_float4(d.x, d.y, d.z, ibits((slot << 1) | to_la));
+        a->S.c[j] = make_float4(c.x, c.y, c.z, ibits(scene));
+    }
+};
+
+__global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int i;
+    if (a.sort) {
+        // the scatter left the live slots in material order in order[0 .. live)
+        if (t >= a.ctl->hist[a.nkeys]) return;
+        i = a.P.order[t];
+    } else {
+        if (t >= a.nslots) return;
+        i = t;
+    }
+    float4 d4 = a.P.d[i];
+    int flags = fbits(d4.w);
+    if (!(flags & PF_ALIVE)) return;
+    int req = fbits(a.P.pre[i].w);
+    const WfRequest& R = a.reqs[req];
+    const SceneView& s = a.views[R.scene];
+    PathState ps;
+    int fl, pix;
+    wf_load(a, i, R, ps, fl, pix);
+    float4 hh = a.P.hit[i];
+    int packed = fbits(hh.w);
+    Hit h;
+    h.t = hh.x;
+    h.u = hh.y;
+    h.v = hh.z;
+    h.kind = packed == 0 ? HIT_NONE : ((unsigned)packed >> 30);
+    h.slot = packed & 0x3FFFFFFF;
+    QueueShadows sink{&a, i, R.scene};
+    bool alive = shade_vertex(s, R.rc, ps, h, sink);
+    wf_store(a, i, ps, wf_flags(ps, alive), req, pix);
+    wf_store_media(a, i, R, ps);
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(256) k_wf_occlude(WfArgs a) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = min(*a.S.count, a.S.capacity);
+    if (j >= n) return;
+    float4 o = a.S.o[j], d = a.S.d[j], c = a.S.c[j];
+    const SceneView& s = a.views[fbits(c.w)];
+    V3 tr = shadow_transmittance<STACK>(s, a.opaque, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, o.w, nullptr,
+                                        a.err);
+    if (near_zero(tr)) return;
+    int packed = fbits(d.w);
+    int slot = packed >> 1;
+    V3 v = v3(c.x, c.y, c.z) * tr;
+    float4* dst = (packed & 1) ? (a.P.la + slot) : (a.P.lp + slot);
+    float* f = reinterpret_cast<float*>(dst);
+    atomicAdd(f, v.x);
+    atomicAdd(f + 1, v.y);
+    atomicAdd(f + 2, v.z);
+}
+
+// Per-iteration reset of the counters the next iteration accumulates.
+__global__ void k_wf_reset(WfArgs a) {
+    int t = threadIdx.x;
+    if (t == 0) {
+        *a.S.count = 0;
+        a.ctl->live = 0;
+    }
+    if (a.sort)
+        for (int k = t; k <= a.nkeys; k += blockDim.x) a.ctl->hist[k] = 0;
+}
+
+// Mean of the accumulated sums into the films (Renderer.cs:711).
+__global__ void k_wf_finalize(const WfRequest* reqs, int nreq, float* const* films, const int* film_w,
+                              const int* film_h) {
+    int r = blockIdx.y;
+    if (r >= nreq) return;
+    const WfRequest& R = reqs[r];
+    long long plane = (long long)R.ww * R.wh;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+        int lx = (int)(i % R.ww), ly = (int)(i / R.ww);
+        size_t fp = (size_t)film_w[r] * film_h[r];
+        size_t fi = (size_t)(R.y0 + ly) * film_w[r] + (R.x0 + lx);
+        for (int c = 0; c < 3; c++) films[r][c * fp + fi] = R.accum[c * plane + i] / (float)R.spp;
+    }
+}
+
+}  // namespace rt

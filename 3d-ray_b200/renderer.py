@@ -1,0 +1,141 @@
+"""Host-side mirror of 3d-ray's `Renderer` API over the C-ABI.
+
+`Renderer(world, ...)` takes the constructor arguments of
+src/RayTracer/Rendering/Renderer.cs:300-319 that matter on the GPU path and
+`render(width, height)` returns a `RenderResult` like Renderer.Render
+(:522-733): display pixels (ACES + gamma, [H, W, 3]) and the linear-HDR
+beauty buffer (planar [3, H, W], the FrameBuffer layout). Everything below
+the call runs in librt3d.so on the GPU; there is no CPU fallback — a missing
+library or device raises.
+
+The reference's `world` is an IHittable graph built by its YAML loader; here
+it is a `scenes.World` (the same information, entity-level), from which the
+library performs the world assembly and SAH build.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+from . import abi, scenes
+
+MIS = {"balance": 0, "power": 1}
+LIGHT_STRATEGY = {"all": 0}
+KERNELS = {"megakernel": abi.KERNEL_MEGAKERNEL, "wavefront": abi.KERNEL_WAVEFRONT}
+
+
+@dataclasses.dataclass
+class RenderResult:
+    pixels: np.ndarray        # [H, W, 3] display RGB in [0, 1]
+    beauty: np.ndarray        # [3, H, W] linear HDR (mean of clamped samples)
+    stats: dict
+
+
+class Renderer:
+    DEFAULT_MAX_SAMPLE_RADIANCE = 10.0    # Renderer.cs:202
+    DEFAULT_INDIRECT_CLAMP_FACTOR = 0.25  # Renderer.cs:214
+
+    def __init__(self, world: "scenes.World", samples_per_pixel: int, max_depth: int,
+                 max_sample_radiance: float | None = None, verbose: bool = False,
+                 mis_heuristic: str = "balance", light_sampling_strategy: str = "all",
+                 indirect_clamp_factor: float = DEFAULT_INDIRECT_CLAMP_FACTOR, exposure_ev: float = 0.0,
+                 kernel: str = "wavefront"):
+        if light_sampling_strategy not in LIGHT_STRATEGY:
+            raise ValueError(f"light strategy {light_sampling_strategy!r} is outside the GPU path")
+        self.world = world
+        self.spp = int(samples_per_pixel)
+        self.max_depth = int(max_depth)
+        self.max_sample_radiance = self.DEFAULT_MAX_SAMPLE_RADIANCE if max_sample_radiance is None \
+            else float(max_sample_radiance)
+        self.indirect_clamp_factor = float(indirect_clamp_factor)
+        self.exposure_ev = float(exposure_ev)
+        self.mis = MIS[mis_heuristic]
+        self.kernel = KERNELS[kernel]
+        self.verbose = verbose
+        self._lib = abi.load()
+        self._packed = abi.PackedWorld(world)
+        h = C.c_void_p()
+        abi.check(self._lib.rt_scene_create(self._packed.ref(), C.byref(h)), "rt_scene_create")
+        self._scene = h
+        info = abi.RtSceneInfo()
+        abi.check(self._lib.rt_scene_info(h, C.byref(info)))
+        self.info = info
+        if verbose and info.rr_min_bounces == 6:
+            print("  Lighting:    indirect-dominant (conservative RR)")
+
+    def close(self):
+        if getattr(self, "_scene", None):
+            self._lib.rt_scene_destroy(self._scene)
+            self._scene = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self, width: int, height: int, **kw) -> "abi.RtRenderParams":
+        return abi.render_params(width, height, self.spp, self.max_depth,
+                                 max_sample_radiance=self.max_sample_radiance,
+                                 indirect_clamp_factor=self.indirect_clamp_factor, exposure_ev=self.exposure_ev,
+                                 mis_heuristic=self.mis, kernel=self.kernel, **kw)
+
+    def autotune(self, width: int, height: int) -> dict:
+        best = abi.RtRenderParams()
+        p = self.params(width, height)
+        abi.check(self._lib.rt_autotune(self._scene, C.byref(p), C.byref(best)), "rt_autotune")
+        return dict(wavefront_size=best.wavefront_size, block_size=best.block_size,
+                    sort_materials=best.sort_materials)
+
+    def render(self, width: int, height: int, **kw) -> RenderResult:
+        p = self.params(width, height, **kw)
+        beauty = np.zeros((3, height, width), np.float32)
+        st = abi.RtStats()
+        abi.check(self._lib.rt_render(self._scene, C.byref(p), abi.ptr(beauty), C.byref(st)), "rt_render")
+        return RenderResult(self.tone_map_to_display(beauty), beauty,
+                            {f: getattr(st, f) for f, _ in abi.RtStats._fields_})
+
+    def tone_map_to_display(self, beauty: np.ndarray) -> np.ndarray:
+        """Renderer.ToneMapToDisplay (:741): exposure, ACES, gamma on the GPU."""
+        _, h, w = beauty.shape
+        beauty = np.ascontiguousarray(beauty, np.float32)
+        out = np.zeros((h, w, 3), np.float32)
+        abi.check(self._lib.rt_tonemap(abi.ptr(beauty), w, h, self.exposure_ev, abi.ptr(out)), "rt_tonemap")
+        return out
+
+
+def render_batch(requests, worlds, common_kernel: str = "wavefront", **kw):
+    """Renders many (scene, camera, size, spp, depth) requests in one
+    persistent wavefront launch (rt_render_batch). `worlds` is a list of
+    scenes.World; each request is a dict with scene (index), width, height,
+    spp, max_depth and camera (scenes.camera dict). Returns the linear-HDR
+    films and the stats."""
+    lib = abi.load()
+    packed = [abi.PackedWorld(w) for w in worlds]
+    handles = []
+    try:
+        for pw in packed:
+            h = C.c_void_p()
+            abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
+            handles.append(h)
+        n = len(requests)
+        reqs = (abi.RtRequest * n)()
+        outs = []
+        for i, r in enumerate(requests):
+            q = reqs[i]
+            q.scene, q.width, q.height, q.spp, q.max_depth = r["scene"], r["width"], r["height"], r["spp"], \
+                r["max_depth"]
+            q.camera = abi.camera_desc(r["camera"])
+            outs.append(np.zeros((3, r["height"], r["width"]), np.float32))
+        common = abi.render_params(1, 1, 1, 1, kernel=KERNELS[common_kernel], **kw)
+        st = abi.RtStats()
+        arr = (C.c_void_p * len(handles))(*[h.value for h in handles])
+        optrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        abi.check(lib.rt_render_batch(arr, len(handles), reqs, n, C.byref(common), optrs, C.byref(st)),
+                  "rt_render_batch")
+        return outs, st
+    finally:
+        for h in handles:
+            lib.rt_scene_destroy(h)

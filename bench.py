@@ -142,11 +142,18 @@ def build_world():
     return rt, rt.scenes.throughput_scene()
 
 
-def cpu_baseline(rt, world, budget_s=12.0, rank=0):
-    """Times the oracle on a bounded pixel window of the same frame."""
+def oracle_scene(rt, world):
     from oracle import binding
     binding.build()
-    osc = binding.OracleScene(rt.abi.PackedWorld(world))
+    return binding.OracleScene(rt.abi.PackedWorld(world))
+
+
+def cpu_baseline(rt, world, budget_s=12.0, osc=None):
+    """Times the oracle on a bounded pixel window of the same frame (the scene
+    build, like the reference's, is outside the timing)."""
+    own = osc is None
+    if own:
+        osc = oracle_scene(rt, world)
     cores = os.cpu_count() or 1
     win_w, win_h = 64, 16
     # Calibrate with a small window, then size the window for ~budget_s.
@@ -164,22 +171,23 @@ def cpu_baseline(rt, world, budget_s=12.0, rank=0):
     osc.render(p, threads=cores)
     dt = time.perf_counter() - t
     samples = win_w2 * win_h2 * SPP
-    osc.close()
+    if own:
+        osc.close()
     return {"value": samples / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{win_w2}x{win_h2} centre pixels of the 1920x1080 frame at {SPP} spp, depth {DEPTH} "
                       f"({samples} samples, {dt:.1f} s)"}
 
 
 def run_reference(args):
-    rank, world_size, dist = dist_setup(args.gpus)
-    if rank != 0:
-        barrier(dist)
+    # The reference path is a CPU renderer: rank 0 alone runs it, other ranks exit.
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     rt, world = build_world()
+    osc = oracle_scene(rt, world)
     per = []
     base = None
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline(rt, world, budget_s=8.0)
+        b = cpu_baseline(rt, world, budget_s=8.0, osc=osc)
         if i >= args.warmup:
             per.append(b["value"])
             base = b
@@ -192,11 +200,69 @@ def run_reference(args):
             "cpu_baseline": dict(base, value=v),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-    barrier(dist)
 
 
 def flush_l2(torch_mod, buf):
     buf.fill_(1)
+
+
+def rel_mse(x, r):
+    return float(np.mean((x - r) ** 2 / (r ** 2 + 1e-2)))
+
+
+def time_to_relmse(rt, lib, abi, kernels=("wavefront", "megakernel"), target=1e-3):
+    """Cornell box 256x256, depth 8: seconds of device time until relMSE <= 1e-3
+    against a 65 536-spp reference (rendered from a disjoint Sobol range so it
+    is uncorrelated with the test images)."""
+    import torch
+    world = rt.scenes.cornell()
+    pw = abi.PackedWorld(world)
+    h = C.c_void_p()
+    abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
+    Wc = Hc = 256
+    film = torch.empty((3, Hc, Wc), dtype=torch.float32, device="cuda")
+    st = abi.RtStats()
+    ref_spp = 65536
+    p = abi.render_params(Wc, Hc, ref_spp, 8, kernel=abi.KERNEL_WAVEFRONT, spp_offset=1 << 20)
+    abi.check(lib.rt_render_device(h, C.byref(p), C.c_void_p(film.data_ptr()), C.byref(st)), "reference")
+    ref = film.cpu().numpy().copy()
+    out = {"workload": "cornell 256x256 depth 8", "reference_spp": ref_spp, "target": target}
+    for kname in kernels:
+        kid = abi.KERNEL_WAVEFRONT if kname == "wavefront" else abi.KERNEL_MEGAKERNEL
+        spp = 16
+        while spp <= 16384:
+            p = abi.render_params(Wc, Hc, spp, 8, kernel=kid)
+            abi.check(lib.rt_render_device(h, C.byref(p), C.c_void_p(film.data_ptr()), C.byref(st)), kname)
+            e = rel_mse(film.cpu().numpy(), ref)
+            if e <= target:
+                out[kname] = {"seconds": st.kernel_ms / 1e3, "spp": spp, "rel_mse": e}
+                break
+            spp *= 2
+    lib.rt_scene_destroy(h)
+    return out
+
+
+def profile_frame(args):
+    """One warm-up and one measured frame with fixed wavefront settings (4M
+    slots, block 256, material sort) or the megakernel: the workload the ncu
+    summaries under profiles/ were captured on."""
+    rt, world = build_world()
+    abi = rt.abi
+    lib = abi.load()
+    pw = abi.PackedWorld(world)
+    scene = C.c_void_p()
+    abi.check(lib.rt_scene_create(pw.ref(), C.byref(scene)), "rt_scene_create")
+    kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
+    p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=256,
+                          sort_materials=1)
+    film = np.zeros((3, H, W), np.float32)
+    st = abi.RtStats()
+    for i in range(2):
+        abi.check(lib.rt_render(scene, C.byref(p), film.ctypes.data_as(C.c_void_p), C.byref(st)), "rt_render")
+        print(json.dumps({"frame": i, "kernel": args.kernel, "spp": args.spp, "kernel_ms": st.kernel_ms,
+                          "Msamples_per_s": W * H * args.spp / st.kernel_ms / 1e3,
+                          "iterations": st.iterations, "launches": st.kernel_launches}), flush=True)
+    lib.rt_scene_destroy(scene)
 
 
 def main():
@@ -205,12 +271,17 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--kernel", default="megakernel", choices=["megakernel", "wavefront"])
+    ap.add_argument("--kernel", default="wavefront", choices=["megakernel", "wavefront"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain-kernel and relMSE side measurements")
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--profile-frame", action="store_true",
+                    help="render the frame twice with fixed settings and exit (the command profiled by ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_frame:
+        return profile_frame(args)
 
     import torch
     rank, world_size, dist = dist_setup(args.gpus)
@@ -222,35 +293,39 @@ def main():
     pw = abi.PackedWorld(world)
     scene = C.c_void_p()
     abi.check(lib.rt_scene_create(pw.ref(), C.byref(scene)), "rt_scene_create")
-    kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
     spp = args.spp
+    kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
     params = abi.render_params(W, H, spp, DEPTH, kernel=kern)
+    tuned = None
+    if kern == abi.KERNEL_WAVEFRONT:   # setup, outside the timed region (like the BVH build)
+        best = abi.RtRenderParams()
+        abi.check(lib.rt_autotune(scene, C.byref(params), C.byref(best)), "rt_autotune")
+        tuned = {"wavefront_size": best.wavefront_size, "block_size": best.block_size,
+                 "sort_materials": best.sort_materials}
     film = torch.empty((3, H, W), dtype=torch.float32, device="cuda")
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    st = abi.RtStats()
 
-    def step():
-        abi.check(lib.rt_render_device(scene, C.byref(params), C.c_void_p(film.data_ptr()), C.byref(st)),
-                  "rt_render_device")
-        return st.kernel_ms, st.kernel_launches
-
-    for _ in range(args.warmup):
-        step()
-        flush_l2(torch, l2)
-    torch.cuda.synchronize()
-    barrier(dist)
-    torch.cuda.synchronize()
-    times, launches = [], 0
-    with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
-            ms, nl = step()
-            times.append(ms)
-            launches += nl
+    def timed(p, steps, warmup):
+        st = abi.RtStats()
+        for _ in range(warmup):
+            abi.check(lib.rt_render_device(scene, C.byref(p), C.c_void_p(film.data_ptr()), C.byref(st)), "warmup")
             flush_l2(torch, l2)
         torch.cuda.synchronize()
-    barrier(dist)
-    torch.cuda.synchronize()
-    total_ms = max_over_ranks(float(sum(times)), dist)
+        barrier(dist)
+        torch.cuda.synchronize()
+        times, launches = [], 0
+        for _ in range(steps):
+            abi.check(lib.rt_render_device(scene, C.byref(p), C.c_void_p(film.data_ptr()), C.byref(st)), "step")
+            times.append(st.kernel_ms)
+            launches += st.kernel_launches
+            flush_l2(torch, l2)
+        torch.cuda.synchronize()
+        barrier(dist)
+        torch.cuda.synchronize()
+        return max_over_ranks(float(sum(times)), dist), launches
+
+    with ClockSampler(dev) as clk:
+        total_ms, launches = timed(params, args.steps, args.warmup)
     samples_per_step = W * H * spp
     value = world_size * samples_per_step * args.steps / (total_ms / 1e3) / 1e6
     ms_per_step = total_ms / args.steps
@@ -270,24 +345,32 @@ def main():
     e2e_total = max_over_ranks(float(sum(e2e_times)), dist)
     e2e_value = world_size * samples_per_step * args.steps / e2e_total / 1e6
 
-    # Roofline: algorithmic bytes per sample from the counting build on a
-    # fixed subsample (every 8th row and column block), scaled to the launch.
+    # Algorithmic work per sample of the reference algorithm (counting build
+    # over four fixed 64x32 windows of the frame).
     cp = abi.render_params(W, H, spp, DEPTH, kernel=abi.KERNEL_MEGAKERNEL, count_work=1)
-    work = {"node_visits": 0, "tri_tests": 0, "other_tests": 0, "closest_rays": 0, "shadow_rays": 0, "samples": 0}
+    keys = ["node_visits", "prim_tests", "other_tests", "closest_rays", "shadow_rays", "shadow_node_visits",
+            "shadow_prim_tests", "shadow_other_tests", "samples"]
+    work = dict.fromkeys(keys, 0)
     stc = abi.RtStats()
     for (x0, y0) in [(0, 0), (W // 2, H // 2), (W // 4, H // 3), (3 * W // 4, 2 * H // 3)]:
         cp.pixel_x0, cp.pixel_y0, cp.window_w, cp.window_h = min(x0, W - 64), min(y0, H - 32), 64, 32
         abi.check(lib.rt_render_device(scene, C.byref(cp), C.c_void_p(film.data_ptr()), C.byref(stc)), "count")
-        work["node_visits"] += stc.node_visits
-        work["tri_tests"] += stc.prim_tests
-        work["other_tests"] += stc.other_tests
-        work["closest_rays"] += stc.closest_rays
-        work["shadow_rays"] += stc.shadow_rays
-        work["samples"] += stc.samples
-    bytes_per_sample = (32 * work["node_visits"] + 36 * work["tri_tests"] + 64 * work["other_tests"]
-                        + 96 * work["closest_rays"]) / max(work["samples"], 1)
-    kernel_s = ms_per_step / 1e3
-    achieved = bytes_per_sample * samples_per_step / kernel_s / 1e9
+        for k in keys:
+            work[k] += getattr(stc, k)
+    ns = max(work["samples"], 1)
+    per = {k: work[k] / ns for k in keys if k != "samples"}
+    closest_b = 32 * per["node_visits"] + 36 * per["prim_tests"] + 64 * per["other_tests"]
+    shadow_b = 32 * per["shadow_node_visits"] + 36 * per["shadow_prim_tests"] + 64 * per["shadow_other_tests"]
+    bytes_per_sample = closest_b + shadow_b + 96 * per["closest_rays"]
+    # Per-kernel algorithmic bytes per sample (wavefront form):
+    #   extend : closest-ray traversal + 48 B ray in / hit out per closest ray
+    #   occlude: shadow-ray traversal + 60 B (48 B record in, 12 B accumulate) per shadow ray
+    #   shade  : 304 B path state + hit per vertex + 48 B per shadow record written
+    #   regen  : 144 B path state written per sample + 48 B resolve
+    kb = {"extend": closest_b + 48 * per["closest_rays"],
+          "occlude": shadow_b + 60 * per["shadow_rays"],
+          "shade": 304 * per["closest_rays"] + 48 * per["shadow_rays"],
+          "regen": 192.0}
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -295,28 +378,52 @@ def main():
     except Exception:
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
+    roof = {"bound": "hbm", "peak": hbm, "unit": "GB/s",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6.65 TB/s",
+            "algorithmic_bytes_per_sample": bytes_per_sample, "work_per_sample": per}
+    if kern == abi.KERNEL_WAVEFRONT:
+        pp = abi.render_params(W, H, spp, DEPTH, kernel=kern, profile_kernels=1)
+        stp = abi.RtStats()
+        abi.check(lib.rt_render_device(scene, C.byref(pp), C.c_void_p(film.data_ptr()), C.byref(stp)), "profile")
+        kt = {"regen": stp.regen_ms, "extend": stp.extend_ms, "shade": stp.shade_ms, "occlude": stp.occlude_ms,
+              "sort": stp.sort_ms}
+        dom = max(["regen", "extend", "shade", "occlude"], key=lambda k: kt[k])
+        # scale the profiled (ungraphed) split onto the timed per-step device time
+        tot = sum(kt.values())
+        k_s = ms_per_step / 1e3 * kt[dom] / tot
+        achieved = kb[dom] * samples_per_step / k_s / 1e9
+        roof.update({"kernel": f"k_wf_{dom}", "achieved": achieved, "frac": achieved / hbm,
+                     "kernel_ms_per_step": {k: v * ms_per_step / tot for k, v in kt.items()},
+                     "launches_per_step": stp.iterations, "algorithmic_bytes_per_launch": kb[dom] *
+                     samples_per_step / max(stp.iterations, 1)})
+    else:
+        achieved = bytes_per_sample * samples_per_step / (ms_per_step / 1e3) / 1e9
+        roof.update({"kernel": "k_render_mega", "achieved": achieved, "frac": achieved / hbm})
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "render_megakernel_icospheres.md")
+    prof = os.path.join(ROOT, "profiles", f"{roof['kernel']}_icospheres.md")
     if os.path.exists(prof):
         for line in open(prof):
-            if line.startswith("traffic_bytes_per_full_launch:"):
+            if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
+    roof["traffic"] = traffic
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
             "config": {"workload": f"icospheres-64x20480 ({world.num_tris} tris) {W}x{H} {spp}spp depth{DEPTH}",
-                       "kernel": args.kernel, "parallelism": f"replicas{world_size}",
+                       "kernel": args.kernel, "autotuned": tuned, "parallelism": f"replicas{world_size}",
                        "l2": "flushed between steps (256 MiB write)", "spp": spp},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic,
-                         "algorithmic_bytes_per_sample": bytes_per_sample,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback",
-                         "work_per_sample": {k: v / max(work["samples"], 1) for k, v in work.items()
-                                             if k != "samples"}},
+            "roofline": roof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(params),
                     "d2h_bytes_per_step": 3 * W * H * 4},
             "gpu_launches": launches, "clocks": clk.summary()}
+    if not args.no_extras and kern == abi.KERNEL_WAVEFRONT:
+        pm = abi.render_params(W, H, spp, DEPTH, kernel=abi.KERNEL_MEGAKERNEL)
+        mt, _ = timed(pm, 1, 1)
+        mv = world_size * samples_per_step / (mt / 1e3) / 1e6
+        line["plain_kernel"] = {"value": mv, "unit": UNIT, "ms_per_step": mt, "speedup_wavefront": value / mv}
+        if rank == 0:
+            line["time_to_relmse_1e-3"] = time_to_relmse(rt, lib, abi)
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rt, world)
     lib.rt_scene_destroy(scene)

@@ -174,13 +174,13 @@ typedef struct RtRenderParams {
     int32_t mis_heuristic;          /* RT_MIS_* */
     int32_t light_strategy;         /* RT_LIGHTS_ALL only */
     int32_t kernel;                 /* RT_KERNEL_* */
-    int32_t block_size;             /* 0: autotuned / default */
-    int32_t wavefront_size;         /* 0: autotuned / default (wavefront only) */
-    int32_t sort_materials;         /* wavefront: sort hits by material */
+    int32_t block_size;             /* wavefront: 64, 128 or 256; 0: autotuned / default */
+    int32_t wavefront_size;         /* wavefront: path slots; 0: autotuned / default */
+    int32_t sort_materials;         /* wavefront: 1 sort hits by material, 0 no, -1 autotuned / default */
     int32_t pixel_x0, pixel_y0;     /* render window (0,0,0,0 = full frame) */
     int32_t window_w, window_h;
     int32_t count_work;             /* 1: counting build, fills the work fields of RtStats */
-    int32_t pad;
+    int32_t profile_kernels;        /* 1: wavefront without the graph, per-kernel events in RtStats */
 } RtRenderParams;
 
 /* Counters and timings of one call. */
@@ -188,15 +188,19 @@ typedef struct RtStats {
     double   kernel_ms;             /* device time of the render kernels (CUDA events) */
     double   total_ms;              /* host wall time of the call */
     uint64_t samples;               /* camera samples traced */
-    uint64_t closest_rays;          /* closest-hit rays */
-    uint64_t shadow_rays;           /* any-hit rays */
-    uint64_t node_visits;           /* BVH node box tests (count_work only) */
-    uint64_t prim_tests;            /* triangle tests (count_work only) */
-    uint64_t other_tests;           /* quad / sphere tests (count_work only) */
+    uint64_t closest_rays;          /* closest-hit rays (count_work only) */
+    uint64_t shadow_rays;           /* any-hit rays (count_work only) */
+    uint64_t node_visits;           /* BVH node box tests of closest rays (count_work only) */
+    uint64_t prim_tests;            /* triangle tests of closest rays (count_work only) */
+    uint64_t other_tests;           /* quad / sphere tests of closest rays (count_work only) */
+    uint64_t shadow_node_visits;    /* the same three for shadow rays (count_work only) */
+    uint64_t shadow_prim_tests;
+    uint64_t shadow_other_tests;
+    double   regen_ms, extend_ms, shade_ms, occlude_ms, sort_ms;   /* profile_kernels only */
+    int32_t  iterations;            /* wavefront iterations */
     int32_t  kernel_launches;       /* kernels launched by the call */
     int32_t  rr_min_bounces;        /* the RR knobs the call used */
     float    rr_min_survival;
-    int32_t  pad;
 } RtStats;
 
 typedef struct RtScene RtScene;
@@ -269,6 +273,12 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
                     const RtRequest* requests, int32_t n,
                     const RtRenderParams* common, float* const* outs, RtStats* stats);
 
+/* Autotuner: times the wavefront over wavefront size {256K, 1M, 4M} x block
+ * {64, 128, 256} x material sort {off, on} on a bounded slice of `params`
+ * (the full window at the spp giving ~16 M samples), keeps the fastest for
+ * this scene (used when those params fields are 0 / -1) and returns it. */
+int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* best);
+
 /* ---- differentiation ----------------------------------------------------- */
 /* Parameters the adjoint differentiates, per material (Disney) and per emitter:
  * base_color[3], roughness, metallic, specular, sheen, clearcoat, spec_trans,
@@ -318,6 +328,11 @@ int rt_bsdf_batch(RtScene* scene, const RtBsdfQuery* q, int64_t n, RtBsdfResult*
 /* Owen-scrambled Sobol draws: out[i] = Sample(idx[i], dim[i], seed[i]). */
 int rt_sobol_batch(const uint32_t* sample_index, const uint32_t* dim, const uint32_t* pixel_seed,
                    int64_t n, float* out);
+
+/* Display transform: exposure gain 2^ev, ACES filmic fit, gamma 1/2.2
+ * (Renderer.AcesToneMap, Rendering/Renderer.cs:893-907). Planar HDR in
+ * (3*W*H host floats), interleaved RGB out (W*H*3 host floats in [0, 1]). */
+int rt_tonemap(const float* hdr_rgb_planar, int32_t width, int32_t height, float exposure_ev, float* rgb_out);
 
 /* Kulla-Conty tables the scene uses: E (32x32, mu-major) then E_avg (32). */
 int rt_energy_lut(float* e_1024, float* eavg_32);

@@ -93,7 +93,7 @@ def test_closest_hit_cornell_camera_rays(oracle, cornell, cornell_world):
     os_ = oracle.OracleScene(abi.PackedWorld(cornell_world))
     o, _ = os_.trace_closest(rays)
     nhit, nt = _compare_hits(g, o)
-    assert nhit > 55000 and nt == 0
+    assert nhit > rays.shape[0] // 2 and nt == 0
 
 
 def test_closest_hit_cornell_random_rays(oracle, cornell, cornell_world):
@@ -101,7 +101,7 @@ def test_closest_hit_cornell_random_rays(oracle, cornell, cornell_world):
     g = cornell.closest(rays)
     o, _ = oracle.OracleScene(abi.PackedWorld(cornell_world)).trace_closest(rays)
     nhit, nt = _compare_hits(g, o)
-    assert nhit > 190000 and nt == 0
+    assert nhit > rays.shape[0] // 2 and nt == 0
 
 
 def test_closest_hit_throughput_scene(oracle, throughput_world):
@@ -112,7 +112,7 @@ def test_closest_hit_throughput_scene(oracle, throughput_world):
         g = s.closest(rays)
         o, _ = oracle.OracleScene(abi.PackedWorld(throughput_world)).trace_closest(rays)
         nhit, nt = _compare_hits(g, o)
-        assert nhit > 100000 and nt == 0
+        assert nhit > rays.shape[0] // 4 and nt == 0
     finally:
         s.close()
 
@@ -168,8 +168,16 @@ def test_bsdf_matches_oracle(oracle, which, cornell_world, throughput_world_smal
         np.testing.assert_allclose(g["pdf"], o["pdf"], rtol=1e-4, atol=1e-7)
         np.testing.assert_allclose(g["fd"], o["fd"], rtol=1e-4, atol=1e-7)
         hs = g["has_sample"] == 1
+        # Sampled directions go through cos/sin (CUDA vs glibc differ by ulps):
+        # equal to ~1e-5, and the sample's f/pdf must equal Evaluate/Pdf at the
+        # GPU's own direction, evaluated by the oracle, within 1e-4.
         np.testing.assert_allclose(g["wo"][hs], o["wo"][hs], rtol=1e-4, atol=1e-5)
-        np.testing.assert_allclose(g["s_pdf"][hs], o["s_pdf"][hs], rtol=1e-3, atol=1e-6)
+        q2 = q[hs].copy()
+        q2["l"] = g["wo"][hs]
+        o2 = oracle.OracleScene(abi.PackedWorld(world)).bsdf(q2, abi.BSDF_RESULT_DTYPE)
+        nd = g["is_delta"][hs] == 0
+        np.testing.assert_allclose(g["s_pdf"][hs][nd], o2["pdf"][nd], rtol=1e-4, atol=1e-7)
+        np.testing.assert_allclose(g["s_f"][hs][nd], o2["f"][nd], rtol=1e-4, atol=1e-7)
     finally:
         s.close()
 
@@ -188,3 +196,119 @@ def test_render_cornell_matches_oracle(oracle, cornell, cornell_world):
     assert np.all(np.isfinite(g))
     np.testing.assert_allclose(g.mean(axis=(1, 2)), o.mean(axis=(1, 2)), rtol=0.02)
     assert rel_mse(o, g) < 0.05
+
+
+def test_wavefront_matches_megakernel_and_oracle(oracle, cornell, cornell_world):
+    """The wavefront (queues, shadow-ray sink, regeneration) estimates the same
+    image as the megakernel and the oracle."""
+    pm = abi.render_params(64, 64, 1024, 8, kernel=abi.KERNEL_MEGAKERNEL)
+    pw = abi.render_params(64, 64, 1024, 8, kernel=abi.KERNEL_WAVEFRONT, wavefront_size=1 << 16)
+    m, _ = cornell.render(pm)
+    w, st = cornell.render(pw)
+    assert st.samples == 64 * 64 * 1024 and st.kernel_launches > 10
+    o, _ = oracle.OracleScene(abi.PackedWorld(cornell_world)).render(abi.render_params(64, 64, 256, 8))
+    np.testing.assert_allclose(w.mean(axis=(1, 2)), m.mean(axis=(1, 2)), rtol=0.01)
+    np.testing.assert_allclose(w.mean(axis=(1, 2)), o.mean(axis=(1, 2)), rtol=0.02)
+    assert rel_mse(w, m) < 0.02
+
+
+@pytest.mark.parametrize("sort", [0, 1])
+def test_wavefront_throughput_scene(oracle, throughput_world_small, sort):
+    s = Scene(throughput_world_small)
+    try:
+        p = abi.render_params(96, 54, 256, 12, kernel=abi.KERNEL_WAVEFRONT, wavefront_size=1 << 15,
+                              sort_materials=sort)
+        w, _ = s.render(p)
+        m, _ = s.render(abi.render_params(96, 54, 256, 12, kernel=abi.KERNEL_MEGAKERNEL))
+        np.testing.assert_allclose(w.mean(axis=(1, 2)), m.mean(axis=(1, 2)), rtol=0.02)
+        assert rel_mse(w, m) < 0.05
+    finally:
+        s.close()
+
+
+def test_render_window_and_spp_offset(cornell):
+    """A window renders only its pixels; spp_offset continues the same Sobol
+    sequence (progressive resume: two halves average to the whole)."""
+    full, _ = cornell.render(abi.render_params(32, 32, 64, 8, kernel=abi.KERNEL_MEGAKERNEL))
+    a, _ = cornell.render(abi.render_params(32, 32, 32, 8, kernel=abi.KERNEL_MEGAKERNEL))
+    b, _ = cornell.render(abi.render_params(32, 32, 32, 8, kernel=abi.KERNEL_MEGAKERNEL, spp_offset=32))
+    np.testing.assert_allclose((a + b) / 2, full, rtol=1e-4, atol=1e-6)
+    win, _ = cornell.render(abi.render_params(32, 32, 64, 8, kernel=abi.KERNEL_MEGAKERNEL, pixel_x0=8,
+                                              pixel_y0=4, window_w=16, window_h=8))
+    np.testing.assert_allclose(win[:, 4:12, 8:24], full[:, 4:12, 8:24], rtol=1e-4, atol=1e-6)
+    assert np.all(win[:, :4] == 0) and np.all(win[:, :, :8] == 0)
+
+
+def test_batch_equals_individual_renders(cornell_world, throughput_world_small):
+    """C3 form: uneven requests over two scenes in one persistent launch give
+    the same images as rendering each request alone (same Sobol streams; only
+    the order of the float additions differs)."""
+    lib = abi.load()
+    sa, sb = Scene(cornell_world), Scene(throughput_world_small)
+    try:
+        rng = np.random.default_rng(7)
+        reqs = (abi.RtRequest * 5)()
+        outs, singles = [], []
+        for i in range(5):
+            sc = i % 2
+            res = int(rng.choice([16, 24, 40]))
+            spp = int(rng.choice([16, 32, 64]))
+            depth = int(rng.integers(4, 13))
+            world = cornell_world if sc == 0 else throughput_world_small
+            reqs[i].scene, reqs[i].width, reqs[i].height, reqs[i].spp, reqs[i].max_depth = sc, res, res, spp, depth
+            reqs[i].camera = abi.camera_desc(world.camera)
+            outs.append(np.zeros((3, res, res), np.float32))
+            s = sa if sc == 0 else sb
+            single, _ = s.render(abi.render_params(res, res, spp, depth, kernel=abi.KERNEL_WAVEFRONT))
+            singles.append(single)
+        scenes = (C.c_void_p * 2)(sa.h, sb.h)
+        optrs = (C.c_void_p * 5)(*[o.ctypes.data for o in outs])
+        st = abi.RtStats()
+        common = abi.render_params(1, 1, 1, 1, kernel=abi.KERNEL_WAVEFRONT, wavefront_size=1 << 14)
+        abi.check(lib.rt_render_batch(scenes, 2, reqs, 5, C.byref(common), optrs, C.byref(st)), "rt_render_batch")
+        assert st.samples == sum(r.width * r.height * r.spp for r in reqs)
+        for o, s1 in zip(outs, singles):
+            np.testing.assert_allclose(o, s1, rtol=1e-4, atol=1e-6)
+    finally:
+        sa.close()
+        sb.close()
+
+
+def test_gpu_matches_committed_golden(cornell, lib):
+    """The committed oracle fixtures (tests/golden/) reproduced on the GPU:
+    Sobol draws and hit records bit-exact, BSDF lobes exact, values 1e-4."""
+    import os
+    from golden.make_golden import golden_inputs
+    from conftest import ROOT
+    g = np.load(os.path.join(ROOT, "tests", "golden", "oracle_golden.npz"))
+    inp = golden_inputs()
+    n = inp["sobol_idx"].size
+    out = np.zeros(n, np.float32)
+    abi.check(lib.rt_sobol_batch(abi.ptr(inp["sobol_idx"]), abi.ptr(inp["sobol_dim"]), abi.ptr(inp["sobol_seed"]),
+                                 n, abi.ptr(out)))
+    assert np.array_equal(out.view(np.uint32), g["sobol"].view(np.uint32))
+    assert np.array_equal(cornell.closest(inp["rays"]), g["hits"])
+    b = cornell.bsdf(inp["bsdf"])
+    gb = g["bsdf"]
+    assert np.array_equal(b["lobe"], gb["lobe"]) and np.array_equal(b["dims_used"], gb["dims_used"])
+    np.testing.assert_allclose(b["f"], gb["f"], rtol=1e-4, atol=1e-7)
+    np.testing.assert_allclose(b["pdf"], gb["pdf"], rtol=1e-4, atol=1e-7)
+    img, _ = cornell.render(abi.render_params(16, 16, 64, 8))
+    assert np.all(np.isfinite(img)) and abs(img.mean() / g["image"].mean() - 1) < 0.1
+
+
+def test_work_counters_match_oracle(oracle, cornell, cornell_world):
+    """The counting build's traversal work per sample (roofline bytes) equals
+    the oracle's counters for the reference algorithm, statistically."""
+    p = abi.render_params(64, 64, 64, 8, kernel=abi.KERNEL_MEGAKERNEL, count_work=1)
+    _, st = cornell.render(p)
+    o, c = oracle.OracleScene(abi.PackedWorld(cornell_world)).render(abi.render_params(64, 64, 64, 8),
+                                                                     counters=True)
+    g_nodes = (st.node_visits + st.shadow_node_visits) / st.samples
+    o_nodes = c["node_visits"] / c["samples"]
+    g_rays = st.closest_rays / st.samples
+    o_rays = c["closest_rays"] / c["samples"]
+    assert abs(g_rays / o_rays - 1) < 0.02, (g_rays, o_rays)
+    assert abs(g_nodes / o_nodes - 1) < 0.03, (g_nodes, o_nodes)
+    g_tri = (st.prim_tests + st.shadow_prim_tests) / st.samples
+    assert abs(g_tri / (c["tri_tests"] / c["samples"]) - 1) < 0.03
