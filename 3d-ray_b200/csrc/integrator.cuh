@@ -163,7 +163,10 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
             if (ls.occluded || !ls.has_ray) continue;
             V3 brdf = bsdf_eval_direct(s, m, rec, ls.dir, view, rec.n);
             brdf = brdf * (view_term * shadow_terminator(rec.n, rec.n, ls.dir));
-            if (is_zero(brdf)) continue;
+            if (is_zero(brdf)) {
+                sink.skipped(ls.ray_o, ls.dir, ls.ray_tmax);
+                continue;
+            }
             V3 tr_m = v3(1.0f);
             if (s.has_medium) tr_m = medium_tr(s, ls.dist >= kInf ? 1e30f : ls.dist);
             float wgt = 1.0f;
@@ -347,6 +350,11 @@ struct InlineShadows {
         V3 tr = shadow_transmittance<STACK>(*s, opaque, o, d, kEps, tmax, cnt, err);
         if (near_zero(tr)) return;
         ps.add(c * tr, to_la);
+    }
+    // A shadow ray the reference casts but whose contribution is zero: traced
+    // only by the counting build, so the work counts are the reference's.
+    RT_D void skipped(V3 o, V3 d, float tmax) {
+        if (cnt) shadow_transmittance<STACK>(*s, opaque, o, d, kEps, tmax, cnt, err);
     }
 };
 

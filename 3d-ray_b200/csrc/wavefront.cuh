@@ -293,6 +293,7 @@ struct QueueShadows {
         a->S.d[j] = make_float4(d.x, d.y, d.z, ibits((slot << 1) | to_la));
         a->S.c[j] = make_float4(c.x, c.y, c.z, ibits(scene));
     }
+    RT_D void skipped(V3, V3, float) {}
 };
 
 __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
