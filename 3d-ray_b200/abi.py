@@ -243,6 +243,7 @@ def load(path: str | None = None):
                                        P, C.c_int64]),
         "rt_render": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtStats)]),
         "rt_render_device": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtStats)]),
+        "rt_render_device_noalloc": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtStats)]),
         "rt_render_batch": (C.c_int, [P, C.c_int32, P, C.c_int32, C.POINTER(RtRenderParams), P,
                                       C.POINTER(RtStats)]),
         "rt_adjoint": (C.c_int, [P, C.POINTER(RtRenderParams), P, P, C.POINTER(RtStats)]),

@@ -860,6 +860,111 @@ int rt_render_device(RtScene* sc, const RtRenderParams* p, float* d_film, RtStat
     return render_to_device(sc, p, sc->host.camera, d_film, st);
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free megakernel render.
+//
+// Some hosts cannot allocate device memory while they render: a host that
+// reserves its whole device-memory budget at start-up and must not grow it,
+// or one that renders from a latency-critical thread where cudaMalloc and
+// cudaFree (which synchronise the device) are not allowed. For them the
+// megakernel's scratch — the per-chunk partial sums and the error word — lives
+// in this one fixed array instead of memory allocated per call. The array is
+// 32 MiB (kNoAllocFloats floats): the error word in its first 256 bytes, the
+// partial sums after it. Every GPU that loads the library holds it until the
+// process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocFloats = size_t(8) << 20;   // 32 MiB
+constexpr size_t kNoAllocHeader = 64;                // floats before the partial sums (256 B)
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
+
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[64] = {};
+
+// The device address of g_noalloc_scratch on the current device, looked up
+// once per device (the host-side name is only a stand-in for it).
+int noalloc_scratch(int device, float** out) {
+    if (device < 0 || device >= 64) return fail(RT_ERR_INVALID_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(RT_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = static_cast<float*>(ptr);
+    }
+    *out = g_noalloc_ptr[device];
+    return RT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rt_render_device_noalloc(RtScene* sc, const RtRenderParams* p, float* d_film, RtStats* st) {
+    if (!sc || !p || !d_film) return fail(RT_ERR_INVALID_ARG, "null argument");
+    if (p->count_work) return fail(RT_ERR_INVALID_ARG, "count_work is not available without allocation");
+    std::lock_guard<std::mutex> lk(sc->mu);
+    auto t0 = std::chrono::steady_clock::now();
+    int rc_ = validate_params(sc, p);
+    if (rc_ != RT_OK) return rc_;
+    CUDA_TRY(cudaSetDevice(sc->device));
+    float* scratch = nullptr;
+    rc_ = noalloc_scratch(sc->device, &scratch);
+    if (rc_ != RT_OK) return rc_;
+    int ww = p->window_w > 0 ? p->window_w : p->width;
+    int wh = p->window_h > 0 ? p->window_h : p->height;
+    int64_t npix = (int64_t)ww * wh;
+    const int64_t cap = (int64_t)(kNoAllocFloats - kNoAllocHeader);
+    if (3 * npix > cap)
+        return fail(RT_ERR_INVALID_ARG, "render window of " + std::to_string(npix) +
+                                            " pixels exceeds the allocation-free maximum of " +
+                                            std::to_string(cap / 3) + " pixels");
+    // The same chunking as rt_render_device, reduced until the partial sums fit.
+    int64_t target = 148LL * 2048 * 2;
+    int nchunks = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, (target + npix - 1) / npix));
+    nchunks = (int)std::min<int64_t>(nchunks, cap / (3 * npix));
+    int per_chunk = (p->spp + nchunks - 1) / nchunks;
+    nchunks = (p->spp + per_chunk - 1) / per_chunk;
+    rt::RenderConst rc = make_rc(sc, p, sc->host.camera);
+    int* err = reinterpret_cast<int*>(scratch);
+    auto* work = reinterpret_cast<unsigned long long*>(scratch + 16);
+    float* partial = scratch + kNoAllocHeader;
+    // The array keeps the previous call's contents: only the error word must
+    // start at zero (every partial sum is overwritten by the kernel).
+    CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), sc->stream));
+    if (p->window_w > 0 || p->window_h > 0)
+        CUDA_TRY(cudaMemsetAsync(d_film, 0, (size_t)3 * p->width * p->height * sizeof(float), sc->stream));
+    dim3 grid((ww + 15) / 16, (wh + 7) / 8, nchunks);
+    CUDA_TRY(cudaEventRecord(sc->ev0, sc->stream));
+    k_render_mega<kStack, false><<<grid, kBlock, 0, sc->stream>>>(sc->view, rc, p->pixel_x0, p->pixel_y0, ww, wh,
+                                                                  p->spp_offset, per_chunk, p->spp, partial, work,
+                                                                  err);
+    k_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, sc->stream>>>(partial, nchunks, ww, wh, p->width, p->height,
+                                                                     p->pixel_x0, p->pixel_y0, p->spp, d_film);
+    CUDA_TRY(cudaEventRecord(sc->ev1, sc->stream));
+    CUDA_TRY(cudaGetLastError());
+    int e = 0;
+    CUDA_TRY(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+    CUDA_TRY(cudaStreamSynchronize(sc->stream));
+    if (e == RT_ERR_STACK) return fail(RT_ERR_STACK, "traversal stack bound exceeded");
+    if (e != 0) return fail(RT_ERR_BOUNDS, "device error " + std::to_string(e));
+    if (st) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+        st->kernel_ms = ms;
+        st->samples = (uint64_t)npix * (uint64_t)p->spp;
+        st->kernel_launches = 2;
+        st->rr_min_bounces = rc.rr_min_bounces;
+        st->rr_min_survival = rc.rr_min_survival;
+        st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return RT_OK;
+}
+
 int rt_render(RtScene* sc, const RtRenderParams* p, float* out, RtStats* st) {
     if (!sc || !out || !p) return fail(RT_ERR_INVALID_ARG, "null argument");
     std::lock_guard<std::mutex> lk(sc->mu);

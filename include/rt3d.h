@@ -259,6 +259,24 @@ int rt_render(RtScene* scene, const RtRenderParams* params, float* hdr_rgb_plana
 int rt_render_device(RtScene* scene, const RtRenderParams* params, float* d_hdr_rgb_planar,
                      RtStats* stats);
 
+/* Allocation-free variant of rt_render_device (megakernel only). No
+ * counterpart in the reference. For hosts that cannot allocate device memory
+ * while rendering — a host whose device-memory budget is fixed at start-up,
+ * or one rendering from a latency-critical thread where cudaMalloc/cudaFree
+ * (which synchronise the device) are not allowed. The caller passes the scene
+ * and a device film of 3*W*H floats; the kernel's scratch (partial sums and
+ * the error word) lives in one fixed 32 MiB array inside the library, so the
+ * call makes no allocation. Limits and rules:
+ *   - the render window may hold at most 2 796 181 pixels (3 floats each in
+ *     8 Mi floats minus a 256-byte header); larger windows return
+ *     RT_ERR_INVALID_ARG; count_work is rejected;
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture;
+ *   - every call shares the array: calls that overlap on the GPU (any scenes,
+ *     any threads) race and must be serialised by the caller. */
+int rt_render_device_noalloc(RtScene* scene, const RtRenderParams* params, float* d_hdr_rgb_planar,
+                             RtStats* stats);
+
 /* One request of a batch. */
 typedef struct RtRequest {
     int32_t scene;                /* index into the scenes array */
