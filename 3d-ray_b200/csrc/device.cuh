@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <climits>
 
 #include "scene_types.h"
 
@@ -104,14 +105,6 @@ struct Counters {
 
 RT_D V3 ld3(const float4& f) { return v3(f.x, f.y, f.z); }
 
-RT_D bool box_hit(float4 lo, float4 hi, V3 o, V3 inv, float tmin, float tmax) {   // Core/AABB.cs:28-52
-    float t0x = (lo.x - o.x) * inv.x, t0y = (lo.y - o.y) * inv.y, t0z = (lo.z - o.z) * inv.z;
-    float t1x = (hi.x - o.x) * inv.x, t1y = (hi.y - o.y) * inv.y, t1z = (hi.z - o.z) * inv.z;
-    float te = fmaxf(tmin, fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))));
-    float tx = fminf(tmax, fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z))));
-    return tx >= te;
-}
-
 // Geometry/Triangle.cs:49-89 (Moller-Trumbore, |a| < 1e-7 reject, inclusive t range)
 RT_D bool tri_test(const float4* tris, int i, V3 o, V3 d, float tmin, float tmax, float& t, float& u, float& v) {
     float4 a0 = __ldg(tris + 3 * i), a1 = __ldg(tris + 3 * i + 1), a2 = __ldg(tris + 3 * i + 2);
@@ -181,94 +174,143 @@ RT_D bool entity_test(const SceneView& s, int e, V3 o, V3 d, float tmin, float t
     return true;
 }
 
+// Slab test of one child box; te receives max(tmin, entry distance).
+RT_D bool box_hit_te(float lx, float ly, float lz, float hx, float hy, float hz, V3 o, V3 inv, float tmin,
+                     float tmax, float& te) {   // Core/AABB.cs:28-52
+    float t0x = (lx - o.x) * inv.x, t0y = (ly - o.y) * inv.y, t0z = (lz - o.z) * inv.z;
+    float t1x = (hx - o.x) * inv.x, t1y = (hy - o.y) * inv.y, t1z = (hz - o.z) * inv.z;
+    te = fmaxf(tmin, fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))));
+    float tx = fminf(tmax, fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z))));
+    return tx >= te;
+}
+
 // Ordered depth-first traversal reproducing HittableList -> BvhNode -> Mesh ->
-// BvhNode -> Triangle (Geometry/HittableList.cs:19-37, Acceleration/BvhNode.cs:157-206):
-// near child first by sign(dir[axis]), fat leaves scanned in order, a later
-// primitive at an equal t wins, the far child is tested against the closest t
-// found in the near subtree. ANY = true stops at the first accepted hit
-// (opaque shadow rays). Stack entries: node index (>= 0) or ~entity.
+// BvhNode -> Triangle (Geometry/HittableList.cs:19-37, Acceleration/BvhNode.cs:157-206).
+// The near child (sign of dir[split axis]) is visited first, fat leaves are
+// scanned in order, a later primitive at an equal t wins (inclusive range).
+// Each 64-byte node record holds both children's boxes: both are tested
+// against the current closest t when the parent is visited, and a pushed far
+// child keeps its entry distance so it is dropped at pop time exactly when
+// BvhNode's own box test (against the closer t found meanwhile) would reject
+// it. Box tests only prune, never accept, so the primitive test sequence is
+// the reference's minus primitives that cannot be hit: ids and t match.
+// ANY = true stops at the first accepted hit (opaque shadow rays).
+// has_root restricts the walk to one mesh BVH (a light's own geometry).
 // Returns false on stack overflow (err set).
-// root >= 0 restricts the walk to one mesh BVH (a light's own geometry).
 template <bool ANY, int STACK>
 __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
-                                         TravCounters* cnt, int* err, int root = -1) {
+                                         TravCounters* cnt, int* err, bool has_root = false, int root = 0) {
+    const int kNone = INT_MIN;   // "pop the next entry" (no leaf code can take this value)
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
-    int stack[STACK];
+    int st_code[STACK];
+    float st_te[STACK];
     int sp = 0;
     float closest = tmax;
     best.kind = HIT_NONE;
-    if (root >= 0) {
-        stack[sp++] = root;
-    } else if (s.top_root >= 0) {
-        stack[sp++] = s.top_root;
+    int code = kNone;
+    if (has_root) {
+        code = root;
+        if (cnt && root >= 0) cnt->nodes++;   // the mesh root's own BvhNode.Hit
+    } else if (s.top_is_bvh) {
+        code = s.top_root;
+        if (cnt) cnt->nodes++;                // the world root's BvhNode.Hit
     } else {
-        for (int i = s.num_top_items - 1; i >= 0; --i) stack[sp++] = ~s.top_items[i];
-    }
-    while (sp > 0) {
-        int e = stack[--sp];
-        int node;
-        if (e < 0) {
-            int ent = ~e;
-            Entity en = s.entities[ent];
-            if (en.kind != ENT_MESH) {
-                if (cnt) cnt->others++;
-                Hit h;
-                if (entity_test(s, ent, o, d, tmin, closest, h)) {
-                    best = h;
-                    closest = h.t;
-                    if (ANY) return true;
-                }
-                continue;
-            }
-            node = en.index;
-        } else {
-            node = e;
+        for (int i = s.num_top_items - 1; i >= 0; --i) {
+            st_code[sp] = leaf_code(s.top_items[i], LEAF_ENT1, 1);
+            st_te[sp] = -kInf;
+            sp++;
         }
-        for (;;) {
-            const float4* np = reinterpret_cast<const float4*>(s.nodes + node);
-            float4 lo = __ldg(np), hi = __ldg(np + 1);
-            int a = __float_as_int(lo.w), b = __float_as_int(hi.w);
-            if (cnt) cnt->nodes++;
-            if (a >= 0) {
-                if (!box_hit(lo, hi, o, inv, tmin, closest)) break;
-                int right = b & 0x3FFFFFFF;
-                int axis = (int)((unsigned)b >> 30);
-                float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
-                int near_c = da >= 0.0f ? a : right;
-                int far_c = da >= 0.0f ? right : a;
+    }
+    for (;;) {
+        // Descend interior records: test both children, go near, stack far.
+        while (code >= 0) {
+            const float4* np = s.cnodes + (size_t)code * 4;
+            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), e = __ldg(np + 3);
+            if (cnt) cnt->nodes += 2;
+            float tel, ter;
+            bool hl = box_hit_te(a.x, a.y, a.z, b.x, b.y, b.z, o, inv, tmin, closest, tel);
+            bool hr = box_hit_te(c.x, c.y, c.z, e.x, e.y, e.z, o, inv, tmin, closest, ter);
+            int axis = __float_as_int(c.w);
+            float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
+            bool left_near = da >= 0.0f;
+            int lc = __float_as_int(a.w), rc = __float_as_int(b.w);
+            int nc = left_near ? lc : rc, fc = left_near ? rc : lc;
+            bool hn = left_near ? hl : hr, hf = left_near ? hr : hl;
+            float tf = left_near ? ter : tel;
+            if (hn && hf) {
                 if (sp >= STACK) {
                     *err = RT_ERR_STACK;
                     return false;
                 }
-                stack[sp++] = far_c;
-                node = near_c;
-                continue;
+                st_code[sp] = fc;
+                st_te[sp] = tf;
+                sp++;
             }
-            int kind = b >> 16;
-            int count = b & 0xFFFF;
-            int first = ~a;
-            if (kind != LEAF_LIST && !box_hit(lo, hi, o, inv, tmin, closest)) break;
-            if (kind == LEAF_ENTS) {
+            code = hn ? nc : (hf ? fc : kNone);
+        }
+        // A leaf (or nothing): primitives in order.
+        if (code != kNone) {
+            int v = ~code;
+            int first = v >> 5;
+            int kind = (v >> 3) & 3;
+            int count = (v & 7) + 1;
+            code = kNone;
+            if (kind == LEAF_ENT1) {
+                Entity en = s.entities[first];
+                if (en.kind == ENT_MESH) {   // Mesh.Hit -> its BVH root (box test) or flat list
+                    if (en.index >= 0) {
+                        if (cnt) cnt->nodes++;
+                        float4 lo = __ldg(s.ent_box + 2 * first), hi = __ldg(s.ent_box + 2 * first + 1);
+                        float te;
+                        if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
+                            code = en.index;
+                            continue;
+                        }
+                    } else {
+                        code = en.index;   // <= 4 triangles: HittableList, no box test
+                        continue;
+                    }
+                } else {
+                    if (cnt) cnt->others++;
+                    Hit h;
+                    if (entity_test(s, first, o, d, tmin, closest, h)) {
+                        best = h;
+                        closest = h.t;
+                        if (ANY) return true;
+                    }
+                }
+            } else if (kind == LEAF_ENTS) {   // top-level fat leaf: entities in order
                 if (sp + count > STACK) {
                     *err = RT_ERR_STACK;
                     return false;
                 }
-                for (int i = count - 1; i >= 0; --i) stack[sp++] = ~s.top_items[first + i];
-                break;
-            }
-            for (int i = 0; i < count; i++) {
-                float t, u, v;
-                if (cnt) cnt->tris++;
-                if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, v)) {
-                    best = Hit{t, u, v, HIT_TRI, first + i};
-                    closest = t;
-                    if (ANY) return true;
+                for (int i = count - 1; i >= 0; --i) {
+                    st_code[sp] = leaf_code(s.top_items[first + i], LEAF_ENT1, 1);
+                    st_te[sp] = -kInf;
+                    sp++;
+                }
+            } else {   // triangle leaf (or a mesh's flat list)
+                for (int i = 0; i < count; i++) {
+                    float t, u, vv;
+                    if (cnt) cnt->tris++;
+                    if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, vv)) {
+                        best = Hit{t, u, vv, HIT_TRI, first + i};
+                        closest = t;
+                        if (ANY) return true;
+                    }
                 }
             }
-            break;
         }
+        // Pop the next entry the current closest t does not prune.
+        while (sp > 0) {
+            --sp;
+            if (!(st_te[sp] > closest)) {
+                code = st_code[sp];
+                break;
+            }
+        }
+        if (code == kNone) return true;
     }
-    return true;
 }
 
 // Surface record of an accepted hit (Core/HitRecord.cs fields on the path).
@@ -1044,7 +1086,7 @@ RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
     if (l.type == LIGHT_GEOM_MESH) {   // ray cast against the emitter mesh alone
         Hit h;
         int err = 0;
-        traverse<false, 64>(s, p, wi, kEps, kInf, h, nullptr, &err, l.mesh_root);
+        traverse<false, 64>(s, p, wi, kEps, kInf, h, nullptr, &err, true, l.mesh_root);
         if (err || h.kind == HIT_NONE) return 0.0f;
         const float4* tp = s.tris + 3 * h.slot;
         V3 n = v3(__ldg(tp).w, __ldg(tp + 1).w, __ldg(tp + 2).w);
@@ -1097,7 +1139,7 @@ __device__ __forceinline__ V3 shadow_transmittance(const SceneView& s, int opaqu
     Hit h;
     TravCounters* tc = cnt ? &cnt->shadow : nullptr;
     if (cnt) cnt->shadow_rays++;
-    if (opaque_scene) {
+    if (opaque_scene && !cnt) {   // the counting build walks like ShadowRay.Transmittance
         traverse<true, STACK>(s, o, d, tmin, tmax, h, tc, err);
         return h.kind == HIT_NONE ? v3(1.0f) : v3(0.0f);
     }

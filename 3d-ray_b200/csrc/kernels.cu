@@ -733,12 +733,13 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     const rt::HostScene& h = sc->host;
     rt::SceneView& v = sc->view;
     int r = RT_OK;
-    r = r ? r : upload(sc, h.nodes, &v.nodes);
+    r = r ? r : upload(sc, h.cnodes, &v.cnodes);
     r = r ? r : upload(sc, h.top_items, &v.top_items);
     r = r ? r : upload(sc, h.tris, &v.tris);
     r = r ? r : upload(sc, h.tri_entity, &v.tri_entity);
     r = r ? r : upload(sc, h.tri_local, &v.tri_local);
     r = r ? r : upload(sc, h.entities, &v.entities);
+    r = r ? r : upload(sc, h.ent_box, &v.ent_box);
     r = r ? r : upload(sc, h.quads, &v.quads);
     r = r ? r : upload(sc, h.spheres, &v.spheres);
     r = r ? r : upload(sc, h.materials, &v.materials);
@@ -752,7 +753,8 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
         return r;
     }
     v.num_lights = (int)h.lights.size();
-    v.top_root = h.top_root;
+    v.top_is_bvh = h.top_is_bvh;
+    v.top_root = h.top_root_code;
     v.num_top_items = (int)h.top_items.size();
     v.has_medium = h.has_medium;
     v.sigma_a = h.sigma_a;

@@ -24,7 +24,17 @@
 
 namespace rt {
 
-enum : int { LEAF_TRIS = 0, LEAF_ENTS = 1, LEAF_LIST = 2 };
+enum : int { LEAF_TRIS = 0, LEAF_ENTS = 1, LEAF_LIST = 2, LEAF_ENT1 = 3 };
+
+// Traversal layout (what the kernels read): one 64-byte record per interior
+// node holding both children's boxes, so a single fetch tests two boxes.
+//   (lmin.xyz, lcode) (lmax.xyz, rcode) (rmin.xyz, axis) (rmax.xyz, -)
+// A child code >= 0 is an interior record index; a negative code is a leaf:
+//   ~code = first << 5 | kind << 3 | (count - 1)
+// kind LEAF_TRIS / LEAF_LIST: triangles [first, first+count); LEAF_ENTS:
+// entity ids top_items[first .. first+count); LEAF_ENT1: the single entity
+// `first` (traversal-stack entries for pending top-level leaf items).
+RT_HD int leaf_code(int first, int kind, int count) { return ~((first << 5) | (kind << 3) | (count - 1)); }
 enum : int { ENT_QUAD = 0, ENT_SPHERE = 1, ENT_MESH = 2 };
 enum : int { ENT_BACKFACE_CULLED = 1 };
 
@@ -37,7 +47,7 @@ struct Entity {
     int kind;
     int material;
     int flags;
-    int index;   // quad / sphere index, or the mesh root node
+    int index;   // quad / sphere index, or the mesh root child code
 };
 
 struct QuadData {   // Geometry/Quad.cs:26-40 precomputed constants
@@ -85,7 +95,7 @@ struct Light {
     int quad;            // geometry-quad light: quad index
     int mesh_first;      // geometry-mesh light: first triangle in light_tris (source order)
     int mesh_count;
-    int mesh_root;       // mesh BVH root node (PdfSolidAngle ray cast)
+    int mesh_root;       // mesh BVH root child code (PdfSolidAngle ray cast)
     int mesh_entity;
     float inv_sqrt;
     float rep_area;      // ISamplable.SurfaceArea
@@ -107,12 +117,13 @@ struct Camera {
 };
 
 struct SceneView {
-    const NodeF* nodes;
+    const float4* cnodes;       // 4 float4 per interior node (child-box layout)
     const int* top_items;
     const float4* tris;
     const int* tri_entity;
     const int* tri_local;
     const Entity* entities;
+    const float4* ent_box;      // 2 per entity: the entity's AABB (a mesh's root box)
     const QuadData* quads;
     const SphereData* spheres;
     const Material* materials;
@@ -122,7 +133,8 @@ struct SceneView {
     const float* lut_e;         // 32 x 32, mu-major
     const float* lut_eavg;      // 32
     int num_lights;
-    int top_root;               // root node of the top-level BVH, or -1 for a flat list
+    int top_is_bvh;             // 0: the world is a flat list of top_items
+    int top_root;               // child code of the top-level root (top_is_bvh only)
     int num_top_items;          // flat list: entity count
     int has_medium;
     V3 sigma_a, sigma_s, sigma_t;

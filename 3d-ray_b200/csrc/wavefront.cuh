@@ -244,7 +244,9 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
             key = a.key_base[a.reqs[req].scene] + s.entities[ent].material;
         }
         a.P.keys[i] = key;
-        atomicAdd(&a.ctl->hist[key], 1);
+        // one atomic per distinct key in the warp (__match_any_sync groups lanes)
+        unsigned grp = __match_any_sync(__activemask(), key);
+        if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&a.ctl->hist[key], __popc(grp));
     }
 }
 
@@ -270,8 +272,15 @@ __global__ void k_wf_scatter(WfArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
     if (!(fbits(a.P.d[i].w) & PF_ALIVE)) return;
-    int pos = atomicAdd(&a.ctl->hist[a.P.keys[i]], 1);
-    a.P.order[pos] = i;
+    int key = a.P.keys[i];
+    unsigned grp = __match_any_sync(__activemask(), key);
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(grp) - 1;
+    int rank = __popc(grp & ((1u << lane) - 1u));
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&a.ctl->hist[key], __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    a.P.order[base + rank] = i;
 }
 
 // Shadow sink of the wavefront: queue the ray with its contribution.

@@ -500,6 +500,10 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
         }
         sc.entities.push_back(en);
     }
+    for (int e = 0; e < ne; e++) {
+        sc.ent_box.push_back(float4{ent_box[e].mn.x, ent_box[e].mn.y, ent_box[e].mn.z, 0.0f});
+        sc.ent_box.push_back(float4{ent_box[e].mx.x, ent_box[e].mx.y, ent_box[e].mx.z, 0.0f});
+    }
     // --- top level (SceneLoader.cs:460-485): BVH above 4 objects, else a flat list
     sc.top_is_bvh = ne > 4;
     int top_depth = 0;
@@ -553,8 +557,47 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
         }
     }
     // Worst-case traversal stack: one far child per interior level of each
-    // tree, plus up to 3 pending entities of a top-level fat leaf.
+    // tree, plus up to 4 pending entities of a top-level fat leaf.
     sc.max_stack = top_depth + 4 + max_blas_depth + 1;
+    // --- child-box traversal layout
+    {
+        std::vector<int> cidx(sc.nodes.size(), -1);
+        int n_int = 0;
+        for (size_t i = 0; i < sc.nodes.size(); i++) {
+            int a;
+            std::memcpy(&a, &sc.nodes[i].lo[3], 4);
+            if (a >= 0) cidx[i] = n_int++;
+        }
+        auto code_of = [&](int node) {
+            int a, b;
+            std::memcpy(&a, &sc.nodes[node].lo[3], 4);
+            std::memcpy(&b, &sc.nodes[node].hi[3], 4);
+            if (a >= 0) return cidx[node];
+            return leaf_code(~a, b >> 16, b & 0xFFFF);
+        };
+        sc.cnodes.resize((size_t)n_int * 4);
+        for (size_t i = 0; i < sc.nodes.size(); i++) {
+            if (cidx[i] < 0) continue;
+            int a, b;
+            std::memcpy(&a, &sc.nodes[i].lo[3], 4);
+            std::memcpy(&b, &sc.nodes[i].hi[3], 4);
+            int l = a, r = b & 0x3FFFFFFF, axis = (int)((unsigned)b >> 30);
+            const NodeF& L = sc.nodes[l];
+            const NodeF& R = sc.nodes[r];
+            int lc = code_of(l), rc = code_of(r);
+            float lcf, rcf, axf, zero = 0.0f;
+            std::memcpy(&lcf, &lc, 4);
+            std::memcpy(&rcf, &rc, 4);
+            std::memcpy(&axf, &axis, 4);
+            float4* c = &sc.cnodes[(size_t)cidx[i] * 4];
+            c[0] = float4{L.lo[0], L.lo[1], L.lo[2], lcf};
+            c[1] = float4{L.hi[0], L.hi[1], L.hi[2], rcf};
+            c[2] = float4{R.lo[0], R.lo[1], R.lo[2], axf};
+            c[3] = float4{R.hi[0], R.hi[1], R.hi[2], zero};
+        }
+        if (sc.top_is_bvh) sc.top_root_code = code_of(sc.top_root);
+        for (int e : mesh_ids) sc.entities[e].index = code_of(sc.entities[e].index);
+    }
     // --- explicit lights (SceneLoader.cs:446-458)
     for (int i = 0; i < w->num_lights; i++) {
         const RtLightDesc& d = w->lights[i];
@@ -623,7 +666,7 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             l.rep_area = sc.quads[l.quad].area;
         } else if (d.kind == RT_ENT_MESH) {
             l.type = LIGHT_GEOM_MESH;
-            l.mesh_root = sc.entities[e].index;
+            l.mesh_root = sc.entities[e].index;   // child code (after the layout pass)
             l.mesh_entity = e;
             l.mesh_first = (int)sc.light_tris.size();
             l.mesh_count = (int)d.count;

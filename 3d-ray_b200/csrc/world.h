@@ -14,12 +14,14 @@
 namespace rt {
 
 struct HostScene {
-    std::vector<NodeF> nodes;
+    std::vector<NodeF> nodes;      // build layout (pre-order), kept for export and tests
+    std::vector<float4> cnodes;    // traversal layout: 4 float4 per interior node
     std::vector<int> top_items;
     std::vector<float4> tris;      // 3 per triangle
     std::vector<int> tri_entity;
     std::vector<int> tri_local;
     std::vector<Entity> entities;
+    std::vector<float4> ent_box;   // 2 per entity
     std::vector<QuadData> quads;
     std::vector<SphereData> spheres;
     std::vector<Material> materials;
@@ -28,7 +30,8 @@ struct HostScene {
     std::vector<int> emitter_light;
     std::vector<float> lut_e, lut_eavg;
     RtCameraDesc camera{};
-    int top_root = -1;
+    int top_root = -1;             // build layout
+    int top_root_code = 0;         // traversal layout (top_is_bvh only)
     int top_is_bvh = 0;
     int max_stack = 0;
     int rr_min_bounces = 3;
