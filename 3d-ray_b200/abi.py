@@ -23,6 +23,15 @@ ERRORS = {-1: "RT_ERR_INVALID_ARG", -2: "RT_ERR_OOM", -3: "RT_ERR_CUDA", -4: "RT
 
 KERNEL_MEGAKERNEL = 0
 KERNEL_WAVEFRONT = 1
+
+# Differentiable parameter vector (include/rt3d.h, RT_ADJ_*): 16 slots per
+# material, then the medium's sigma_a[3], sigma_s[3].
+ADJ_PER_MATERIAL = 16
+ADJ_GLOBAL = 6
+ADJ_SLOTS = {"base_color": 0, "radiance": 0, "roughness": 3, "metallic": 4, "specular": 5, "specular_tint": 6,
+             "sheen": 7, "sheen_tint": 8, "clearcoat": 9, "spec_trans": 10, "anisotropic": 11, "absorption": 12}
+ADJ_MEDIUM_SIGMA_A = 0
+ADJ_MEDIUM_SIGMA_S = 3
 ADJ_PARAMS_PER_MATERIAL = 12
 
 F3 = C.c_float * 3
@@ -246,8 +255,9 @@ def load(path: str | None = None):
         "rt_render_device_noalloc": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtStats)]),
         "rt_render_batch": (C.c_int, [P, C.c_int32, P, C.c_int32, C.POINTER(RtRenderParams), P,
                                       C.POINTER(RtStats)]),
-        "rt_adjoint": (C.c_int, [P, C.POINTER(RtRenderParams), P, P, C.POINTER(RtStats)]),
+        "rt_adjoint": (C.c_int, [P, C.POINTER(RtRenderParams), P, P, P, C.c_int32, C.POINTER(RtStats)]),
         "rt_autotune": (C.c_int, [P, C.POINTER(RtRenderParams), C.POINTER(RtRenderParams)]),
+        "rt_scene_get_params": (C.c_int, [P, P, C.c_int32]),
         "rt_scene_set_params": (C.c_int, [P, P, C.c_int32]),
         "rt_trace_closest": (C.c_int, [P, P, C.c_int64, C.c_float, C.c_float, P]),
         "rt_trace_any": (C.c_int, [P, P, C.c_int64, P]),

@@ -691,9 +691,10 @@ enum : int { LOBE_DIFFUSE = 0, LOBE_SPECULAR, LOBE_TRANSMISSION, LOBE_SHEEN, LOB
 RT_D bool any_nonfinite(V3 a) { return !isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z); }
 
 // ScatterInternal (:1176-1248) with the lobe samplers (:1263-1709). ray_dir is
-// the incoming ray direction; V = normalize(-ray_dir).
+// the incoming ray direction; V = normalize(-ray_dir). When a reflection lobe
+// fails, *tried (if given) receives the direction it drew.
 RT_D bool bsdf_scatter(const SceneView& s, const Material& m, const Surface& rec, V3 ray_dir, float relative_eta,
-                       Sampler& rng, V3& att, V3& dir, int& lobe) {
+                       Sampler& rng, V3& att, V3& dir, int& lobe, V3* tried = nullptr) {
     V3 bc = m.base;
     V3 N = rec.n;
     V3 V = normalize(-ray_dir);
@@ -730,6 +731,7 @@ RT_D bool bsdf_scatter(const SceneView& s, const Material& m, const Surface& rec
             att = v3(0.0f);
             dir = N;
             ok = false;
+            if (tried) *tried = L;
         } else {
             dir = L;
             float vdh = fmaxf(dot(V, H), 1e-4f);
@@ -858,6 +860,7 @@ struct BsdfSample {
     int transition;            // 0 none, 1 enter, 2 exit
     int has_next_absorption;
     V3 next_absorption;
+    V3 tried;                  // a null sample: the direction its lobe drew
 };
 
 // Sample (:893-997). Returns false for a null sample.
@@ -867,7 +870,8 @@ RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec,
     int lobe = -1;
     out.transition = 0;
     out.has_next_absorption = 0;
-    bool ok = bsdf_scatter(s, m, rec, -V, relative_eta, rng, att, wo, lobe);
+    out.tried = rec.n;
+    bool ok = bsdf_scatter(s, m, rec, -V, relative_eta, rng, att, wo, lobe, &out.tried);
     out.lobe = lobe;
     if (!ok) return false;
     float ndwo = dot(rec.n, wo);
@@ -904,7 +908,10 @@ RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec,
         out.is_delta = 1;
         return true;
     }
-    if (ndwo <= 0.0f) return false;
+    if (ndwo <= 0.0f) {
+        out.tried = wo;
+        return false;
+    }
     bool nd_spec = lobe == LOBE_SPECULAR && m.alpha <= kDeltaAlpha;
     bool nd_coat = lobe == LOBE_CLEARCOAT && m.cc_alpha <= kDeltaAlpha;
     if (nd_spec || nd_coat) {

@@ -162,7 +162,8 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
             LightSample ls = light_sample(s, l, rec.p, rec.n, si, ps.rng);
             if (ls.occluded || !ls.has_ray) continue;
             V3 brdf = bsdf_eval_direct(s, m, rec, ls.dir, view, rec.n);
-            brdf = brdf * (view_term * shadow_terminator(rec.n, rec.n, ls.dir));
+            float term = view_term * shadow_terminator(rec.n, rec.n, ls.dir);
+            brdf = brdf * term;
             if (is_zero(brdf)) {
                 sink.skipped(ls.ray_o, ls.dir, ls.ray_tmax);
                 continue;
@@ -179,6 +180,7 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
             }
             V3 c = ps.w * (wgt * ls.color * brdf * tr_m);
             sink.shadow(ps, ls.ray_o, ls.dir, ls.ray_tmax, c, to_la);
+            sink.nee_surface(ps, li, m, rec, ls.dir, view, term, ps.w * (wgt * ls.color), ls.dist, tr_m, to_la);
         }
     }
 }
@@ -202,6 +204,7 @@ RT_D void nee_medium(const SceneView& s, const RenderConst& rc, PathState& ps, V
             }
             V3 c = ps.w * (wgt * ls.color * ph * tr_m);
             sink.shadow(ps, ls.ray_o, ls.dir, ls.ray_tmax, c, to_la);
+            sink.nee_medium(ps, li, ls.dist, to_la);
         }
     }
 }
@@ -223,6 +226,29 @@ RT_D bool russian_roulette(const RenderConst& rc, int depth, V3& att, V3& next_b
 
 RT_D V3 bl_factor(V3 sigma, float t) { return beer_lambert(v3(1.0f), sigma, t); }
 
+// Adjoint hooks. shade_vertex reports every factor that multiplies the path
+// weight and every term it adds, so that the path-replay adjoint can run the
+// same code; the forward sinks inherit these empty versions, which compile
+// away.
+enum : int { SEG_ABSORPTION = 0, SEG_MEDIUM_PASS = 1, SEG_MEDIUM_SCATTER = 2 };
+enum : int { SCATTER_SAMPLED = 0, SCATTER_DELTA = 1, SCATTER_LEGACY = 2 };
+struct NoAdjoint {
+    // ps.w is about to be multiplied by the factors of a segment of length t:
+    // interior Beer-Lambert (all modes but SEG_MEDIUM_PASS) and the medium.
+    RT_D void segment(const PathState&, float, int) {}
+    // The interior absorption now belongs to material `mat` (-1: none).
+    RT_D void interior(int) {}
+    // An emitted-radiance term ps.w * we was just added.
+    RT_D void emission(const PathState&, int, V3, int) {}
+    // A surface NEE sample: the term coef * brdf * term * tr_m * tr went through shadow().
+    RT_D void nee_surface(const PathState&, int, const Material&, const Surface&, V3, V3, float, V3, float, V3,
+                          int) {}
+    RT_D void nee_medium(const PathState&, int, float, int) {}
+    // The vertex attenuation: att_pre before Russian roulette, att after. For
+    // the legacy path, the lobe and direction of the null sample before it.
+    RT_D void scatter(const PathState&, const Material&, const Surface&, V3, V3, int, int, float, V3, V3, int, V3) {}
+};
+
 // One vertex of TraceRay given the closest hit of the current ray: the
 // volumetric branch (Renderer.cs:1704-1782), ShadeSurface (:1008-1228) and
 // ShadeSampleBounce (:1235-1383). Returns true when the path continues with
@@ -239,6 +265,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         bool sc = medium_sample(s, tmax, ps.rng, tmed, mb);
         if (sc) {
             V3 p = ps.o + ps.d * tmed;
+            sink.segment(ps, tmed, SEG_MEDIUM_SCATTER);
             ps.w = ps.w * bl_factor(ps.cur_abs, tmed) * mb;
             nee_medium(s, rc, ps, p, ps.d, sink);
             V3 mthr = ps.beta * mb;
@@ -265,18 +292,22 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
             ps.depth -= 1;
             return path_alive(ps);
         }
+        sink.segment(ps, tmax, SEG_MEDIUM_PASS);
         ps.w = ps.w * mb;
         beta_s = ps.beta * mb;
     }
     if (!hit) return false;   // black flat sky: SampleSky returns 0
+    sink.segment(ps, h.t, SEG_ABSORPTION);
     ps.w = ps.w * bl_factor(ps.cur_abs, h.t);
     Surface rec = make_surface(s, h, ps.o, ps.d);
     const Material& m = s.materials[rec.material];
     int to_la = ps.clamp_mode;
     if (m.type != 0) {   // Emissive: Emit (front face only), no NEE, no scatter
-        if (rec.front && (m.emission.x > 0.0f || m.emission.y > 0.0f || m.emission.z > 0.0f))
-            ps.add(ps.w * weight_emission(s, rc, m.emission, rec.material, ps.o, ps.d, ps.prev_pdf, ps.prev_delta),
-                   to_la);
+        if (rec.front && (m.emission.x > 0.0f || m.emission.y > 0.0f || m.emission.z > 0.0f)) {
+            V3 we = weight_emission(s, rc, m.emission, rec.material, ps.o, ps.d, ps.prev_pdf, ps.prev_delta);
+            ps.add(ps.w * we, to_la);
+            sink.emission(ps, rec.material, we, to_la);
+        }
         return false;
     }
     V3 view = normalize(-ps.d);
@@ -297,13 +328,19 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
             att = bs.f * a / bs.pdf;
         }
         next_beta = beta_s * att;
+        V3 att_pre = att;
         if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
+        sink.scatter(ps, m, rec, view, bs.wo, bs.lobe, bs.is_delta ? SCATTER_DELTA : SCATTER_SAMPLED, bs.pdf,
+                     att_pre, att, -1, bs.wo);
         V3 off = dot(bs.wo, rec.n) >= 0.0f ? rec.n : -rec.n;
         next_o = offset_origin(rec.p, off);
         next_d = bs.wo;
         next_pdf = bs.is_delta ? 0.0f : bs.pdf;
         next_delta = bs.is_delta;
-        if (bs.has_next_absorption) ps.cur_abs = bs.next_absorption;
+        if (bs.has_next_absorption) {
+            ps.cur_abs = bs.next_absorption;
+            sink.interior(near_zero(bs.next_absorption) ? -1 : rec.material);
+        }
         if (rc.dielectrics && bs.transition == 1) ps.iors.push(dielectric ? m.ior_raw : ps.iors.top());
         if (rc.dielectrics && bs.transition == 2) ps.iors.pop();
     } else {   // Sample returned null: the legacy Scatter path (:1127-1225)
@@ -311,7 +348,9 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         int lobe;
         if (!bsdf_scatter(s, m, rec, ps.d, rel_eta, ps.rng, att, sdir, lobe)) return false;
         next_beta = beta_s * att;
+        V3 att_pre = att;
         if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
+        sink.scatter(ps, m, rec, view, sdir, lobe, SCATTER_LEGACY, 1.0f, att_pre, att, bs.lobe, bs.tried);
         next_o = rec.p;
         next_d = sdir;
         next_pdf = 0.0f;
@@ -341,7 +380,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
 
 // Shadow sink of the megakernel: traces the shadow ray at once.
 template <int STACK>
-struct InlineShadows {
+struct InlineShadows : NoAdjoint {
     const SceneView* s;
     int opaque;
     Counters* cnt;
@@ -366,7 +405,7 @@ __device__ V3 trace_sample(const SceneView& s, const RenderConst& rc, int px, in
     if (!COUNT) cnt = nullptr;
     PathState ps;
     path_init(ps, rc, px, py, sample_index);
-    InlineShadows<STACK> sink{&s, rc.opaque, cnt, err};
+    InlineShadows<STACK> sink{{}, &s, rc.opaque, cnt, err};
     while (path_alive(ps)) {
         Hit h;
         if (COUNT) cnt->closest_rays++;

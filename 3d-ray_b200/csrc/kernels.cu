@@ -3,12 +3,14 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/rt3d.h"
+#include "adjoint.cuh"
 #include "integrator.cuh"
 #include "wavefront.cuh"
 #include "world.h"
@@ -63,6 +65,12 @@ struct RtScene {
     int* d_err = nullptr;
     int tuned = 0;                 // rt_autotune ran: use the fields below
     int tuned_slots = 0, tuned_block = 0, tuned_sort = 0;
+    // Copy of the world description: rt_scene_set_params rebuilds from it.
+    std::vector<RtMaterialDesc> w_materials;
+    std::vector<RtEntityDesc> w_entities;
+    std::vector<float> w_tris;
+    std::vector<RtLightDesc> w_lights;
+    RtWorldDesc w{};
 };
 
 namespace {
@@ -144,6 +152,113 @@ __global__ void k_resolve(const float* partial, int nchunks, int ww, int wh, int
         for (int k = 1; k < nchunks; k++) a += partial[(size_t)k * 3 * plane + (size_t)c * plane + i];
         film[c * fplane + fi] = a / (float)spp;
     }
+}
+
+// Path-replay adjoint: one thread per (pixel, sample) work item, samples
+// outermost, grid-stride. Gradients gather per thread (when the parameter
+// vector fits kAdjLocal) or in shared memory per block, and go to the global
+// double accumulators once per block.
+struct AdjArgs {
+    int x0, y0, ww, wh, W, H, spp, spp0;
+    const float* dimg;     // 3*H*W planar dLoss/dfilm
+    const float* params;   // raw parameter vector
+    const unsigned* mmask; // per material slot masks
+    unsigned gmask;        // global slot mask
+    double* grad;          // accumulators, nparams
+    int nparams;
+    int medium_base;
+    int use_shared;
+    int use_local;
+};
+
+template <int STACK>
+__global__ void __launch_bounds__(kBlock) k_adjoint(rt::SceneView s, rt::RenderConst rc, AdjArgs a, int* err) {
+    extern __shared__ float sacc[];
+    if (a.use_shared)
+        for (int i = threadIdx.x; i < a.nparams; i += blockDim.x) sacc[i] = 0.0f;
+    __syncthreads();
+    float loc[rt::kAdjLocal];
+    if (a.use_local)
+        for (int i = 0; i < a.nparams; i++) loc[i] = 0.0f;
+    long long npix = (long long)a.ww * a.wh;
+    long long total = npix * a.spp;
+    size_t plane = (size_t)a.W * a.H;
+    float inv_spp = 1.0f / (float)a.spp;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int pix = (int)(idx % npix);
+        int si = (int)(idx / npix);
+        int px = a.x0 + pix % a.ww, py = a.y0 + pix / a.ww;
+        size_t fi = (size_t)py * a.W + px;
+        V3 delta = rt::v3(a.dimg[fi], a.dimg[plane + fi], a.dimg[2 * plane + fi]) * inv_spp;
+        if (rt::is_zero(delta)) continue;
+        uint32_t sidx = (uint32_t)(a.spp0 + si);
+        // primal pass
+        rt::PathState ps;
+        rt::path_init(ps, rc, px, py, sidx);
+        rt::InlineShadows<STACK> fwd{{}, &s, rc.opaque, nullptr, err};
+        while (rt::path_alive(ps)) {
+            rt::Hit h;
+            rt::traverse<false, STACK>(s, ps.o, ps.d, rt::kEps, rt::kInf, h, nullptr, err);
+            if (!rt::shade_vertex(s, rc, ps, h, fwd)) break;
+        }
+        // adjoints of the resolve (path_resolve)
+        rt::AdjointReplay<STACK> adj;
+        adj.s = &s;
+        adj.params = a.params;
+        adj.mmask = a.mmask;
+        adj.gmask = a.gmask;
+        adj.loc = a.use_local ? loc : nullptr;
+        adj.acc = a.use_shared ? sacc : nullptr;
+        adj.gacc = a.grad;
+        adj.medium_base = a.medium_base;
+        adj.opaque = rc.opaque;
+        adj.err = err;
+        adj.abs_mat = -1;
+        adj.sh_added = 0;
+        adj.sh_n = 0;
+        V3 A = ps.lp, X = rt::v3(0.0f), C = rt::v3(0.0f);
+        if (ps.clamp_mode) {
+            X = ps.att0 * rt::sanitize(ps.la);
+            C = rt::clamp_lum(X, rc.ind_max);
+            A = A + ps.pre * C;
+        }
+        adj.tot_a = A;
+        adj.tot_la = ps.la;
+        adj.g_a = rt::clamp_lum_vjp(A, rc.max_rad, delta);
+        adj.g_la = rt::v3(0.0f);
+        adj.g_att0 = rt::v3(0.0f);
+        if (ps.clamp_mode) {
+            V3 gx = rt::clamp_lum_vjp(X, rc.ind_max, adj.g_a * ps.pre);
+            V3 sl = rt::sanitize(ps.la);
+            adj.g_att0 = gx * sl;
+            V3 pos = rt::v3(sl.x > 0.0f ? 1.0f : 0.0f, sl.y > 0.0f ? 1.0f : 0.0f, sl.z > 0.0f ? 1.0f : 0.0f);
+            adj.g_la = gx * ps.att0 * pos;
+        }
+        if (rt::is_zero(adj.g_a)) continue;
+        // replay
+        rt::path_init(ps, rc, px, py, sidx);
+        while (rt::path_alive(ps)) {
+            rt::Hit h;
+            rt::traverse<false, STACK>(s, ps.o, ps.d, rt::kEps, rt::kInf, h, nullptr, err);
+            if (!rt::shade_vertex(s, rc, ps, h, adj)) break;
+        }
+    }
+    if (a.use_local) {   // warp sums of the per-thread accumulators
+        int lane = threadIdx.x & 31;
+        for (int i = 0; i < a.nparams; i++) {
+            float v = loc[i];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0 && v != 0.0f) {
+                if (a.use_shared) atomicAdd(sacc + i, v);
+                else atomicAdd(a.grad + i, (double)v);
+            }
+        }
+    }
+    __syncthreads();
+    if (a.use_shared)
+        for (int i = threadIdx.x; i < a.nparams; i += blockDim.x)
+            if (sacc[i] != 0.0f) atomicAdd(a.grad + i, (double)sacc[i]);
 }
 
 template <int STACK>
@@ -725,6 +840,19 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     auto* sc = new RtScene();
     std::string err;
     int rc = rt::build_world(world, sc->host, err);
+    if (rc == RT_OK) {
+        sc->w = *world;
+        sc->w_materials.assign(world->materials, world->materials + world->num_materials);
+        sc->w_entities.assign(world->entities, world->entities + world->num_entities);
+        if (world->num_tris > 0 && world->tri_verts)
+            sc->w_tris.assign(world->tri_verts, world->tri_verts + world->num_tris * 9);
+        if (world->num_lights > 0 && world->lights)
+            sc->w_lights.assign(world->lights, world->lights + world->num_lights);
+        sc->w.materials = sc->w_materials.data();
+        sc->w.entities = sc->w_entities.data();
+        sc->w.tri_verts = sc->w_tris.empty() ? nullptr : sc->w_tris.data();
+        sc->w.lights = sc->w_lights.empty() ? nullptr : sc->w_lights.data();
+    }
     if (rc != RT_OK) {
         delete sc;
         return fail(rc, err);
@@ -1108,11 +1236,251 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
     return RT_OK;
 }
 
-int rt_adjoint(RtScene*, const RtRenderParams*, const float*, float*, RtStats*) {
-    return fail(RT_ERR_UNSUPPORTED, "adjoint not built yet");
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Differentiable parameter vector and the path-replay adjoint.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kPerMat = RT_ADJ_PARAMS_PER_MATERIAL;
+static_assert(kPerMat == rt::kAdjPerMat, "slot layout");
+
+int param_count(const RtScene* sc) { return (int)sc->w_materials.size() * kPerMat + RT_ADJ_GLOBAL_PARAMS; }
+
+void get_params(const RtScene* sc, float* out) {
+    int nm = (int)sc->w_materials.size();
+    std::fill(out, out + param_count(sc), 0.0f);
+    for (int i = 0; i < nm; i++) {
+        const RtMaterialDesc& d = sc->w_materials[i];
+        const rt::Material& m = sc->host.materials[i];
+        float* p = out + i * kPerMat;
+        if (d.type == RT_MAT_EMISSIVE) {
+            p[RT_ADJ_RADIANCE + 0] = m.emission.x;
+            p[RT_ADJ_RADIANCE + 1] = m.emission.y;
+            p[RT_ADJ_RADIANCE + 2] = m.emission.z;
+            continue;
+        }
+        for (int c = 0; c < 3; c++) p[RT_ADJ_BASE_COLOR + c] = d.base_color[c];
+        p[RT_ADJ_ROUGHNESS] = d.roughness;
+        p[RT_ADJ_METALLIC] = d.metallic;
+        p[RT_ADJ_SPECULAR] = d.specular;
+        p[RT_ADJ_SPECULAR_TINT] = d.specular_tint;
+        p[RT_ADJ_SHEEN] = d.sheen;
+        p[RT_ADJ_SHEEN_TINT] = d.sheen_tint;
+        p[RT_ADJ_CLEARCOAT] = d.clearcoat;
+        p[RT_ADJ_SPEC_TRANS] = d.spec_trans;
+        p[RT_ADJ_ANISOTROPIC] = d.anisotropic;
+        p[RT_ADJ_ABSORPTION + 0] = m.trans_sigma.x;
+        p[RT_ADJ_ABSORPTION + 1] = m.trans_sigma.y;
+        p[RT_ADJ_ABSORPTION + 2] = m.trans_sigma.z;
+    }
+    float* g = out + nm * kPerMat;
+    for (int c = 0; c < 3; c++) {
+        g[RT_ADJ_MEDIUM_SIGMA_A + c] = sc->w.medium.sigma_a[c];
+        g[RT_ADJ_MEDIUM_SIGMA_S + c] = sc->w.medium.sigma_s[c];
+    }
 }
 
-int rt_scene_set_params(RtScene*, const float*, int32_t) { return fail(RT_ERR_UNSUPPORTED, "adjoint not built yet"); }
+// Writes the vector into the stored world description. A slot equal to what
+// get_params reports leaves its description field untouched, so that
+// set(get()) is an exact no-op.
+void put_params(RtScene* sc, const float* in) {
+    int nm = (int)sc->w_materials.size();
+    for (int i = 0; i < nm; i++) {
+        RtMaterialDesc& d = sc->w_materials[i];
+        const rt::Material& m = sc->host.materials[i];
+        const float* p = in + i * kPerMat;
+        if (d.type == RT_MAT_EMISSIVE) {   // radiance = colour * intensity; intensity kept
+            float cur[3] = {m.emission.x, m.emission.y, m.emission.z};
+            if (p[0] == cur[0] && p[1] == cur[1] && p[2] == cur[2]) continue;
+            if (!(d.intensity > 0.0f)) {
+                d.intensity = 1.0f;
+                for (int c = 0; c < 3; c++) d.base_color[c] = p[c];
+            } else {
+                for (int c = 0; c < 3; c++)
+                    if (p[c] != cur[c]) d.base_color[c] = p[c] / d.intensity;
+            }
+            continue;
+        }
+        for (int c = 0; c < 3; c++) d.base_color[c] = p[RT_ADJ_BASE_COLOR + c];
+        d.roughness = p[RT_ADJ_ROUGHNESS];
+        d.metallic = p[RT_ADJ_METALLIC];
+        d.specular = p[RT_ADJ_SPECULAR];
+        d.specular_tint = p[RT_ADJ_SPECULAR_TINT];
+        d.sheen = p[RT_ADJ_SHEEN];
+        d.sheen_tint = p[RT_ADJ_SHEEN_TINT];
+        d.clearcoat = p[RT_ADJ_CLEARCOAT];
+        d.spec_trans = p[RT_ADJ_SPEC_TRANS];
+        d.anisotropic = p[RT_ADJ_ANISOTROPIC];
+        const float* sg = p + RT_ADJ_ABSORPTION;
+        if (sg[0] == m.trans_sigma.x && sg[1] == m.trans_sigma.y && sg[2] == m.trans_sigma.z) continue;
+        // transmission_color = exp(-sigma * depth) (ResolveTransmission, DisneyBsdf.cs:1039-1048)
+        if (!(d.has_transmission_color && d.transmission_depth > 0.0f)) {
+            d.has_transmission_color = 1;
+            d.transmission_depth = 1.0f;
+        }
+        for (int c = 0; c < 3; c++)
+            d.transmission_color[c] = std::exp(-std::fmax(sg[c], 0.0f) * d.transmission_depth);
+    }
+    const float* g = in + nm * kPerMat;
+    for (int c = 0; c < 3; c++) {
+        sc->w.medium.sigma_a[c] = g[RT_ADJ_MEDIUM_SIGMA_A + c];
+        sc->w.medium.sigma_s[c] = g[RT_ADJ_MEDIUM_SIGMA_S + c];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int rt_scene_get_params(const RtScene* sc, float* params, int32_t count) {
+    if (!sc || !params) return fail(RT_ERR_INVALID_ARG, "null argument");
+    if (count != param_count(sc))
+        return fail(RT_ERR_INVALID_ARG, "parameter vector needs " + std::to_string(param_count(sc)) + " floats");
+    get_params(sc, params);
+    return RT_OK;
+}
+
+int rt_scene_set_params(RtScene* sc, const float* params, int32_t count) {
+    if (!sc || !params) return fail(RT_ERR_INVALID_ARG, "null argument");
+    if (count != param_count(sc))
+        return fail(RT_ERR_INVALID_ARG, "parameter vector needs " + std::to_string(param_count(sc)) + " floats");
+    for (int32_t i = 0; i < count; i++)
+        if (!std::isfinite(params[i])) return fail(RT_ERR_INVALID_ARG, "non-finite parameter " + std::to_string(i));
+    std::lock_guard<std::mutex> lk(sc->mu);
+    std::vector<RtMaterialDesc> keep_m = sc->w_materials;
+    RtMediumDesc keep_med = sc->w.medium;
+    put_params(sc, params);
+    rt::HostScene h;
+    std::string err;
+    int rc = rt::build_world(&sc->w, h, err);
+    if (rc != RT_OK || h.materials.size() != sc->host.materials.size() || h.lights.size() != sc->host.lights.size()) {
+        sc->w_materials = keep_m;
+        sc->w.medium = keep_med;
+        return fail(rc != RT_OK ? rc : RT_ERR_INVALID_ARG, rc != RT_OK ? err : "parameter change altered the lights");
+    }
+    CUDA_TRY(cudaSetDevice(sc->device));
+    CUDA_TRY(cudaStreamSynchronize(sc->stream));
+    rt::SceneView& v = sc->view;
+    CUDA_TRY(cudaMemcpy(const_cast<rt::Material*>(v.materials), h.materials.data(),
+                        h.materials.size() * sizeof(rt::Material), cudaMemcpyHostToDevice));
+    if (!h.lights.empty())
+        CUDA_TRY(cudaMemcpy(const_cast<rt::Light*>(v.lights), h.lights.data(), h.lights.size() * sizeof(rt::Light),
+                            cudaMemcpyHostToDevice));
+    v.sigma_a = h.sigma_a;
+    v.sigma_s = h.sigma_s;
+    v.sigma_t = h.sigma_t;
+    v.hg_g = h.hg_g;
+    sc->opaque = 1;
+    sc->dielectrics = 0;
+    for (const rt::Material& m : h.materials) {
+        if (m.type == 0 && m.spec_trans_raw > 0.0f) {
+            sc->opaque = 0;
+            if (!m.thin_walled) sc->dielectrics = 1;
+        }
+    }
+    sc->host = std::move(h);
+    return RT_OK;
+}
+
+int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const uint8_t* mask, float* grad,
+               int32_t count, RtStats* st) {
+    if (!sc || !p || !dimg || !grad) return fail(RT_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(sc->mu);
+    auto t0 = std::chrono::steady_clock::now();
+    int rc_ = validate_params(sc, p);
+    if (rc_ != RT_OK) return rc_;
+    if (p->count_work) return fail(RT_ERR_INVALID_ARG, "count_work is not available in the adjoint");
+    int np = param_count(sc);
+    if (count != np) return fail(RT_ERR_INVALID_ARG, "gradient vector needs " + std::to_string(np) + " floats");
+    CUDA_TRY(cudaSetDevice(sc->device));
+    rt::RenderConst rcon = make_rc(sc, p, sc->host.camera);
+    int ww = p->window_w > 0 ? p->window_w : p->width;
+    int wh = p->window_h > 0 ? p->window_h : p->height;
+    size_t film = (size_t)3 * p->width * p->height;
+    std::vector<float> hp((size_t)np);
+    get_params(sc, hp.data());
+    int nm = (int)sc->w_materials.size();
+    std::vector<unsigned> hm((size_t)nm, 0u);
+    unsigned gm = 0u;
+    for (int i = 0; i < np; i++) {
+        if (mask && !mask[i]) continue;
+        if (i < nm * kPerMat) hm[(size_t)(i / kPerMat)] |= 1u << (i % kPerMat);
+        else gm |= 1u << (i - nm * kPerMat);
+    }
+    size_t bytes = (size_t)np * sizeof(double) + (size_t)np * sizeof(float) + film * sizeof(float) +
+                   (size_t)nm * sizeof(unsigned) + 256;
+    void* mem = nullptr;
+    if (cudaMalloc(&mem, bytes) != cudaSuccess) return fail(RT_ERR_OOM, "adjoint buffers");
+    char* base = static_cast<char*>(mem);
+    double* d_grad = reinterpret_cast<double*>(base);
+    float* d_params = reinterpret_cast<float*>(base + (size_t)np * sizeof(double));
+    float* d_img = d_params + np;
+    unsigned* d_mask = reinterpret_cast<unsigned*>(d_img + film);
+    int rc = RT_OK;
+    auto step = [&](cudaError_t e, const char* what) {
+        if (rc == RT_OK && e != cudaSuccess) rc = fail(RT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    step(cudaMemcpyAsync(d_img, dimg, film * sizeof(float), cudaMemcpyHostToDevice, sc->stream), "dL/dimage copy");
+    step(cudaMemcpyAsync(d_params, hp.data(), (size_t)np * sizeof(float), cudaMemcpyHostToDevice, sc->stream),
+         "parameter copy");
+    step(cudaMemcpyAsync(d_mask, hm.data(), (size_t)nm * sizeof(unsigned), cudaMemcpyHostToDevice, sc->stream),
+         "mask copy");
+    step(cudaMemsetAsync(d_grad, 0, (size_t)np * sizeof(double), sc->stream), "gradient clear");
+    step(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream), "error clear");
+    AdjArgs a;
+    a.x0 = p->pixel_x0;
+    a.y0 = p->pixel_y0;
+    a.ww = ww;
+    a.wh = wh;
+    a.W = p->width;
+    a.H = p->height;
+    a.spp = p->spp;
+    a.spp0 = p->spp_offset;
+    a.dimg = d_img;
+    a.params = d_params;
+    a.mmask = d_mask;
+    a.gmask = gm;
+    a.grad = d_grad;
+    a.nparams = np;
+    a.medium_base = nm * kPerMat;
+    size_t shmem = (size_t)np * sizeof(float);
+    a.use_shared = shmem <= 48 * 1024;
+    if (!a.use_shared) shmem = 0;
+    a.use_local = np <= rt::kAdjLocal;
+    long long total = (long long)ww * wh * p->spp;
+    long long blocks = std::min<long long>((total + kBlock - 1) / kBlock, 148LL * 16);
+    if (rc == RT_OK) {
+        step(cudaEventRecord(sc->ev0, sc->stream), "event");
+        k_adjoint<kStack><<<(unsigned)std::max<long long>(blocks, 1), kBlock, shmem, sc->stream>>>(sc->view, rcon, a,
+                                                                                                     sc->d_err);
+        step(cudaGetLastError(), "k_adjoint launch");
+        step(cudaEventRecord(sc->ev1, sc->stream), "event");
+    }
+    std::vector<double> hg((size_t)np, 0.0);
+    if (rc == RT_OK) {
+        step(cudaMemcpyAsync(hg.data(), d_grad, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, sc->stream),
+             "gradient copy");
+        step(cudaStreamSynchronize(sc->stream), "adjoint");
+    }
+    if (rc == RT_OK) rc = check_err(sc);
+    float ms = 0.0f;
+    if (rc == RT_OK) cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+    cudaFree(mem);
+    if (rc != RT_OK) return rc;
+    for (int i = 0; i < np; i++) grad[i] = (float)hg[(size_t)i];
+    if (st) {
+        *st = RtStats{};
+        st->kernel_ms = ms;
+        st->samples = (uint64_t)total;
+        st->kernel_launches = 1;
+        st->rr_min_bounces = rcon.rr_min_bounces;
+        st->rr_min_survival = rcon.rr_min_survival;
+        st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return RT_OK;
+}
 
 int rt_trace_closest(RtScene* sc, const float* rays, int64_t n, float tmin, float tmax, int32_t* hits) {
     if (!sc || !rays || !hits || n < 0) return fail(RT_ERR_INVALID_ARG, "null argument");

@@ -284,7 +284,7 @@ __global__ void k_wf_scatter(WfArgs a) {
 }
 
 // Shadow sink of the wavefront: queue the ray with its contribution.
-struct QueueShadows {
+struct QueueShadows : NoAdjoint {
     const WfArgs* a;
     int slot;
     int scene;
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
     h.v = hh.z;
     h.kind = packed == 0 ? HIT_NONE : ((unsigned)packed >> 30);
     h.slot = packed & 0x3FFFFFFF;
-    QueueShadows sink{&a, i, R.scene};
+    QueueShadows sink{{}, &a, i, R.scene};
     bool alive = shade_vertex(s, R.rc, ps, h, sink);
     wf_store(a, i, ps, wf_flags(ps, alive), req, pix);
     wf_store_media(a, i, R, ps);

@@ -298,15 +298,56 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
 int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* best);
 
 /* ---- differentiation ----------------------------------------------------- */
-/* Parameters the adjoint differentiates, per material (Disney) and per emitter:
- * base_color[3], roughness, metallic, specular, sheen, clearcoat, spec_trans,
- * emission[3] — 12 floats per material, in material order. */
-#define RT_ADJ_PARAMS_PER_MATERIAL 12
+/* The differentiable parameter vector of a scene: 16 floats per material, in
+ * material order, then 6 floats of the global medium. Total
+ * RT_ADJ_PARAMS_PER_MATERIAL * num_materials + RT_ADJ_GLOBAL_PARAMS.
+ * Disney material slots (the RtMaterialDesc fields, before the constructor's
+ * clamps; a clamped-out value has zero derivative): */
+#define RT_ADJ_BASE_COLOR      0   /* [3] baseColor                                   */
+#define RT_ADJ_ROUGHNESS       3
+#define RT_ADJ_METALLIC        4
+#define RT_ADJ_SPECULAR        5
+#define RT_ADJ_SPECULAR_TINT   6
+#define RT_ADJ_SHEEN           7
+#define RT_ADJ_SHEEN_TINT      8
+#define RT_ADJ_CLEARCOAT       9
+#define RT_ADJ_SPEC_TRANS     10
+#define RT_ADJ_ANISOTROPIC    11
+#define RT_ADJ_ABSORPTION     12   /* [3] interior Beer-Lambert sigma_a per unit length:
+                                      -ln(transmission_color) / transmission_depth     */
+/* Emissive material slots: */
+#define RT_ADJ_RADIANCE        0   /* [3] emitted radiance, colour * intensity         */
+#define RT_ADJ_PARAMS_PER_MATERIAL 16
+/* Global slots after the materials: homogeneous medium sigma_a[3], sigma_s[3]. */
+#define RT_ADJ_MEDIUM_SIGMA_A  0
+#define RT_ADJ_MEDIUM_SIGMA_S  3
+#define RT_ADJ_GLOBAL_PARAMS   6
+
+/* Path-replay adjoint. dL_dimage_planar is the host gradient of a scalar
+ * loss with respect to the 3*H*W planar HDR film that rt_render returns for
+ * the same params (same spp and spp_offset). Every sample is traced twice from
+ * its Sobol indices: a primal pass for the sample radiance, then a replay that
+ * accumulates the gradient; nothing is stored per bounce. Sampling decisions
+ * (directions, lobe choice, light samples, MIS weights, Russian roulette) are
+ * held fixed, with score terms for the two discrete events whose probability
+ * the reference's estimator keeps (a lobe weight divided by max(p, floor), and
+ * a null Sample followed by the legacy Scatter draw); geometry and visibility
+ * edges are not differentiated. Writes the gradient (float, host) in the
+ * parameter-vector layout above; count is that layout's length. mask (count
+ * bytes, or NULL for all) selects the slots to differentiate; unselected slots
+ * come back 0 and cost nothing (a material with no selected BSDF slot skips
+ * the dual-number BSDF evaluations). The megakernel form is used whatever
+ * params->kernel says; count_work must be 0. */
 int rt_adjoint(RtScene* scene, const RtRenderParams* params,
-               const float* dL_dimage_planar, float* dL_dparams, RtStats* stats);
-/* Overwrites the differentiable parameters of the scene's materials
- * (same 12-float layout as rt_adjoint's output). */
-int rt_scene_set_params(RtScene* scene, const float* params, int32_t num_materials);
+               const float* dL_dimage_planar, const uint8_t* mask,
+               float* dL_dparams, int32_t count, RtStats* stats);
+/* Reads / overwrites the parameter vector (count floats, layout above). Set
+ * rebuilds the scene's materials, lights and Russian-roulette classifier from
+ * the stored world description, exactly as rt_scene_create would from a world
+ * with those values; the BVH is untouched. A slot equal to what get reports
+ * leaves its field untouched, so set(get()) changes nothing. */
+int rt_scene_get_params(const RtScene* scene, float* params, int32_t count);
+int rt_scene_set_params(RtScene* scene, const float* params, int32_t count);
 
 /* ---- test-only entry points --------------------------------------------- */
 /* Ray in: origin[3], dir[3] (8 floats per ray, last two ignored).

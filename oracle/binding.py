@@ -36,6 +36,10 @@ def lib():
             ("or_sobol", C.c_float, [C.c_uint32, C.c_uint32, C.c_uint32]),
             ("or_sobol_batch", C.c_int, [P, P, P, C.c_int64, P]),
             ("or_energy_lut", C.c_int, [P, P]),
+            ("or_hg_eval", C.c_float, [C.c_float, P, P]),
+            ("or_hg_sample", C.c_float, [C.c_float, P, C.c_float, C.c_float, P]),
+            ("or_medium_transmittance", C.c_int, [P, C.c_float, P]),
+            ("or_medium_sample", C.c_int, [P, P, C.c_float, C.c_float, C.c_float, P, P]),
             ("or_scene_create", C.c_int, [P, C.POINTER(P)]),
             ("or_scene_destroy", C.c_int, [P]),
             ("or_scene_info", C.c_int, [P, P, P, P, P, P]),
@@ -64,6 +68,38 @@ def sobol(idx, dim, seed) -> np.ndarray:
     out = np.empty(idx.shape, np.float32)
     lib().or_sobol_batch(_p(idx), _p(dim), _p(seed), idx.size, _p(out))
     return out
+
+
+def hg_eval(g, wo, wi) -> float:
+    """HenyeyGreensteinPhase.Evaluate."""
+    a = np.ascontiguousarray(wo, np.float32)
+    b = np.ascontiguousarray(wi, np.float32)
+    return float(lib().or_hg_eval(g, _p(a), _p(b)))
+
+
+def hg_sample(g, wo, u1, u2):
+    """HenyeyGreensteinPhase.Sample for the uniform draws (u1, u2): (wi, pdf)."""
+    a = np.ascontiguousarray(wo, np.float32)
+    wi = np.empty(3, np.float32)
+    pdf = lib().or_hg_sample(g, _p(a), u1, u2, _p(wi))
+    return wi, float(pdf)
+
+
+def medium_transmittance(sigma_t, t) -> np.ndarray:
+    s = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma_t, np.float32), (3,)))
+    out = np.empty(3, np.float32)
+    lib().or_medium_transmittance(_p(s), t, _p(out))
+    return out
+
+
+def medium_sample(sigma_a, sigma_s, tmax, u_ch, u_d):
+    """HomogeneousMedium.Sample for the draws (u_ch, u_d): (scattered, t, beta)."""
+    sa = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma_a, np.float32), (3,)))
+    ss = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma_s, np.float32), (3,)))
+    t = np.zeros(1, np.float32)
+    beta = np.empty(3, np.float32)
+    sc = lib().or_medium_sample(_p(sa), _p(ss), tmax, u_ch, u_d, _p(t), _p(beta))
+    return bool(sc), float(t[0]), beta
 
 
 def energy_lut():

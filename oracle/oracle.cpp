@@ -1761,6 +1761,61 @@ struct IorStack {   // Volumetrics/IorStack.cs
     }
 };
 
+// ---------------------------------------------------------------------------
+// Homogeneous medium and Henyey-Greenstein phase (Volumetrics/), as free
+// functions of their parameters and uniform draws.
+// ---------------------------------------------------------------------------
+static V3 medium_transmittance(V3 sigma_t, float t) {   // HomogeneousMedium.Transmittance (:36-44)
+    float d = std::fmin(std::fmax(t, 0.0f), 1e30f);
+    return v3(std::exp(-sigma_t.x * d), std::exp(-sigma_t.y * d), std::exp(-sigma_t.z * d));
+}
+static float hg_evaluate(float g, V3 wo, V3 wi) {   // HenyeyGreensteinPhase.cs:23-30
+    float mu = dot(wo, wi);
+    float denom = 1.0f + g * g - 2.0f * g * mu;
+    return kInv4Pi * (1.0f - g * g) / (denom * std::sqrt(denom));
+}
+static V3 hg_draw(float g, V3 wo, float u1, float u2, float& pdf) {   // HenyeyGreensteinPhase.cs:32-54
+    float ct;
+    if (std::fabs(g) < 1e-3f) {
+        ct = 1.0f - 2.0f * u1;
+    } else {
+        float sqr = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
+        ct = (1.0f + g * g - sqr * sqr) / (2.0f * g);
+    }
+    float st = std::sqrt(std::fmax(0.0f, 1.0f - ct * ct));
+    float phi = 2.0f * kPi * u2;
+    V3 w = wo;
+    V3 a = std::fabs(w.x) > 0.9f ? v3(0, 1, 0) : v3(1, 0, 0);
+    V3 v = normalize(cross(w, a));
+    V3 u = cross(w, v);
+    V3 wi = st * std::cos(phi) * u + st * std::sin(phi) * v + ct * w;
+    wi = normalize(wi);
+    pdf = hg_evaluate(g, wo, wi);
+    return wi;
+}
+// HomogeneousMedium.Sample (:46-76): hero channel floor(3 u_ch), then the
+// distance draw (taken only when that channel's sigma_t is positive).
+template <class Draw>
+static bool medium_draw(V3 sigma_t, V3 sigma_s, float tmax, float u_ch, Draw draw, float& t, V3& beta) {
+    int ch = (int)(u_ch * 3.0f);
+    if (ch > 2) ch = 2;
+    float st = ch == 0 ? sigma_t.x : ch == 1 ? sigma_t.y : sigma_t.z;
+    if (st <= 0.0f) {
+        t = tmax;
+        beta = v3(1.0f);
+        return false;
+    }
+    float dist = -std::log(1.0f - draw()) / st;
+    bool scattered = dist < tmax;
+    t = scattered ? dist : tmax;
+    V3 tr = medium_transmittance(sigma_t, t);
+    V3 dens = scattered ? sigma_t * tr : tr;
+    float pdf = (dens.x + dens.y + dens.z) / 3.0f;
+    if (pdf < 1e-20f) pdf = 1.0f;
+    beta = scattered ? (tr * sigma_s / pdf) : (tr / pdf);
+    return scattered;
+}
+
 struct RenderCfg {
     int max_depth;
     float max_radiance, indirect_max;
@@ -1843,36 +1898,11 @@ struct Tracer {
         return result;
     }
 
-    V3 medium_tr(float t) const {   // HomogeneousMedium.Transmittance (:36-44)
-        float d = std::fmin(std::fmax(t, 0.0f), 1e30f);
-        return v3(std::exp(-sc.sigma_t.x * d), std::exp(-sc.sigma_t.y * d), std::exp(-sc.sigma_t.z * d));
-    }
-    float hg_eval(V3 wo, V3 wi) const {   // HenyeyGreensteinPhase.cs:23-30
-        float g = sc.hg_g;
-        float mu = dot(wo, wi);
-        float denom = 1.0f + g * g - 2.0f * g * mu;
-        return kInv4Pi * (1.0f - g * g) / (denom * std::sqrt(denom));
-    }
-    V3 hg_sample(V3 wo, float& pdf) const {   // HenyeyGreensteinPhase.cs:32-54
-        float g = sc.hg_g;
+    V3 medium_tr(float t) const { return medium_transmittance(sc.sigma_t, t); }
+    float hg_eval(V3 wo, V3 wi) const { return hg_evaluate(sc.hg_g, wo, wi); }
+    V3 hg_sample(V3 wo, float& pdf) const {
         float u1 = random_float(), u2 = random_float();
-        float ct;
-        if (std::fabs(g) < 1e-3f) {
-            ct = 1.0f - 2.0f * u1;
-        } else {
-            float sqr = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
-            ct = (1.0f + g * g - sqr * sqr) / (2.0f * g);
-        }
-        float st = std::sqrt(std::fmax(0.0f, 1.0f - ct * ct));
-        float phi = 2.0f * kPi * u2;
-        V3 w = wo;
-        V3 a = std::fabs(w.x) > 0.9f ? v3(0, 1, 0) : v3(1, 0, 0);
-        V3 v = normalize(cross(w, a));
-        V3 u = cross(w, v);
-        V3 wi = st * std::cos(phi) * u + st * std::sin(phi) * v + ct * w;
-        wi = normalize(wi);
-        pdf = hg_eval(wo, wi);
-        return wi;
+        return hg_draw(sc.hg_g, wo, u1, u2, pdf);
     }
     // ComputeDirectLightingMedium, strategy All (:2162-2203)
     V3 direct_lighting_medium(V3 p, V3 wo) const {
@@ -1902,23 +1932,8 @@ struct Tracer {
     }
     // HomogeneousMedium.Sample (:46-76)
     bool medium_sample(float tmax, float& t, V3& beta) const {
-        int ch = (int)(random_float() * 3.0f);
-        if (ch > 2) ch = 2;
-        float st = ch == 0 ? sc.sigma_t.x : ch == 1 ? sc.sigma_t.y : sc.sigma_t.z;
-        if (st <= 0.0f) {
-            t = tmax;
-            beta = v3(1.0f);
-            return false;
-        }
-        float dist = -std::log(1.0f - random_float()) / st;
-        bool scattered = dist < tmax;
-        t = scattered ? dist : tmax;
-        V3 tr = medium_tr(t);
-        V3 dens = scattered ? sc.sigma_t * tr : tr;
-        float pdf = (dens.x + dens.y + dens.z) / 3.0f;
-        if (pdf < 1e-20f) pdf = 1.0f;
-        beta = scattered ? (tr * sc.sigma_s / pdf) : (tr / pdf);
-        return scattered;
+        float u_ch = random_float();
+        return medium_draw(sc.sigma_t, sc.sigma_s, tmax, u_ch, [&] { return random_float(); }, t, beta);
     }
     static V3 beer_lambert(V3 rad, V3 sigma, float t) {   // :1791-1800
         if (sigma.x <= 0.0f && sigma.y <= 0.0f && sigma.z <= 0.0f) return rad;
@@ -2149,6 +2164,36 @@ float or_sobol(uint32_t idx, uint32_t dim, uint32_t seed) { return sobol_sample(
 int or_sobol_batch(const uint32_t* idx, const uint32_t* dim, const uint32_t* seed, int64_t n, float* out) {
     for (int64_t i = 0; i < n; i++) out[i] = sobol_sample(idx[i], dim[i], seed[i]);
     return 0;
+}
+
+// Medium and phase test entry points (VolumetricsTests.cs).
+float or_hg_eval(float g, const float* wo, const float* wi) {
+    return hg_evaluate(g, v3(wo[0], wo[1], wo[2]), v3(wi[0], wi[1], wi[2]));
+}
+float or_hg_sample(float g, const float* wo, float u1, float u2, float* wi) {
+    float pdf = 0.0f;
+    V3 r = hg_draw(g, v3(wo[0], wo[1], wo[2]), u1, u2, pdf);
+    wi[0] = r.x;
+    wi[1] = r.y;
+    wi[2] = r.z;
+    return pdf;
+}
+int or_medium_transmittance(const float* sigma_t, float t, float* out) {
+    V3 r = medium_transmittance(v3(sigma_t[0], sigma_t[1], sigma_t[2]), t);
+    out[0] = r.x;
+    out[1] = r.y;
+    out[2] = r.z;
+    return 0;
+}
+int or_medium_sample(const float* sigma_a, const float* sigma_s, float tmax, float u_ch, float u_d, float* t,
+                     float* beta) {
+    V3 sa = v3(sigma_a[0], sigma_a[1], sigma_a[2]), ss = v3(sigma_s[0], sigma_s[1], sigma_s[2]);
+    V3 b;
+    bool sc = medium_draw(sa + ss, ss, tmax, u_ch, [&] { return u_d; }, *t, b);
+    beta[0] = b.x;
+    beta[1] = b.y;
+    beta[2] = b.z;
+    return sc ? 1 : 0;
 }
 
 int or_energy_lut(float* e, float* eavg) {

@@ -229,3 +229,82 @@ def test_oracle_reproduces_golden(oracle, cornell_world):
     np.testing.assert_allclose(img, g["image"], rtol=1e-5, atol=1e-6)
     e, ea = oracle.energy_lut()
     assert np.array_equal(e, g["lut_e"]) and np.array_equal(ea, g["lut_eavg"])
+
+
+# --- VolumetricsTests.cs: homogeneous medium and Henyey-Greenstein phase -------
+@pytest.mark.parametrize("sigma_t,dist,expected", [(0.0, 1.0, 1.0), (1.0, 0.0, 1.0), (1.0, 1.0, 0.3679),
+                                                   (0.5, 2.0, 0.3679), (2.0, 3.0, 0.0025)])
+def test_medium_transmittance_matches_analytic(oracle, sigma_t, dist, expected):
+    tr = oracle.medium_transmittance(sigma_t, dist)
+    assert np.all(np.abs(tr - expected) <= 1e-3)
+
+
+def test_medium_transmittance_decreasing_and_channels_independent(oracle):
+    prev = 2.0
+    for d in np.linspace(0.0, 10.0, 21)[1:]:
+        tr = oracle.medium_transmittance(0.3, float(d))[0]
+        assert tr < prev
+        prev = tr
+    tr = oracle.medium_transmittance([2.0, 0.0, 0.05], 1.0)
+    assert tr[0] < 0.2 and abs(tr[1] - 1.0) < 1e-4 and tr[2] > 0.9
+
+
+def test_medium_sample_beta_bounded_and_vacuum_never_scatters(oracle):
+    rng = np.random.default_rng(7)
+    worst = 0.0
+    for u_ch, u_d in rng.uniform(0.0, 1.0, (1000, 2)):
+        _, _, beta = oracle.medium_sample(0.5, 0.6, 5.0, float(u_ch), float(u_d))
+        worst = max(worst, float(0.2126 * beta[0] + 0.7152 * beta[1] + 0.0722 * beta[2]))
+    assert worst < 10.0
+    for u_ch, u_d in rng.uniform(0.0, 1.0, (200, 2)):
+        sc, t, beta = oracle.medium_sample(0.0, 0.0, 100.0, float(u_ch), float(u_d))
+        assert not sc and t == 100.0 and np.all(beta == 1.0)
+
+
+def test_medium_sample_is_an_unbiased_free_flight(oracle):
+    """E[beta * 1{pass}] = Tr(tmax) and E[beta * 1{scatter}] = integral of
+    Tr(t) sigma_s dt over [0, tmax], per channel (the estimator the loop uses)."""
+    sa, ss, tmax = np.array([0.2, 0.05, 0.4], np.float32), np.array([0.3, 0.6, 0.1], np.float32), 3.0
+    st = sa + ss
+    n = 4096
+    pas, sca = np.zeros(3), np.zeros(3)
+    for u_ch in (1.0 / 6.0, 0.5, 5.0 / 6.0):   # each hero channel once
+        for u_d in (np.arange(n) + 0.5) / n:
+            sc, t, beta = oracle.medium_sample(sa, ss, tmax, float(u_ch), float(u_d))
+            (sca if sc else pas)[:] += beta
+    pas /= 3 * n
+    sca /= 3 * n
+    np.testing.assert_allclose(pas, np.exp(-st * tmax), rtol=5e-3)
+    np.testing.assert_allclose(sca, ss / st * (1.0 - np.exp(-st * tmax)), rtol=5e-3)
+
+
+@pytest.mark.parametrize("g", [0.0, 0.5, -0.5, 0.9])
+def test_hg_pdf_integrates_to_one(oracle, g):
+    wo = np.array([0.0, 0.0, -1.0], np.float32)
+    n = 224
+    us = (np.arange(n) + 0.5) / n
+    acc, cnt = 0.0, 0
+    for u1 in us:
+        for u2 in us[::7]:
+            wi, pdf = oracle.hg_sample(g, wo, float(u1), float(u2))
+            if pdf > 1e-12:
+                acc += oracle.hg_eval(g, wo, wi) / pdf
+            cnt += 1
+    assert 0.95 <= acc / cnt <= 1.05
+    # the density itself integrates to one: 2 pi * integral over cos(theta)
+    n = 40000
+    mu = (np.arange(n) + 0.5) / (n / 2) - 1.0
+    vals = np.array([oracle.hg_eval(g, wo, np.array([np.sqrt(1 - m * m), 0.0, -m], np.float32)) for m in mu])
+    assert abs(2 * np.pi * vals.mean() * 2.0 - 1.0) < 5e-3
+
+
+@pytest.mark.parametrize("g", [0.5, -0.5, 0.9])
+def test_hg_sample_mean_cosine_is_g(oracle, g):
+    """The HG mean cosine between wo and wi equals g."""
+    wo = np.array([0.3, 0.4, -np.sqrt(0.75)], np.float32)
+    wo /= np.linalg.norm(wo)
+    n = 128
+    us = (np.arange(n) + 0.5) / n
+    m = np.mean([float(np.dot(oracle.hg_sample(g, wo, float(u1), float(u2))[0], wo))
+                 for u1 in us for u2 in us[::16]])
+    assert abs(m - g) < 2e-2
