@@ -85,7 +85,8 @@ class RtRenderParams(C.Structure):
                 ("exposure_ev", C.c_float), ("mis_heuristic", C.c_int32), ("light_strategy", C.c_int32),
                 ("kernel", C.c_int32), ("block_size", C.c_int32), ("wavefront_size", C.c_int32),
                 ("sort_materials", C.c_int32), ("pixel_x0", C.c_int32), ("pixel_y0", C.c_int32),
-                ("window_w", C.c_int32), ("window_h", C.c_int32), ("count_work", C.c_int32), ("profile_kernels", C.c_int32)]
+                ("window_w", C.c_int32), ("window_h", C.c_int32), ("count_work", C.c_int32), ("profile_kernels", C.c_int32),
+                ("node_layout", C.c_int32), ("reserved", C.c_int32)]
 
 
 class RtStats(C.Structure):
@@ -259,8 +260,8 @@ def load(path: str | None = None):
         "rt_autotune": (C.c_int, [P, C.POINTER(RtRenderParams), C.POINTER(RtRenderParams)]),
         "rt_scene_get_params": (C.c_int, [P, P, C.c_int32]),
         "rt_scene_set_params": (C.c_int, [P, P, C.c_int32]),
-        "rt_trace_closest": (C.c_int, [P, P, C.c_int64, C.c_float, C.c_float, P]),
-        "rt_trace_any": (C.c_int, [P, P, C.c_int64, P]),
+        "rt_trace_closest": (C.c_int, [P, P, C.c_int64, C.c_float, C.c_float, P, C.c_int32]),
+        "rt_trace_any": (C.c_int, [P, P, C.c_int64, P, C.c_int32]),
         "rt_bsdf_batch": (C.c_int, [P, P, C.c_int64, P]),
         "rt_sobol_batch": (C.c_int, [P, P, P, C.c_int64, P]),
         "rt_energy_lut": (C.c_int, [P, P]),

@@ -27,6 +27,11 @@ constexpr int kAdjPerMat = 16;    // RT_ADJ_PARAMS_PER_MATERIAL
 constexpr int kAdjBsdfDirs = 12;  // slots 0..11 enter the BSDF
 constexpr int kAdjLocal = 128;    // per-thread accumulators when the vector fits (7 materials)
 
+// The dual-number BSDF code is large and reached from several hooks; one
+// out-of-line copy of each function keeps the kernel within the instruction
+// cache (inlined at every call site it thrashed it).
+#define RT_NI __device__ __noinline__
+
 // ---------------------------------------------------------------------------
 // Forward-mode dual numbers: a value and one directional derivative.
 // ---------------------------------------------------------------------------
@@ -128,7 +133,7 @@ RT_D Df lut_e_dual(const float* e, float mu, Df alpha) {
     return Df{x0 + (x1 - x0) * tu, dx0 + (dx1 - dx0) * tu};
 }
 
-RT_D DMat dual_material(const SceneView& s, const Material& m, const float* p, int k) {
+RT_NI DMat dual_material(const SceneView& s, const Material& m, const float* p, int k) {
     auto seed = [&](int i) { return Df{p[i], i == k ? 1.0f : 0.0f}; };
     DMat r;
     D3 bc = D3{seed(0), seed(1), seed(2)};
@@ -213,7 +218,7 @@ RT_D D3 fresnel_schlick_dual(float c, D3 f0) {
     float w = schlick_weight(c);
     return f0 + (1.0f - f0) * w;
 }
-RT_D D3 multiscatter_dual(const SceneView& s, const DMat& dm, float ndv, float ndl) {   // :1906-1926
+RT_NI D3 multiscatter_dual(const SceneView& s, const DMat& dm, float ndv, float ndl) {   // :1906-1926
     Df e_out = lut_e_dual(s.lut_e, ndv, dm.alpha_iso);
     Df e_in = lut_e_dual(s.lut_e, ndl, dm.alpha_iso);
     Df one_m = dmax(1.0f - dm.e_avg, 1e-6f);
@@ -237,7 +242,7 @@ RT_D float clearcoat_shape(const Material& m, float cndv, float cndl, float cndh
 }
 
 // EvaluateDirect (bsdf_eval_direct).
-RT_D D3 eval_direct_dual(const SceneView& s, const Material& m, const DMat& dm, const Surface& rec, V3 L, V3 V) {
+RT_NI D3 eval_direct_dual(const SceneView& s, const Material& m, const DMat& dm, const Surface& rec, V3 L, V3 V) {
     V3 N = rec.n;
     D3 r = d3(v3(0.0f));
     float ndl = fmaxf(dot(N, L), 0.0f);
@@ -271,7 +276,7 @@ RT_D D3 eval_direct_dual(const SceneView& s, const Material& m, const DMat& dm, 
 }
 
 // Evaluate (bsdf_eval), without the cosine.
-RT_D D3 eval_dual(const SceneView& s, const Material& m, const DMat& dm, const Surface& rec, V3 V, V3 L) {
+RT_NI D3 eval_dual(const SceneView& s, const Material& m, const DMat& dm, const Surface& rec, V3 V, V3 L) {
     V3 N = rec.n;
     D3 r = d3(v3(0.0f));
     float ndl = dot(N, L);
@@ -311,8 +316,8 @@ RT_D D3 eval_dual(const SceneView& s, const Material& m, const DMat& dm, const S
 // The attenuation formula of one lobe of ScatterInternal (bsdf_scatter) for a
 // direction already drawn: delta samples of Sample and the legacy Scatter
 // path. The lobe selection probability in the divisor stays detached.
-RT_D D3 lobe_att_dual(const SceneView& s, const Material& m, const DMat& dm, const Surface& rec, V3 V, V3 dir,
-                      int lobe) {
+RT_NI D3 lobe_att_dual(const SceneView& s, const Material& m, const DMat& dm, const Surface& rec, V3 V, V3 dir,
+                       int lobe) {
     V3 N = rec.n;
     switch (lobe) {
     case LOBE_DIFFUSE: {
@@ -374,7 +379,7 @@ RT_D D3 lobe_att_dual(const SceneView& s, const Material& m, const DMat& dm, con
 //     log-derivative.
 RT_D float lobe_floor(int lobe) { return (lobe == LOBE_MULTISCATTER || lobe == LOBE_DIFFTRANS) ? 0.05f : 0.1f; }
 
-RT_D float null_sample_score(const Material& m, const DMat& dm, const Surface& rec, V3 V, int lobe, V3 tried) {
+RT_NI float null_sample_score(const Material& m, const DMat& dm, const Surface& rec, V3 V, int lobe, V3 tried) {
     if (lobe < 0 || lobe > LOBE_CLEARCOAT) return 0.0f;
     float sc = dlog(dm.pl[lobe]);
     if (lobe == LOBE_SPECULAR) {   // VNDF density of the drawn L: G1(V) D(H) / (4 N.V)
@@ -509,7 +514,7 @@ struct AdjointSink {
     // Gradients shared by the surface and medium NEE terms: the emitter's
     // radiance, the medium transmittance over the light distance and the
     // shadow ray's absorption and surface crossings.
-    RT_D void nee_common(const PathState& ps, int li, float dist, int to_la) {
+    RT_NI void nee_common(const PathState& ps, int li, float dist, int to_la) {
         V3 gx = gain(ps, to_la) * sh_x;
         if (is_zero(gx)) return;
         const Light& l = s->lights[li];
@@ -593,8 +598,8 @@ struct AdjointSink {
         if (m.emission.z > 0.0f) add(b + 2, g.z / m.emission.z);
     }
 
-    RT_D void nee_surface(const PathState& ps, int li, const Material& m, const Surface& rec, V3 L, V3 V,
-                          float term, V3 coef, float dist, V3 tr_m, int to_la) {
+    RT_NI void nee_surface(const PathState& ps, int li, const Material& m, const Surface& rec, V3 L, V3 V,
+                           float term, V3 coef, float dist, V3 tr_m, int to_la) {
         if (!sh_added) return;
         nee_common(ps, li, dist, to_la);
         // the term is coef * (f_direct * term) * tr_m * tr: differentiate f_direct
@@ -613,8 +618,8 @@ struct AdjointSink {
         if (sh_added) nee_common(ps, li, dist, to_la);
     }
 
-    RT_D void scatter(const PathState& ps, const Material& m, const Surface& rec, V3 V, V3 dir, int lobe, int mode,
-                      float pdf, V3 att_pre, V3 att, int null_lobe, V3 null_dir) {
+    RT_NI void scatter(const PathState& ps, const Material& m, const Surface& rec, V3 V, V3 dir, int lobe, int mode,
+                       float pdf, V3 att_pre, V3 att, int null_lobe, V3 null_dir) {
         unsigned bits = mmask[rec.material] & ((1u << kAdjBsdfDirs) - 1u);
         if (!bits) return;
         V3 coef;

@@ -313,6 +313,148 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
     }
 }
 
+// The same walk over the four-wide records (SceneView::cnodes4). A record tests
+// the boxes of up to four grandchildren of a binary node at once and visits
+// the hit ones in the binary tree's order for this ray (near group first by
+// the node's split axis, then near first within each group by the child's
+// axis), pushing the others in reverse. A grandchild box lies inside its
+// parent's box (the build takes exact float unions), so a hit on it implies
+// the hit the binary walk would have required first; pruning at pop time is
+// the same entry-distance test. The primitive test sequence, hence the hit
+// and the tie-breaking, is the binary walk's.
+RT_D float sel4(int j, float a, float b, float c, float d) { return j == 0 ? a : (j == 1 ? b : (j == 2 ? c : d)); }
+RT_D int sel4i(int j, int a, int b, int c, int d) { return j == 0 ? a : (j == 1 ? b : (j == 2 ? c : d)); }
+
+template <bool ANY, int STACK>
+__device__ __forceinline__ bool traverse4(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
+                                          int* err) {
+    const int kNone = INT_MIN;
+    V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
+    int st_code[STACK];
+    float st_te[STACK];
+    int sp = 0;
+    float closest = tmax;
+    best.kind = HIT_NONE;
+    int code = kNone;
+    if (s.top_is_bvh) {
+        code = s.top_root4;
+    } else {
+        for (int i = s.num_top_items - 1; i >= 0; --i) {
+            st_code[sp] = leaf_code(s.top_items[i], LEAF_ENT1, 1);
+            st_te[sp] = -kInf;
+            sp++;
+        }
+    }
+    for (;;) {
+        while (code >= 0) {
+            const float4* q = s.cnodes4 + (size_t)code * 8;
+            float4 lx = __ldg(q), ly = __ldg(q + 1), lz = __ldg(q + 2);
+            float4 hx = __ldg(q + 3), hy = __ldg(q + 4), hz = __ldg(q + 5);
+            float4 cc = __ldg(q + 6), mt = __ldg(q + 7);
+            int c0 = __float_as_int(cc.x), c1 = __float_as_int(cc.y), c2 = __float_as_int(cc.z),
+                c3 = __float_as_int(cc.w);
+            float t0, t1, t2, t3;
+            int hm = 0;
+            if (box_hit_te(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, o, inv, tmin, closest, t0) && c0 != kNone) hm |= 1;
+            if (box_hit_te(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, o, inv, tmin, closest, t1) && c1 != kNone) hm |= 2;
+            if (box_hit_te(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, o, inv, tmin, closest, t2) && c2 != kNone) hm |= 4;
+            if (box_hit_te(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, o, inv, tmin, closest, t3) && c3 != kNone) hm |= 8;
+            code = kNone;
+            if (!hm) break;
+            int axn = __float_as_int(mt.x), axl = __float_as_int(mt.y), axr = __float_as_int(mt.z);
+            bool ln = (axn == 0 ? d.x : (axn == 1 ? d.y : d.z)) >= 0.0f;
+            bool l0 = (axl == 0 ? d.x : (axl == 1 ? d.y : d.z)) >= 0.0f;
+            bool r0 = (axr == 0 ? d.x : (axr == 1 ? d.y : d.z)) >= 0.0f;
+            int la = l0 ? 0 : 1, lb = l0 ? 1 : 0, ra = r0 ? 2 : 3, rb = r0 ? 3 : 2;
+            // slots in visit order v0..v3; walk them backwards, pushing all but the first hit
+            int v0 = ln ? la : ra, v1 = ln ? lb : rb, v2 = ln ? ra : la, v3 = ln ? rb : lb;
+            int pend = -1;
+#pragma unroll
+            for (int k = 3; k >= 0; --k) {
+                int j = k == 0 ? v0 : (k == 1 ? v1 : (k == 2 ? v2 : v3));
+                if (!((hm >> j) & 1)) continue;
+                if (pend >= 0) {
+                    if (sp >= STACK) {
+                        *err = RT_ERR_STACK;
+                        return false;
+                    }
+                    st_code[sp] = sel4i(pend, c0, c1, c2, c3);
+                    st_te[sp] = sel4(pend, t0, t1, t2, t3);
+                    sp++;
+                }
+                pend = j;
+            }
+            code = sel4i(pend, c0, c1, c2, c3);
+        }
+        if (code != kNone) {
+            int v = ~code;
+            int first = v >> 5;
+            int kind = (v >> 3) & 3;
+            int count = (v & 7) + 1;
+            code = kNone;
+            if (kind == LEAF_ENT1) {
+                Entity en = s.entities[first];
+                if (en.kind == ENT_MESH) {
+                    int r4 = __ldg(s.mesh_root4 + first);
+                    if (en.index >= 0) {
+                        float4 lo = __ldg(s.ent_box + 2 * first), hi = __ldg(s.ent_box + 2 * first + 1);
+                        float te;
+                        if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
+                            code = r4;
+                            continue;
+                        }
+                    } else {
+                        code = r4;
+                        continue;
+                    }
+                } else {
+                    Hit h;
+                    if (entity_test(s, first, o, d, tmin, closest, h)) {
+                        best = h;
+                        closest = h.t;
+                        if (ANY) return true;
+                    }
+                }
+            } else if (kind == LEAF_ENTS) {
+                if (sp + count > STACK) {
+                    *err = RT_ERR_STACK;
+                    return false;
+                }
+                for (int i = count - 1; i >= 0; --i) {
+                    st_code[sp] = leaf_code(s.top_items[first + i], LEAF_ENT1, 1);
+                    st_te[sp] = -kInf;
+                    sp++;
+                }
+            } else {
+                for (int i = 0; i < count; i++) {
+                    float t, u, vv;
+                    if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, vv)) {
+                        best = Hit{t, u, vv, HIT_TRI, first + i};
+                        closest = t;
+                        if (ANY) return true;
+                    }
+                }
+            }
+        }
+        while (sp > 0) {
+            --sp;
+            if (!(st_te[sp] > closest)) {
+                code = st_code[sp];
+                break;
+            }
+        }
+        if (code == kNone) return true;
+    }
+}
+
+// The node layout as a template switch (counting builds use the two-wide one).
+template <bool ANY, int STACK, bool L4>
+__device__ __forceinline__ bool trace(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
+                                      TravCounters* cnt, int* err) {
+    if (L4) return traverse4<ANY, STACK>(s, o, d, tmin, tmax, best, err);
+    return traverse<ANY, STACK>(s, o, d, tmin, tmax, best, cnt, err);
+}
+
 // Surface record of an accepted hit (Core/HitRecord.cs fields on the path).
 struct Surface {
     V3 p, n, tangent, bitangent;
@@ -1140,14 +1282,14 @@ RT_D float mis_weight(float p, float q, int power) {   // Renderer.cs:1534-1543
 // Geometry/ShadowRay.cs:59-157. Opaque scenes take the any-hit fast path: with
 // no transmissive material the walk returns 0 at the first hit, so "any hit in
 // [tmin, tmax]" decides it exactly.
-template <int STACK>
+template <int STACK, bool L4 = false>
 __device__ __forceinline__ V3 shadow_transmittance(const SceneView& s, int opaque_scene, V3 o, V3 d, float tmin,
                                                    float tmax, Counters* cnt, int* err) {
     Hit h;
     TravCounters* tc = cnt ? &cnt->shadow : nullptr;
     if (cnt) cnt->shadow_rays++;
     if (opaque_scene && !cnt) {   // the counting build walks like ShadowRay.Transmittance
-        traverse<true, STACK>(s, o, d, tmin, tmax, h, tc, err);
+        trace<true, STACK, L4>(s, o, d, tmin, tmax, h, tc, err);
         return h.kind == HIT_NONE ? v3(1.0f) : v3(0.0f);
     }
     V3 thr = v3(1.0f);
@@ -1155,7 +1297,7 @@ __device__ __forceinline__ V3 shadow_transmittance(const SceneView& s, int opaqu
     V3 sigma = v3(0.0f), entry = v3(0.0f);
     bool in_med = false;
     for (int i = 0; i < 8; i++) {
-        traverse<false, STACK>(s, o, d, tmin, remaining, h, tc, err);
+        trace<false, STACK, L4>(s, o, d, tmin, remaining, h, tc, err);
         if (h.kind == HIT_NONE) return thr;
         Surface rec = make_surface(s, h, o, d);
         const Material& m = s.materials[rec.material];

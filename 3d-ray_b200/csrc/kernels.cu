@@ -37,7 +37,7 @@ static_assert(sizeof(RtEntityDesc) == 80, "ABI layout");
 static_assert(sizeof(RtLightDesc) == 88, "ABI layout");
 static_assert(sizeof(RtCameraDesc) == 48, "ABI layout");
 static_assert(sizeof(RtMediumDesc) == 36, "ABI layout");
-static_assert(sizeof(RtRenderParams) == 88, "ABI layout");
+static_assert(sizeof(RtRenderParams) == 96, "ABI layout");
 static_assert(sizeof(RtStats) == 144, "ABI layout");
 static_assert(sizeof(RtBsdfQuery) == 96, "ABI layout");
 static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
@@ -64,7 +64,7 @@ struct RtScene {
     size_t scratch_bytes = 0;
     int* d_err = nullptr;
     int tuned = 0;                 // rt_autotune ran: use the fields below
-    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0;
+    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2;
     // Copy of the world description: rt_scene_set_params rebuilds from it.
     std::vector<RtMaterialDesc> w_materials;
     std::vector<RtEntityDesc> w_entities;
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(rt::SceneView s, rt::RenderC
             if (sacc[i] != 0.0f) atomicAdd(a.grad + i, (double)sacc[i]);
 }
 
-template <int STACK>
+template <int STACK, bool L4>
 __global__ void k_trace_closest(rt::SceneView s, const float* rays, int64_t n, float tmin, float tmax, int* hits,
                                 int* err) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -269,7 +269,7 @@ __global__ void k_trace_closest(rt::SceneView s, const float* rays, int64_t n, f
     const float* r = rays + i * 8;
     V3 o = rt::v3(r[0], r[1], r[2]), d = rt::v3(r[3], r[4], r[5]);
     rt::Hit h;
-    rt::traverse<false, STACK>(s, o, d, tmin, tmax, h, nullptr, err);
+    rt::trace<false, STACK, L4>(s, o, d, tmin, tmax, h, nullptr, err);
     int* out = hits + i * 6;
     if (h.kind == rt::HIT_NONE) {
         out[0] = out[1] = out[2] = 0;
@@ -286,13 +286,13 @@ __global__ void k_trace_closest(rt::SceneView s, const float* rays, int64_t n, f
     out[5] = 1;
 }
 
-template <int STACK>
+template <int STACK, bool L4>
 __global__ void k_trace_any(rt::SceneView s, int opaque, const float* rays, int64_t n, float* out, int* err) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float* r = rays + i * 8;
-    V3 t = rt::shadow_transmittance<STACK>(s, opaque, rt::v3(r[0], r[1], r[2]), rt::v3(r[3], r[4], r[5]), r[6], r[7],
-                                           nullptr, err);
+    V3 t = rt::shadow_transmittance<STACK, L4>(s, opaque, rt::v3(r[0], r[1], r[2]), rt::v3(r[3], r[4], r[5]), r[6],
+                                               r[7], nullptr, err);
     out[i * 3] = t.x;
     out[i * 3 + 1] = t.y;
     out[i * 3 + 2] = t.z;
@@ -509,6 +509,7 @@ struct WfConfig {
     int block = 256;
     int sort = 1;
     int profile = 0;   // per-kernel events instead of the graph
+    int layout = 2;    // BVH records of extend/occlude: 2 or 4 wide
 };
 
 int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st) {
@@ -662,6 +663,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     CUDA_TRY(cudaStreamSynchronize(stream));   // host vectors above go out of scope
     // One iteration: reset, regen, extend, [scan, scatter], shade, occlude.
     int blk = cfg.block;
+    bool l4 = cfg.layout == 4;
+    for (const HostReq& q : reqs) l4 = l4 && q.scene->host.max_stack4 <= kStack;
     unsigned gs = (unsigned)((nslots + blk - 1) / blk);
     unsigned gsh = (unsigned)((cap + blk - 1) / blk);
     unsigned g256 = (unsigned)((nslots + 255) / 256);
@@ -671,7 +674,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         rt::k_wf_reset<<<1, 256, 0, stream>>>(a);
         rt::k_wf_regen<<<g256, 256, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[1], stream);
-        rt::k_wf_extend<kStack><<<gs, blk, 0, stream>>>(a);
+        if (l4) rt::k_wf_extend<kStack, true><<<gs, blk, 0, stream>>>(a);
+        else rt::k_wf_extend<kStack, false><<<gs, blk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[2], stream);
         if (sort) {
             rt::k_wf_scan<<<1, 256, 0, stream>>>(a);
@@ -680,7 +684,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         if (ev) cudaEventRecord(ev[3], stream);
         rt::k_wf_shade<<<gs, blk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[4], stream);
-        rt::k_wf_occlude<kStack><<<gsh, blk, 0, stream>>>(a);
+        if (l4) rt::k_wf_occlude<kStack, true><<<gsh, blk, 0, stream>>>(a);
+        else rt::k_wf_occlude<kStack, false><<<gsh, blk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[5], stream);
     };
     const int batch = 4;
@@ -803,10 +808,12 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
         cfg.slots = sc->tuned_slots;
         cfg.block = sc->tuned_block;
         cfg.sort = sc->tuned_sort;
+        cfg.layout = sc->tuned_layout;
     }
     if (p->wavefront_size > 0) cfg.slots = p->wavefront_size;
     if (p->block_size > 0) cfg.block = p->block_size;
     if (p->sort_materials >= 0) cfg.sort = p->sort_materials;
+    if (p->node_layout == 2 || p->node_layout == 4) cfg.layout = p->node_layout;
     cfg.profile = p->profile_kernels != 0;
     if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
         return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
@@ -862,6 +869,8 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     rt::SceneView& v = sc->view;
     int r = RT_OK;
     r = r ? r : upload(sc, h.cnodes, &v.cnodes);
+    r = r ? r : upload(sc, h.cnodes4, &v.cnodes4);
+    r = r ? r : upload(sc, h.mesh_root4, &v.mesh_root4);
     r = r ? r : upload(sc, h.top_items, &v.top_items);
     r = r ? r : upload(sc, h.tris, &v.tris);
     r = r ? r : upload(sc, h.tri_entity, &v.tri_entity);
@@ -883,6 +892,7 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     v.num_lights = (int)h.lights.size();
     v.top_is_bvh = h.top_is_bvh;
     v.top_root = h.top_root_code;
+    v.top_root4 = h.top_root4;
     v.num_top_items = (int)h.top_items.size();
     v.has_medium = h.has_medium;
     v.sigma_a = h.sigma_a;
@@ -1164,10 +1174,12 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
             cfg.slots = s0->tuned_slots;
             cfg.block = s0->tuned_block;
             cfg.sort = s0->tuned_sort;
+            cfg.layout = s0->tuned_layout;
         }
         if (common->wavefront_size > 0) cfg.slots = common->wavefront_size;
         if (common->block_size > 0) cfg.block = common->block_size;
         if (common->sort_materials >= 0) cfg.sort = common->sort_materials;
+        if (common->node_layout == 2 || common->node_layout == 4) cfg.layout = common->node_layout;
         rc = wf_render(hq, cfg, st);
     }
     for (int i = 0; i < n; i++) {
@@ -1199,39 +1211,46 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
         return fail(RT_ERR_OOM, "film allocation failed");
     const int sizes[3] = {1 << 18, 1 << 20, 1 << 22};
     const int blocks[3] = {64, 128, 256};
+    const int layouts[2] = {2, 4};
+    int nl = sc->host.max_stack4 <= kStack ? 2 : 1;
     double best_ms = 1e30;
     WfConfig pick;
     for (int si = 0; si < 3 && rc == RT_OK; si++)
         for (int bi = 0; bi < 3 && rc == RT_OK; bi++)
-            for (int so = 0; so < 2 && rc == RT_OK; so++) {
-                RtRenderParams p = *params;
-                p.kernel = RT_KERNEL_WAVEFRONT;
-                p.spp = spp;
-                p.count_work = 0;
-                p.wavefront_size = sizes[si];
-                p.block_size = blocks[bi];
-                p.sort_materials = so;
-                RtStats s1{};
-                rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
-                if (rc == RT_OK && s1.kernel_ms < best_ms) {
-                    best_ms = s1.kernel_ms;
-                    pick.slots = sizes[si];
-                    pick.block = blocks[bi];
-                    pick.sort = so;
+            for (int so = 0; so < 2 && rc == RT_OK; so++)
+                for (int li = 0; li < nl && rc == RT_OK; li++) {
+                    RtRenderParams p = *params;
+                    p.kernel = RT_KERNEL_WAVEFRONT;
+                    p.spp = spp;
+                    p.count_work = 0;
+                    p.wavefront_size = sizes[si];
+                    p.block_size = blocks[bi];
+                    p.sort_materials = so;
+                    p.node_layout = layouts[li];
+                    RtStats s1{};
+                    rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
+                    if (rc == RT_OK && s1.kernel_ms < best_ms) {
+                        best_ms = s1.kernel_ms;
+                        pick.slots = sizes[si];
+                        pick.block = blocks[bi];
+                        pick.sort = so;
+                        pick.layout = layouts[li];
+                    }
                 }
-            }
     cudaFree(d_film);
     if (rc != RT_OK) return rc;
     sc->tuned = 1;
     sc->tuned_slots = pick.slots;
     sc->tuned_block = pick.block;
     sc->tuned_sort = pick.sort;
+    sc->tuned_layout = pick.layout;
     if (best) {
         *best = *params;
         best->kernel = RT_KERNEL_WAVEFRONT;
         best->wavefront_size = pick.slots;
         best->block_size = pick.block;
         best->sort_materials = pick.sort;
+        best->node_layout = pick.layout;
     }
     return RT_OK;
 }
@@ -1482,12 +1501,15 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
     return RT_OK;
 }
 
-int rt_trace_closest(RtScene* sc, const float* rays, int64_t n, float tmin, float tmax, int32_t* hits) {
+int rt_trace_closest(RtScene* sc, const float* rays, int64_t n, float tmin, float tmax, int32_t* hits,
+                     int32_t node_layout) {
     if (!sc || !rays || !hits || n < 0) return fail(RT_ERR_INVALID_ARG, "null argument");
+    if (node_layout != 2 && node_layout != 4) return fail(RT_ERR_INVALID_ARG, "node_layout must be 2 or 4");
     if (n == 0) return RT_OK;
     std::lock_guard<std::mutex> lk(sc->mu);
     CUDA_TRY(cudaSetDevice(sc->device));
-    if (sc->host.max_stack > kStack) return fail(RT_ERR_STACK, "scene stack bound exceeded");
+    if ((node_layout == 4 ? sc->host.max_stack4 : sc->host.max_stack) > kStack)
+        return fail(RT_ERR_STACK, "scene stack bound exceeded");
     size_t rb = (size_t)n * 8 * sizeof(float), hb = (size_t)n * 6 * sizeof(int);
     int rc = ensure_scratch(sc, rb + hb);
     if (rc != RT_OK) return rc;
@@ -1495,18 +1517,24 @@ int rt_trace_closest(RtScene* sc, const float* rays, int64_t n, float tmin, floa
     int* d_h = reinterpret_cast<int*>(static_cast<char*>(sc->scratch) + rb);
     CUDA_TRY(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream));
     CUDA_TRY(cudaMemcpyAsync(d_r, rays, rb, cudaMemcpyHostToDevice, sc->stream));
-    k_trace_closest<kStack><<<(unsigned)((n + 127) / 128), 128, 0, sc->stream>>>(sc->view, d_r, n, tmin, tmax, d_h,
-                                                                                 sc->d_err);
+    unsigned g = (unsigned)((n + 127) / 128);
+    if (node_layout == 4)
+        k_trace_closest<kStack, true><<<g, 128, 0, sc->stream>>>(sc->view, d_r, n, tmin, tmax, d_h, sc->d_err);
+    else
+        k_trace_closest<kStack, false><<<g, 128, 0, sc->stream>>>(sc->view, d_r, n, tmin, tmax, d_h, sc->d_err);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(hits, d_h, hb, cudaMemcpyDeviceToHost, sc->stream));
     return check_err(sc);
 }
 
-int rt_trace_any(RtScene* sc, const float* rays, int64_t n, float* out) {
+int rt_trace_any(RtScene* sc, const float* rays, int64_t n, float* out, int32_t node_layout) {
     if (!sc || !rays || !out || n < 0) return fail(RT_ERR_INVALID_ARG, "null argument");
+    if (node_layout != 2 && node_layout != 4) return fail(RT_ERR_INVALID_ARG, "node_layout must be 2 or 4");
     if (n == 0) return RT_OK;
     std::lock_guard<std::mutex> lk(sc->mu);
     CUDA_TRY(cudaSetDevice(sc->device));
+    if ((node_layout == 4 ? sc->host.max_stack4 : sc->host.max_stack) > kStack)
+        return fail(RT_ERR_STACK, "scene stack bound exceeded");
     size_t rb = (size_t)n * 8 * sizeof(float), ob = (size_t)n * 3 * sizeof(float);
     int rc = ensure_scratch(sc, rb + ob);
     if (rc != RT_OK) return rc;
@@ -1514,8 +1542,11 @@ int rt_trace_any(RtScene* sc, const float* rays, int64_t n, float* out) {
     float* d_o = reinterpret_cast<float*>(static_cast<char*>(sc->scratch) + rb);
     CUDA_TRY(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream));
     CUDA_TRY(cudaMemcpyAsync(d_r, rays, rb, cudaMemcpyHostToDevice, sc->stream));
-    k_trace_any<kStack><<<(unsigned)((n + 127) / 128), 128, 0, sc->stream>>>(sc->view, sc->opaque, d_r, n, d_o,
-                                                                             sc->d_err);
+    unsigned g = (unsigned)((n + 127) / 128);
+    if (node_layout == 4)
+        k_trace_any<kStack, true><<<g, 128, 0, sc->stream>>>(sc->view, sc->opaque, d_r, n, d_o, sc->d_err);
+    else
+        k_trace_any<kStack, false><<<g, 128, 0, sc->stream>>>(sc->view, sc->opaque, d_r, n, d_o, sc->d_err);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, d_o, ob, cudaMemcpyDeviceToHost, sc->stream));
     return check_err(sc);

@@ -116,8 +116,20 @@ struct Camera {
     V3 origin, llc, horizontal, vertical;
 };
 
+// Four-wide traversal layout: one 128-byte record per node of the binary tree
+// at even depth, holding the boxes of its (up to) four grandchildren
+// {LL, LR, RL, RR} as SoA float4s and their codes:
+//   q[0..2] lo.x/y/z of the four slots, q[3..5] hi.x/y/z, q[6] child codes,
+//   q[7] (axis of the node, axis of L, axis of R, -).
+// A slot whose binary child is a leaf holds that leaf in its first position
+// (LL or RL) and an empty box in the second. A code >= 0 is another record;
+// a leaf code as in the two-wide layout; an empty slot is INT_MIN.
+// The three axes give the binary tree's visit order for a ray, so the
+// traversal tests the same primitives in the same order as the two-wide one.
 struct SceneView {
     const float4* cnodes;       // 4 float4 per interior node (child-box layout)
+    const float4* cnodes4;      // 8 float4 per four-wide record
+    const int* mesh_root4;      // per entity: a mesh's root code in cnodes4
     const int* top_items;
     const float4* tris;
     const int* tri_entity;
@@ -135,6 +147,7 @@ struct SceneView {
     int num_lights;
     int top_is_bvh;             // 0: the world is a flat list of top_items
     int top_root;               // child code of the top-level root (top_is_bvh only)
+    int top_root4;              // the same in the four-wide layout
     int num_top_items;          // flat list: entity count
     int has_medium;
     V3 sigma_a, sigma_s, sigma_t;

@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
     atomicAdd(&a.ctl->live, 1);
 }
 
-template <int STACK>
+template <int STACK, bool L4>
 __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
     int req = fbits(a.P.pre[i].w);
     const SceneView& s = a.views[a.reqs[req].scene];
     Hit h;
-    traverse<false, STACK>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf, h, nullptr, a.err);
+    trace<false, STACK, L4>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf, h, nullptr, a.err);
     int packed = h.kind == HIT_NONE ? 0 : ((h.kind << 30) | h.slot);
     a.P.hit[i] = make_float4(h.t, h.u, h.v, ibits(packed));
     if (a.sort) {   // material key for the counting sort
@@ -339,15 +339,15 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
     wf_store_media(a, i, R, ps);
 }
 
-template <int STACK>
+template <int STACK, bool L4>
 __global__ void __launch_bounds__(256) k_wf_occlude(WfArgs a) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     int n = min(*a.S.count, a.S.capacity);
     if (j >= n) return;
     float4 o = a.S.o[j], d = a.S.d[j], c = a.S.c[j];
     const SceneView& s = a.views[fbits(c.w)];
-    V3 tr = shadow_transmittance<STACK>(s, a.opaque, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, o.w, nullptr,
-                                        a.err);
+    V3 tr = shadow_transmittance<STACK, L4>(s, a.opaque, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, o.w, nullptr,
+                                            a.err);
     if (near_zero(tr)) return;
     int packed = fbits(d.w);
     int slot = packed >> 1;

@@ -5,9 +5,11 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <thread>
 
 namespace rt {
@@ -596,6 +598,87 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             c[3] = float4{R.hi[0], R.hi[1], R.hi[2], zero};
         }
         if (sc.top_is_bvh) sc.top_root_code = code_of(sc.top_root);
+        // --- four-wide layout: one record per interior node at even depth of
+        // each tree, holding its grandchildren (see SceneView).
+        {
+            auto kids = [&](int node, int& l, int& r, int& axis) {
+                int a, b;
+                std::memcpy(&a, &sc.nodes[node].lo[3], 4);
+                std::memcpy(&b, &sc.nodes[node].hi[3], 4);
+                if (a < 0) return false;
+                l = a;
+                r = b & 0x3FFFFFFF;
+                axis = (int)((unsigned)b >> 30);
+                return true;
+            };
+            std::vector<int> ridx(sc.nodes.size(), -1), rnode;
+            std::vector<int> work;
+            if (sc.top_is_bvh) work.push_back(sc.top_root);
+            for (int e : mesh_ids) work.push_back(sc.entities[e].index);
+            while (!work.empty()) {
+                int n = work.back();
+                work.pop_back();
+                int l = 0, r = 0, ax = 0;
+                if (ridx[n] >= 0 || !kids(n, l, r, ax)) continue;
+                ridx[n] = (int)rnode.size();
+                rnode.push_back(n);
+                for (int c : {l, r}) {
+                    int cl = 0, cr = 0, cax = 0;
+                    if (kids(c, cl, cr, cax)) {
+                        work.push_back(cl);
+                        work.push_back(cr);
+                    }
+                }
+            }
+            auto code4 = [&](int node) {
+                int l = 0, r = 0, ax = 0;
+                return kids(node, l, r, ax) ? ridx[node] : code_of(node);
+            };
+            sc.cnodes4.assign(rnode.size() * 8, float4{0.0f, 0.0f, 0.0f, 0.0f});
+            const float inf = std::numeric_limits<float>::infinity();
+            for (size_t k = 0; k < rnode.size(); k++) {
+                int l = 0, r = 0, ax = 0;
+                kids(rnode[k], l, r, ax);
+                int slot_node[4] = {-1, -1, -1, -1};
+                int axes[3] = {ax, 0, 0};
+                for (int side = 0; side < 2; side++) {
+                    int c = side == 0 ? l : r;
+                    int cl = 0, cr = 0, cax = 0;
+                    if (kids(c, cl, cr, cax)) {
+                        slot_node[2 * side] = cl;
+                        slot_node[2 * side + 1] = cr;
+                        axes[1 + side] = cax;
+                    } else {
+                        slot_node[2 * side] = c;
+                    }
+                }
+                float lo[3][4], hi[3][4];
+                int codes[4];
+                for (int j = 0; j < 4; j++) {
+                    int g = slot_node[j];
+                    for (int a = 0; a < 3; a++) {
+                        lo[a][j] = g >= 0 ? sc.nodes[g].lo[a] : inf;
+                        hi[a][j] = g >= 0 ? sc.nodes[g].hi[a] : inf;
+                    }
+                    codes[j] = g >= 0 ? code4(g) : INT_MIN;
+                }
+                float4* q = &sc.cnodes4[k * 8];
+                for (int a = 0; a < 3; a++) {
+                    q[a] = float4{lo[a][0], lo[a][1], lo[a][2], lo[a][3]};
+                    q[3 + a] = float4{hi[a][0], hi[a][1], hi[a][2], hi[a][3]};
+                }
+                float cf[4], af[3];
+                std::memcpy(cf, codes, sizeof(cf));
+                std::memcpy(af, axes, sizeof(af));
+                q[6] = float4{cf[0], cf[1], cf[2], cf[3]};
+                q[7] = float4{af[0], af[1], af[2], 0.0f};
+            }
+            sc.mesh_root4.assign((size_t)ne, 0);
+            for (int e : mesh_ids) sc.mesh_root4[(size_t)e] = code4(sc.entities[e].index);
+            if (sc.top_is_bvh) sc.top_root4 = code4(sc.top_root);
+            // a record pushes at most three slots; it spans two binary levels
+            sc.max_stack4 = 3 * ((top_depth + 1) / 2) + 4 + 3 * ((max_blas_depth + 1) / 2) + 1;
+        }
         for (int e : mesh_ids) sc.entities[e].index = code_of(sc.entities[e].index);
     }
     // --- explicit lights (SceneLoader.cs:446-458)

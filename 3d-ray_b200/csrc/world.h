@@ -16,6 +16,10 @@ namespace rt {
 struct HostScene {
     std::vector<NodeF> nodes;      // build layout (pre-order), kept for export and tests
     std::vector<float4> cnodes;    // traversal layout: 4 float4 per interior node
+    std::vector<float4> cnodes4;   // four-wide traversal layout: 8 float4 per record
+    std::vector<int> mesh_root4;   // per entity: mesh root code in cnodes4 (else 0)
+    int top_root4 = 0;             // four-wide code of the top-level root (top_is_bvh only)
+    int max_stack4 = 0;            // worst-case traversal stack in the four-wide layout
     std::vector<int> top_items;
     std::vector<float4> tris;      // 3 per triangle
     std::vector<int> tri_entity;

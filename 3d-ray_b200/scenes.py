@@ -246,6 +246,17 @@ def cornell_volume(shadow_samples: int = 1) -> World:
     return w
 
 
+def volume_views(n: int = 8) -> list:
+    """C5's eight views: cameras on a circle of radius 150 around the default
+    Cornell camera, all looking at the box centre."""
+    views = []
+    for k in range(n):
+        a = 2.0 * math.pi * k / n
+        eye = (278.0 + 150.0 * math.cos(a), 278.0 + 100.0 * math.sin(a), -800.0)
+        views.append(camera(eye, (278, 278, 278), (0, 1, 0), 40.0))
+    return views
+
+
 def throughput_scene(seed: int = DEFAULT_SCENE_SEED, n_spheres: int = 64, level: int = 5,
                      shadow_samples: int = 1) -> World:
     """C2: ~1.31 M triangles (64 x 20 480 + 2)."""

@@ -277,6 +277,160 @@ def profile_frame(args):
     lib.rt_scene_destroy(scene)
 
 
+def gradcheck(args):
+    """The path-replay adjoint against central finite differences under common
+    random numbers: C4 (the Cornell box with a Disney sphere: the sphere's
+    baseColor, roughness, metallic, specular and sheen, and the emitter's
+    radiance), once with the reference's luminance clamps and once without, and
+    C5 (the medium's sigma_a and sigma_s and the glass sphere's absorption). The
+    samples are split into 8 independent Sobol batches; per parameter the line
+    gives the mean adjoint and finite-difference gradients, their relative
+    difference, and the standard error of the per-batch difference. The loss is
+    a fixed random weighting of the HDR film."""
+    rt = load_package()
+    abi = rt.abi
+    spp = args.spp if args.spp != SPP else 16384
+    nb = 8
+    sphere = dict(base_color=(0.6, 0.3, 0.2), roughness=0.4, metallic=0.2, specular=0.6, sheen=0.3)
+    for name, clamps in (("c4", True), ("c4", False), ("c5", True)):
+        if name == "c4":
+            w = rt.scenes.cornell_sphere(sphere)
+            res = 64
+        else:
+            w = rt.scenes.cornell_volume()
+            res = 48
+        ds = rt.DiffScene(w)
+        kw = {} if clamps else dict(max_sample_radiance=1e30, indirect_clamp_factor=1.0)
+        rp = abi.render_params(res, res, max(spp // nb, 1), 8, kernel=abi.KERNEL_MEGAKERNEL, **kw)
+        wimg = np.random.default_rng(1).uniform(0.0, 1.0, (3, res, res)).astype(np.float32)
+        theta = ds.get_params()
+        if name == "c4":
+            slots = {f"sphere.base_color[{c}]": (ds.slot("fit_sphere", "base_color", c), 1e-3) for c in range(3)}
+            for n in ("roughness", "metallic", "specular", "sheen"):
+                slots[f"sphere.{n}"] = (ds.slot("fit_sphere", n), 1e-2)
+            for c in range(3):
+                i = ds.slot("light", "radiance", c)
+                slots[f"light.radiance[{c}]"] = (i, 1e-3 * float(theta[i]))
+        else:
+            slots = {}
+            for c in range(3):
+                for nm in ("sigma_a", "sigma_s"):
+                    i = ds.medium_slot(nm, c)
+                    slots[f"medium.{nm}[{c}]"] = (i, 1e-2 * float(theta[i]))
+                i = ds.slot("glass", "absorption", c)
+                slots[f"glass.absorption[{c}]"] = (i, 1e-2 * float(theta[i]))
+        idx = [i for i, _ in slots.values()]
+
+        def loss(th):
+            ds.set_params(th)
+            return float((ds.render(rp).astype(np.float64) * wimg).sum())
+
+        adj = np.zeros((nb, len(idx)))
+        fd = np.zeros((nb, len(idx)))
+        adj_ms = 0.0
+        for b in range(nb):
+            rp.spp_offset = b * rp.spp
+            g = ds.adjoint(rp, wimg, idx)
+            adj_ms += ds.last_stats.kernel_ms
+            for j, (i, eps) in enumerate(slots.values()):
+                tp, tm = theta.copy(), theta.copy()
+                tp[i] += eps
+                tm[i] -= eps
+                fd[b, j] = (loss(tp) - loss(tm)) / (2.0 * eps)
+                adj[b, j] = g[i]
+            ds.set_params(theta)
+        rows = {}
+        for j, (key, (i, eps)) in enumerate(slots.items()):
+            d = adj[:, j] - fd[:, j]
+            ma, mf = float(adj[:, j].mean()), float(fd[:, j].mean())
+            se = float(d.std(ddof=1) / np.sqrt(nb))
+            rows[key] = {"adjoint": ma, "fd": mf, "eps": eps, "rel_err": abs(ma - mf) / max(abs(mf), 1e-30),
+                         "diff_stderr_rel": se / max(abs(mf), 1e-30), "z": float(d.mean() / se) if se > 0 else 0.0}
+        n = res * res * rp.spp * nb
+        print(json.dumps({"gradcheck": name, "clamps": clamps, "image": f"{res}x{res}", "samples": n,
+                          "batches": nb, "adjoint_ms": adj_ms, "adjoint_msamples_per_s": n / adj_ms / 1e3,
+                          "params": rows}), flush=True)
+        ds.close()
+
+
+def fit(args):
+    """C4: recover the sphere's Disney parameters (baseColor, roughness,
+    metallic, specular, sheen) and the emitter radiance from a 1024-spp target
+    rendered with seeded ground truth drawn uniformly in valid ranges. Adam,
+    lr 1e-2, 200 steps of 32 spp, L2 loss on the 256x256 HDR film; gradients
+    from rt_adjoint. The radiance is optimised as its logarithm (Adam moves a
+    parameter by about lr per step, and radiance is O(10)). Each step uses a
+    fresh Sobol range (spp_offset), so the fit sees independent samples."""
+    import torch
+    rt = load_package()
+    abi = rt.abi
+    steps = args.steps if args.steps != 3 else 200
+    rng = np.random.default_rng(2024)
+    names = ["base_color", "base_color", "base_color", "roughness", "metallic", "specular", "sheen"]
+    chans = [0, 1, 2, 0, 0, 0, 0]
+
+    def draw():
+        return np.concatenate([rng.uniform(0.05, 0.95, 3), rng.uniform(0.05, 1.0, 1), rng.uniform(0.0, 1.0, 1),
+                               rng.uniform(0.0, 1.0, 1), rng.uniform(0.0, 1.0, 1)]).astype(np.float32), \
+            (np.array([17.0, 12.0, 4.0]) * rng.uniform(0.6, 1.4, 3)).astype(np.float32)
+
+    truth_s, truth_e = draw()
+    init_s, init_e = draw()
+    ds = rt.DiffScene(rt.scenes.cornell_sphere())
+    theta0 = ds.get_params()
+    s_idx = [ds.slot("fit_sphere", n, c) for n, c in zip(names, chans)]
+    e_idx = [ds.slot("light", "radiance", c) for c in range(3)]
+
+    def vec(sv, ev):
+        th = theta0.copy()
+        th[s_idx] = sv
+        th[e_idx] = ev
+        return th
+
+    res = 256
+    ds.set_params(vec(truth_s, truth_e))
+    tp = abi.render_params(res, res, 1024, 8, kernel=abi.KERNEL_WAVEFRONT, spp_offset=1 << 24)
+    target = ds.render(tp)
+    x_s = torch.tensor(init_s, dtype=torch.float64, requires_grad=True)
+    x_le = torch.tensor(np.log(init_e), dtype=torch.float64, requires_grad=True)
+    opt = torch.optim.Adam([x_s, x_le], lr=1e-2)
+    mask = s_idx + e_idx
+    hist = []
+    t0 = time.perf_counter()
+    adj_ms = 0.0
+    for it in range(steps):
+        sv = x_s.detach().numpy().astype(np.float32)
+        ev = np.exp(x_le.detach().numpy()).astype(np.float32)
+        ds.set_params(vec(sv, ev))
+        rp = abi.render_params(res, res, 32, 8, kernel=abi.KERNEL_MEGAKERNEL, spp_offset=it * 32)
+        img = ds.render(rp)
+        diff = img.astype(np.float64) - target
+        loss = float((diff ** 2).mean())
+        g = ds.adjoint(rp, (2.0 * diff / diff.size).astype(np.float32), mask)
+        adj_ms += ds.last_stats.kernel_ms
+        opt.zero_grad()
+        x_s.grad = torch.from_numpy(g[s_idx].astype(np.float64))
+        x_le.grad = torch.from_numpy(g[e_idx].astype(np.float64) * ev)   # d/dlog e = e d/de
+        opt.step()
+        with torch.no_grad():
+            x_s.clamp_(0.0, 1.0)
+        hist.append(loss)
+    wall = time.perf_counter() - t0
+    final_s = x_s.detach().numpy()
+    final_e = np.exp(x_le.detach().numpy())
+    keys = ["base_r", "base_g", "base_b", "roughness", "metallic", "specular", "sheen"]
+    print(json.dumps({
+        "fit": "c4", "image": f"{res}x{res}", "steps": steps, "spp_per_step": 32, "lr": 1e-2, "target_spp": 1024,
+        "loss_first": hist[0], "loss_last10_mean": float(np.mean(hist[-10:])),
+        "param_abs_err_init": dict(zip(keys, map(float, np.abs(init_s - truth_s)))),
+        "param_abs_err_final": dict(zip(keys, map(float, np.abs(final_s - truth_s)))),
+        "radiance_rel_err_init": list(map(float, np.abs(init_e / truth_e - 1))),
+        "radiance_rel_err_final": list(map(float, np.abs(final_e / truth_e - 1))),
+        "seconds": wall, "adjoint_ms_per_step": adj_ms / steps,
+        "loss_curve_every_20": [float(h) for h in hist[::20]]}), flush=True)
+    ds.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -287,6 +441,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-kernel and relMSE side measurements")
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
+    ap.add_argument("--gradcheck", action="store_true",
+                    help="adjoint gradients against central finite differences (C4, C5) and exit")
     ap.add_argument("--profile-frame", action="store_true",
                     help="render the frame twice with fixed settings and exit (the command profiled by ncu)")
     args = ap.parse_args()
@@ -294,6 +451,10 @@ def main():
         return run_reference(args)
     if args.profile_frame:
         return profile_frame(args)
+    if args.gradcheck:
+        return gradcheck(args)
+    if args.fit:
+        return fit(args)
 
     import torch
     rank, world_size, dist = dist_setup(args.gpus)

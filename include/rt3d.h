@@ -181,6 +181,9 @@ typedef struct RtRenderParams {
     int32_t window_w, window_h;
     int32_t count_work;             /* 1: counting build, fills the work fields of RtStats */
     int32_t profile_kernels;        /* 1: wavefront without the graph, per-kernel events in RtStats */
+    int32_t node_layout;            /* BVH records the wavefront's extend/occlude read: 2 two-wide,
+                                       4 four-wide, 0 the autotuned choice (else two-wide) */
+    int32_t reserved;
 } RtRenderParams;
 
 /* Counters and timings of one call. */
@@ -292,9 +295,10 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
                     const RtRenderParams* common, float* const* outs, RtStats* stats);
 
 /* Autotuner: times the wavefront over wavefront size {256K, 1M, 4M} x block
- * {64, 128, 256} x material sort {off, on} on a bounded slice of `params`
- * (the full window at the spp giving ~16 M samples), keeps the fastest for
- * this scene (used when those params fields are 0 / -1) and returns it. */
+ * {64, 128, 256} x material sort {off, on} x node layout {two-wide,
+ * four-wide} on a bounded slice of `params` (the full window at the spp
+ * giving ~16 M samples), keeps the fastest for this scene (used when those
+ * params fields are 0 / -1) and returns it. */
 int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* best);
 
 /* ---- differentiation ----------------------------------------------------- */
@@ -352,11 +356,12 @@ int rt_scene_set_params(RtScene* scene, const float* params, int32_t count);
 /* ---- test-only entry points --------------------------------------------- */
 /* Ray in: origin[3], dir[3] (8 floats per ray, last two ignored).
  * Closest hit out per ray: t, u, v as float, entity id, local primitive id
- * (int32 bits), and a hit flag: 6 words. */
+ * (int32 bits), and a hit flag: 6 words. node_layout: 2 (two-wide records)
+ * or 4 (four-wide), the layouts the wavefront can run on. */
 int rt_trace_closest(RtScene* scene, const float* rays, int64_t n, float tmin, float tmax,
-                     int32_t* hits);
+                     int32_t* hits, int32_t node_layout);
 /* Shadow rays in: origin[3], dir[3], tmin, tmax. Out: transmittance rgb. */
-int rt_trace_any(RtScene* scene, const float* rays, int64_t n, float* transmittance);
+int rt_trace_any(RtScene* scene, const float* rays, int64_t n, float* transmittance, int32_t node_layout);
 
 /* BSDF batch. Each record (RtBsdfQuery) carries the shading inputs; the
  * results are the Sample outcome and Evaluate/Pdf/EvaluateDirect values. */

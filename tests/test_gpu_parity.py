@@ -32,17 +32,17 @@ class Scene:
             self.lib.rt_scene_destroy(self.h)
             self.h = None
 
-    def closest(self, rays, tmin=1e-4, tmax=3.4028235e38):
+    def closest(self, rays, tmin=1e-4, tmax=3.4028235e38, layout=2):
         rays = np.ascontiguousarray(rays, np.float32)
         hits = np.zeros((rays.shape[0], 6), np.int32)
-        abi.check(self.lib.rt_trace_closest(self.h, abi.ptr(rays), rays.shape[0], tmin, tmax, abi.ptr(hits)),
+        abi.check(self.lib.rt_trace_closest(self.h, abi.ptr(rays), rays.shape[0], tmin, tmax, abi.ptr(hits), layout),
                   "rt_trace_closest")
         return hits
 
-    def any(self, rays):
+    def any(self, rays, layout=2):
         rays = np.ascontiguousarray(rays, np.float32)
         out = np.zeros((rays.shape[0], 3), np.float32)
-        abi.check(self.lib.rt_trace_any(self.h, abi.ptr(rays), rays.shape[0], abi.ptr(out)), "rt_trace_any")
+        abi.check(self.lib.rt_trace_any(self.h, abi.ptr(rays), rays.shape[0], abi.ptr(out), layout), "rt_trace_any")
         return out
 
     def bsdf(self, q):
@@ -312,3 +312,120 @@ def test_work_counters_match_oracle(oracle, cornell, cornell_world):
     assert abs(g_nodes / o_nodes - 1) < 0.03, (g_nodes, o_nodes)
     g_tri = (st.prim_tests + st.shadow_prim_tests) / st.samples
     assert abs(g_tri / (c["tri_tests"] / c["samples"]) - 1) < 0.03
+
+
+# --- C5: homogeneous medium and a dielectric sphere with Beer-Lambert absorption ---
+@pytest.fixture(scope="module")
+def volume_world():
+    return rt.scenes.cornell_volume()
+
+
+def test_shadow_walk_through_glass_matches_oracle(oracle, volume_world):
+    """ShadowRay.Transmittance's transparent walk: rays aimed through the
+    glass sphere cross two interfaces with Beer-Lambert between them."""
+    rng = np.random.default_rng(11)
+    n = 50000
+    o = rng.uniform((20, 20, 20), (535, 535, 200), (n, 3))
+    target = np.array([370.0, 90.0, 350.0]) + rng.uniform(-110, 110, (n, 3))
+    d = target - o
+    dist = np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3], rays[:, 3:6] = o, d / dist
+    rays[:, 6] = 1e-4
+    rays[:, 7] = (dist[:, 0] * 1.5).astype(np.float32)
+    s = Scene(volume_world)
+    try:
+        g = s.any(rays)
+    finally:
+        s.close()
+    ref = oracle.OracleScene(abi.PackedWorld(volume_world)).trace_any(rays)
+    partial = np.mean((ref[:, 0] > 0) & (ref[:, 0] < 0.999))
+    assert partial > 0.05, "too few rays crossed the glass"
+    assert np.array_equal(g > 0, ref > 0)
+    np.testing.assert_allclose(g, ref, rtol=2e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("kernel", [abi.KERNEL_MEGAKERNEL, abi.KERNEL_WAVEFRONT])
+def test_render_volume_matches_oracle(oracle, volume_world, kernel):
+    """C5 estimator (free-flight sampling, phase NEE with MIS, glass with an
+    IOR stack and interior absorption) against the oracle, statistically."""
+    s = Scene(volume_world)
+    try:
+        g, st = s.render(abi.render_params(48, 48, 1024, 16, kernel=kernel, wavefront_size=1 << 16))
+    finally:
+        s.close()
+    assert st.samples == 48 * 48 * 1024 and np.all(np.isfinite(g))
+    o, _ = oracle.OracleScene(abi.PackedWorld(volume_world)).render(abi.render_params(48, 48, 256, 16))
+    np.testing.assert_allclose(g.mean(axis=(1, 2)), o.mean(axis=(1, 2)), rtol=0.03)
+    assert rel_mse(o, g) < 0.1
+
+
+def test_volume_views_batch_equals_individual_renders(volume_world):
+    """C5's eight views in one persistent launch equal the views rendered alone."""
+    lib = abi.load()
+    s = Scene(volume_world)
+    try:
+        views = rt.scenes.volume_views()
+        reqs = (abi.RtRequest * len(views))()
+        outs, singles = [], []
+        for i, cam in enumerate(views):
+            reqs[i].scene, reqs[i].width, reqs[i].height, reqs[i].spp, reqs[i].max_depth = 0, 32, 32, 32, 16
+            reqs[i].camera = abi.camera_desc(cam)
+            outs.append(np.zeros((3, 32, 32), np.float32))
+            w1 = rt.scenes.cornell_volume()
+            w1.camera = cam
+            one = Scene(w1)
+            try:
+                img, _ = one.render(abi.render_params(32, 32, 32, 16, kernel=abi.KERNEL_WAVEFRONT))
+            finally:
+                one.close()
+            singles.append(img)
+        scenes = (C.c_void_p * 1)(s.h)
+        optrs = (C.c_void_p * len(views))(*[o.ctypes.data for o in outs])
+        st = abi.RtStats()
+        common = abi.render_params(1, 1, 1, 1, kernel=abi.KERNEL_WAVEFRONT, wavefront_size=1 << 14)
+        abi.check(lib.rt_render_batch(scenes, 1, reqs, len(views), C.byref(common), optrs, C.byref(st)),
+                  "rt_render_batch")
+        for o, s1 in zip(outs, singles):
+            np.testing.assert_allclose(o, s1, rtol=1e-4, atol=1e-6)
+        assert not np.allclose(outs[0], outs[4])   # the views differ
+    finally:
+        s.close()
+
+
+# --- the four-wide node layout ------------------------------------------------------
+def test_four_wide_layout_hits_equal_two_wide_and_oracle(oracle, cornell, cornell_world, throughput_world_small):
+    """Closest and any hits through the four-wide records are bit for bit the
+    two-wide walk's (same primitives in the same order, so the same ties) and
+    the oracle's."""
+    rays = camera_rays(cornell_world, 96, 96)
+    two, four = cornell.closest(rays, layout=2), cornell.closest(rays, layout=4)
+    assert np.array_equal(two, four)
+    _compare_hits(four, oracle.OracleScene(abi.PackedWorld(cornell_world)).trace_closest(rays))
+    rr = random_rays(((1, 1, 1), (554, 554, 554)), 100000, seed=21)
+    assert np.array_equal(cornell.closest(rr, layout=2), cornell.closest(rr, layout=4))
+    rr[:, 6] = 1e-4
+    rr[:, 7] = np.random.default_rng(22).uniform(1, 800, rr.shape[0]).astype(np.float32)
+    assert np.array_equal(cornell.any(rr, layout=2), cornell.any(rr, layout=4))
+    s = Scene(throughput_world_small)
+    try:
+        rt_rays = random_rays(((-12, -12, -12), (12, 12, 12)), 100000, seed=23)
+        assert np.array_equal(s.closest(rt_rays, layout=2), s.closest(rt_rays, layout=4))
+    finally:
+        s.close()
+
+
+def test_four_wide_layout_renders_like_two_wide(throughput_world_small, volume_world):
+    """The wavefront on either layout renders the same samples: images equal up
+    to the order of the float additions (opaque scene and the glass walk)."""
+    for world in (throughput_world_small, volume_world):
+        s = Scene(world)
+        try:
+            imgs = []
+            for layout in (2, 4):
+                p = abi.render_params(64, 48, 64, 12, kernel=abi.KERNEL_WAVEFRONT, wavefront_size=1 << 15,
+                                      node_layout=layout)
+                imgs.append(s.render(p)[0])
+            np.testing.assert_allclose(imgs[0], imgs[1], rtol=1e-4, atol=1e-6)
+        finally:
+            s.close()
