@@ -265,6 +265,7 @@ def load(path: str | None = None):
         "rt_bsdf_batch": (C.c_int, [P, P, C.c_int64, P]),
         "rt_sobol_batch": (C.c_int, [P, P, P, C.c_int64, P]),
         "rt_energy_lut": (C.c_int, [P, P]),
+        "rt_probe_l2_bandwidth": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, C.POINTER(C.c_double)]),
         "rt_tonemap": (C.c_int, [P, C.c_int32, C.c_int32, C.c_float, P]),
     }
     for name, (res, args) in sig.items():

@@ -1616,6 +1616,62 @@ int rt_tonemap(const float* hdr, int32_t width, int32_t height, float exposure_e
     return rc;
 }
 
+}  // extern "C"
+
+namespace {
+
+// L2 read bandwidth: every thread streams float4s through L2 only (.cg), a
+// grid-stride pass over a buffer small enough to stay L2-resident, several
+// times. The sum is written so the loads cannot be dropped.
+__global__ void __launch_bounds__(256) k_l2_probe(const float4* buf, int64_t n4, int passes, float* sink) {
+    float acc = 0.0f;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int p = 0; p < passes; p++)
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+            float4 v = __ldcg(buf + i);
+            acc += (v.x + v.y) + (v.z + v.w);
+        }
+    if (acc == 1.2345678f) sink[0] = acc;   // never true for the zeroed buffer; keeps the loads live
+}
+
+}  // namespace
+
+extern "C" {
+
+int rt_probe_l2_bandwidth(int32_t device, int64_t bytes, int32_t passes, double* gbs) {
+    if (!gbs || bytes < (1 << 20) || passes < 1) return fail(RT_ERR_INVALID_ARG, "bytes >= 1 MiB and passes >= 1");
+    CUDA_TRY(cudaSetDevice(device));
+    int64_t n4 = bytes / 16;
+    void* mem = nullptr;
+    if (cudaMalloc(&mem, (size_t)n4 * 16 + 256) != cudaSuccess) return fail(RT_ERR_OOM, "probe buffer");
+    float4* buf = static_cast<float4*>(mem);
+    float* sink = reinterpret_cast<float*>(static_cast<char*>(mem) + (size_t)n4 * 16);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = RT_OK;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMemset(mem, 0, (size_t)n4 * 16 + 256) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess) {
+        rc = fail(RT_ERR_CUDA, "probe set-up");
+    } else {
+        unsigned grid = (unsigned)sms * 8;
+        k_l2_probe<<<grid, 256>>>(buf, n4, 1, sink);   // warm: bring the buffer into L2
+        cudaEventRecord(e0);
+        k_l2_probe<<<grid, 256>>>(buf, n4, passes, sink);
+        cudaEventRecord(e1);
+        float ms = 0.0f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+            cudaGetLastError() != cudaSuccess)
+            rc = fail(RT_ERR_CUDA, "probe run");
+        else
+            *gbs = (double)n4 * 16.0 * passes / (ms * 1e-3) / 1e9;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(mem);
+    return rc;
+}
+
 int rt_energy_lut(float* e, float* eavg) {
     std::vector<float> a(1024), b(32);
     rt::build_energy_lut(a.data(), b.data());

@@ -230,11 +230,13 @@ def cornell_sphere(params: dict | None = None, shadow_samples: int = 1) -> World
     return w
 
 
-def cornell_volume(shadow_samples: int = 1) -> World:
-    """C5: homogeneous medium (sigma_t 0.02, albedo 0.8, HG g 0.6) filling the
-    box, and a dielectric sphere (IOR 1.5, Beer-Lambert sigma_a (0.1,0.3,0.5)
-    per unit via transmission_color = exp(-sigma_a), depth 1) in place of the
-    tall box."""
+def cornell_volume(shadow_samples: int = 1, density: float = 1.0) -> World:
+    """C5: homogeneous medium (sigma_t 0.02 per unit times `density`, albedo
+    0.8, HG g 0.6) filling the box, and a dielectric sphere (IOR 1.5,
+    Beer-Lambert sigma_a (0.1,0.3,0.5) per unit via transmission_color =
+    exp(-sigma_a), depth 1) in place of the tall box. The medium is global, so
+    the camera sits in the box's open side (at sigma_t 0.02 the 800 units from
+    the C1 camera alone have optical depth 16)."""
     w = cornell(shadow_samples, tall_box=False)
     w.name = "cornell-volume"
     sig = np.array([0.1, 0.3, 0.5])
@@ -242,18 +244,19 @@ def cornell_volume(shadow_samples: int = 1) -> World:
                                            transmission_color=tuple(float(x) for x in np.exp(-sig)),
                                            transmission_depth=1.0))
     w.add_sphere((370, 90, 350), 90.0, glass, name="glass_sphere")
-    w.medium = dict(sigma_a=(0.004, 0.004, 0.004), sigma_s=(0.016, 0.016, 0.016), g=0.6)
+    w.medium = dict(sigma_a=(0.004 * density,) * 3, sigma_s=(0.016 * density,) * 3, g=0.6)
+    w.camera = camera((278, 278, 1), (278, 278, 555), (0, 1, 0), 75.0)
     return w
 
 
 def volume_views(n: int = 8) -> list:
-    """C5's eight views: cameras on a circle of radius 150 around the default
-    Cornell camera, all looking at the box centre."""
+    """C5's eight views: cameras on a circle of radius 80 in the box's open
+    side, all looking at the box centre."""
     views = []
     for k in range(n):
         a = 2.0 * math.pi * k / n
-        eye = (278.0 + 150.0 * math.cos(a), 278.0 + 100.0 * math.sin(a), -800.0)
-        views.append(camera(eye, (278, 278, 278), (0, 1, 0), 40.0))
+        eye = (278.0 + 80.0 * math.cos(a), 278.0 + 80.0 * math.sin(a), 1.0)
+        views.append(camera(eye, (278, 278, 278), (0, 1, 0), 75.0))
     return views
 
 

@@ -266,14 +266,18 @@ def profile_frame(args):
     abi.check(lib.rt_scene_create(pw.ref(), C.byref(scene)), "rt_scene_create")
     kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
     p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=256,
-                          sort_materials=1)
+                          sort_materials=1, node_layout=args.node_layout, profile_kernels=int(args.split))
     film = np.zeros((3, H, W), np.float32)
     st = abi.RtStats()
     for i in range(2):
         abi.check(lib.rt_render(scene, C.byref(p), film.ctypes.data_as(C.c_void_p), C.byref(st)), "rt_render")
-        print(json.dumps({"frame": i, "kernel": args.kernel, "spp": args.spp, "kernel_ms": st.kernel_ms,
-                          "Msamples_per_s": W * H * args.spp / st.kernel_ms / 1e3,
-                          "iterations": st.iterations, "launches": st.kernel_launches}), flush=True)
+        line = {"frame": i, "kernel": args.kernel, "node_layout": args.node_layout, "spp": args.spp,
+                "kernel_ms": st.kernel_ms, "Msamples_per_s": W * H * args.spp / st.kernel_ms / 1e3,
+                "iterations": st.iterations, "launches": st.kernel_launches}
+        if args.split:
+            line.update(regen_ms=st.regen_ms, extend_ms=st.extend_ms, sort_ms=st.sort_ms, shade_ms=st.shade_ms,
+                        occlude_ms=st.occlude_ms)
+        print(json.dumps(line), flush=True)
     lib.rt_scene_destroy(scene)
 
 
@@ -395,10 +399,14 @@ def fit(args):
     x_le = torch.tensor(np.log(init_e), dtype=torch.float64, requires_grad=True)
     opt = torch.optim.Adam([x_s, x_le], lr=1e-2)
     mask = s_idx + e_idx
-    hist = []
+    hist, hist_truth = [], []
     t0 = time.perf_counter()
     adj_ms = 0.0
     for it in range(steps):
+        if it >= steps - 10:   # the loss the ground truth gets on the same samples
+            ds.set_params(vec(truth_s, truth_e))
+            rp = abi.render_params(res, res, 32, 8, kernel=abi.KERNEL_MEGAKERNEL, spp_offset=it * 32)
+            hist_truth.append(float(((ds.render(rp).astype(np.float64) - target) ** 2).mean()))
         sv = x_s.detach().numpy().astype(np.float32)
         ev = np.exp(x_le.detach().numpy()).astype(np.float32)
         ds.set_params(vec(sv, ev))
@@ -422,6 +430,7 @@ def fit(args):
     print(json.dumps({
         "fit": "c4", "image": f"{res}x{res}", "steps": steps, "spp_per_step": 32, "lr": 1e-2, "target_spp": 1024,
         "loss_first": hist[0], "loss_last10_mean": float(np.mean(hist[-10:])),
+        "loss_at_truth_last10_mean": float(np.mean(hist_truth)),
         "param_abs_err_init": dict(zip(keys, map(float, np.abs(init_s - truth_s)))),
         "param_abs_err_final": dict(zip(keys, map(float, np.abs(final_s - truth_s)))),
         "radiance_rel_err_init": list(map(float, np.abs(init_e / truth_e - 1))),
@@ -441,6 +450,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-kernel and relMSE side measurements")
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--node-layout", type=int, default=2, choices=[2, 4],
+                    help="BVH records for --profile-frame: two-wide or four-wide")
+    ap.add_argument("--split", action="store_true", help="--profile-frame: per-kernel event times")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
     ap.add_argument("--gradcheck", action="store_true",
                     help="adjoint gradients against central finite differences (C4, C5) and exit")
@@ -474,7 +486,7 @@ def main():
         best = abi.RtRenderParams()
         abi.check(lib.rt_autotune(scene, C.byref(params), C.byref(best)), "rt_autotune")
         tuned = {"wavefront_size": best.wavefront_size, "block_size": best.block_size,
-                 "sort_materials": best.sort_materials}
+                 "sort_materials": best.sort_materials, "node_layout": best.node_layout}
     film = torch.empty((3, H, W), dtype=torch.float32, device="cuda")
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -572,13 +584,27 @@ def main():
     else:
         achieved = bytes_per_sample * samples_per_step / (ms_per_step / 1e3) / 1e9
         roof.update({"kernel": "k_render_mega", "achieved": achieved, "frac": achieved / hbm})
-    traffic = None
+    traffic, l2_bytes = None, None
     prof = os.path.join(ROOT, "profiles", f"{roof['kernel']}_icospheres.md")
     if os.path.exists(prof):
         for line in open(prof):
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
+            if line.startswith("l2_bytes_per_launch:"):
+                l2_bytes = float(line.split(":")[1])
     roof["traffic"] = traffic
+    # L2 roofline beside the HBM one: the scene is largely L2-resident, so the
+    # traversal kernels are judged against L2 bandwidth too. The peak is a
+    # project micro-benchmark (L2-only float4 streams over a 32 MiB buffer).
+    l2_peak = C.c_double(0.0)
+    if lib.rt_probe_l2_bandwidth(dev, 32 << 20, 64, C.byref(l2_peak)) == abi.RT_OK:
+        l2 = {"peak": l2_peak.value, "unit": "GB/s", "peak_source": "rt_probe_l2_bandwidth (32 MiB, 64 passes)",
+              "bytes_per_launch": l2_bytes}
+        if l2_bytes and "kernel_ms_per_step" in roof:
+            per_launch_s = roof["kernel_ms_per_step"][roof["kernel"][5:]] / 1e3 / max(roof["launches_per_step"], 1)
+            l2["achieved"] = l2_bytes / per_launch_s / 1e9
+            l2["frac"] = l2["achieved"] / l2_peak.value
+        roof["l2"] = l2
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

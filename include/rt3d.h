@@ -400,6 +400,10 @@ int rt_tonemap(const float* hdr_rgb_planar, int32_t width, int32_t height, float
 
 /* Kulla-Conty tables the scene uses: E (32x32, mu-major) then E_avg (32). */
 int rt_energy_lut(float* e_1024, float* eavg_32);
+/* L2 read bandwidth of a device in GB/s: `passes` streams over a `bytes`
+ * buffer (choose it to fit L2) through L2-only loads. The L2 roofline's peak;
+ * no counterpart in the reference. */
+int rt_probe_l2_bandwidth(int32_t device, int64_t bytes, int32_t passes, double* gbs);
 
 #ifdef __cplusplus
 }

@@ -189,7 +189,7 @@ def test_volume_gradients_match_finite_differences():
     slots = [ds.medium_slot("sigma_a", 0), ds.medium_slot("sigma_s", 0), ds.slot("glass", "absorption", 0)]
     adj, fd = _batches(ds, rp, wimg, theta, slots, lambda i: 1e-2 * theta[i], 6)
     assert _agree(adj, fd, 5e-3).all(), (adj.mean(0), fd.mean(0))
-    assert (adj.mean(0) < 0).all()   # more extinction or absorption darkens the box
+    assert adj.mean(0)[0] < 0 and adj.mean(0)[2] <= 0   # more absorption darkens the box
 
 
 def test_gradients_match_cpu_oracle_finite_differences(oracle):

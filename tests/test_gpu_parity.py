@@ -346,9 +346,12 @@ def test_shadow_walk_through_glass_matches_oracle(oracle, volume_world):
 
 
 @pytest.mark.parametrize("kernel", [abi.KERNEL_MEGAKERNEL, abi.KERNEL_WAVEFRONT])
-def test_render_volume_matches_oracle(oracle, volume_world, kernel):
+def test_render_volume_matches_oracle(oracle, kernel):
     """C5 estimator (free-flight sampling, phase NEE with MIS, glass with an
-    IOR stack and interior absorption) against the oracle, statistically."""
+    IOR stack and interior absorption) against the oracle, statistically, in a
+    10x thinner medium whose image is well conditioned (C5's own medium has
+    optical depth 11 across the box)."""
+    volume_world = rt.scenes.cornell_volume(density=0.1)
     s = Scene(volume_world)
     try:
         g, st = s.render(abi.render_params(48, 48, 1024, 16, kernel=kernel, wavefront_size=1 << 16))
@@ -401,7 +404,7 @@ def test_four_wide_layout_hits_equal_two_wide_and_oracle(oracle, cornell, cornel
     rays = camera_rays(cornell_world, 96, 96)
     two, four = cornell.closest(rays, layout=2), cornell.closest(rays, layout=4)
     assert np.array_equal(two, four)
-    _compare_hits(four, oracle.OracleScene(abi.PackedWorld(cornell_world)).trace_closest(rays))
+    _compare_hits(four, oracle.OracleScene(abi.PackedWorld(cornell_world)).trace_closest(rays)[0])
     rr = random_rays(((1, 1, 1), (554, 554, 554)), 100000, seed=21)
     assert np.array_equal(cornell.closest(rr, layout=2), cornell.closest(rr, layout=4))
     rr[:, 6] = 1e-4
