@@ -196,7 +196,145 @@ RT_D bool box_hit_te(float lx, float ly, float lz, float hx, float hy, float hz,
 // the reference's minus primitives that cannot be hit: ids and t match.
 // ANY = true stops at the first accepted hit (opaque shadow rays).
 // has_root restricts the walk to one mesh BVH (a light's own geometry).
-// Returns false on stack overflow (err set).
+// Walker holds the walk's state so that it can run in rounds; the persistent
+// wavefront kernels refill finished lanes of a warp between rounds. A stack
+// overflow ends the walk with ok = false and err set. traverse() below is the
+// same walk as one loop.
+template <bool ANY, int STACK>
+struct Walker {
+    static constexpr int kNone = INT_MIN;   // "pop the next entry" (no leaf code can take this value)
+    V3 o, d, inv;
+    float tmin, closest;
+    Hit best;
+    int code, sp;
+    bool ok;
+    int st_code[STACK];
+    float st_te[STACK];
+
+    RT_D void start(const SceneView& s, V3 o_, V3 d_, float tmin_, float tmax, TravCounters* cnt, bool has_root,
+                    int root) {
+        o = o_;
+        d = d_;
+        inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
+        tmin = tmin_;
+        closest = tmax;
+        best.kind = HIT_NONE;
+        sp = 0;
+        ok = true;
+        code = kNone;
+        if (has_root) {
+            code = root;
+            if (cnt && root >= 0) cnt->nodes++;   // the mesh root's own BvhNode.Hit
+        } else if (s.top_is_bvh) {
+            code = s.top_root;
+            if (cnt) cnt->nodes++;                // the world root's BvhNode.Hit
+        } else {
+            for (int i = s.num_top_items - 1; i >= 0; --i) {
+                st_code[sp] = leaf_code(s.top_items[i], LEAF_ENT1, 1);
+                st_te[sp] = -kInf;
+                sp++;
+            }
+        }
+    }
+
+    // One round: descend interior records to a leaf, test the leaf, pop the
+    // next entry. Returns true when the walk is over.
+    RT_D bool step(const SceneView& s, TravCounters* cnt, int* err) {
+        // Descend interior records: test both children, go near, stack far.
+        while (code >= 0) {
+            const float4* np = s.cnodes + (size_t)code * 4;
+            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), e = __ldg(np + 3);
+            if (cnt) cnt->nodes += 2;
+            float tel, ter;
+            bool hl = box_hit_te(a.x, a.y, a.z, b.x, b.y, b.z, o, inv, tmin, closest, tel);
+            bool hr = box_hit_te(c.x, c.y, c.z, e.x, e.y, e.z, o, inv, tmin, closest, ter);
+            int axis = __float_as_int(c.w);
+            float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
+            bool left_near = da >= 0.0f;
+            int lc = __float_as_int(a.w), rc = __float_as_int(b.w);
+            int nc = left_near ? lc : rc, fc = left_near ? rc : lc;
+            bool hn = left_near ? hl : hr, hf = left_near ? hr : hl;
+            float tf = left_near ? ter : tel;
+            if (hn && hf) {
+                if (sp >= STACK) {
+                    *err = RT_ERR_STACK;
+                    ok = false;
+                    return true;
+                }
+                st_code[sp] = fc;
+                st_te[sp] = tf;
+                sp++;
+            }
+            code = hn ? nc : (hf ? fc : kNone);
+        }
+        // A leaf (or nothing): primitives in order.
+        if (code != kNone) {
+            int v = ~code;
+            int first = v >> 5;
+            int kind = (v >> 3) & 3;
+            int count = (v & 7) + 1;
+            code = kNone;
+            if (kind == LEAF_ENT1) {
+                Entity en = s.entities[first];
+                if (en.kind == ENT_MESH) {   // Mesh.Hit -> its BVH root (box test) or flat list
+                    if (en.index >= 0) {
+                        if (cnt) cnt->nodes++;
+                        float4 lo = __ldg(s.ent_box + 2 * first), hi = __ldg(s.ent_box + 2 * first + 1);
+                        float te;
+                        if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
+                            code = en.index;
+                            return false;
+                        }
+                    } else {
+                        code = en.index;   // <= 4 triangles: HittableList, no box test
+                        return false;
+                    }
+                } else {
+                    if (cnt) cnt->others++;
+                    Hit h;
+                    if (entity_test(s, first, o, d, tmin, closest, h)) {
+                        best = h;
+                        closest = h.t;
+                        if (ANY) return true;
+                    }
+                }
+            } else if (kind == LEAF_ENTS) {   // top-level fat leaf: entities in order
+                if (sp + count > STACK) {
+                    *err = RT_ERR_STACK;
+                    ok = false;
+                    return true;
+                }
+                for (int i = count - 1; i >= 0; --i) {
+                    st_code[sp] = leaf_code(s.top_items[first + i], LEAF_ENT1, 1);
+                    st_te[sp] = -kInf;
+                    sp++;
+                }
+            } else {   // triangle leaf (or a mesh's flat list)
+                for (int i = 0; i < count; i++) {
+                    float t, u, vv;
+                    if (cnt) cnt->tris++;
+                    if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, vv)) {
+                        best = Hit{t, u, vv, HIT_TRI, first + i};
+                        closest = t;
+                        if (ANY) return true;
+                    }
+                }
+            }
+        }
+        // Pop the next entry the current closest t does not prune.
+        while (sp > 0) {
+            --sp;
+            if (!(st_te[sp] > closest)) {
+                code = st_code[sp];
+                break;
+            }
+        }
+        return code == kNone;
+    }
+};
+
+// One walk to the end. The same walk as Walker, in one loop (kept separate:
+// the one-shot form compiles to a smaller stack frame and runs faster).
 template <bool ANY, int STACK>
 __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
                                          TravCounters* cnt, int* err, bool has_root = false, int root = 0) {

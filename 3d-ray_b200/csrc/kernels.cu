@@ -64,7 +64,7 @@ struct RtScene {
     size_t scratch_bytes = 0;
     int* d_err = nullptr;
     int tuned = 0;                 // rt_autotune ran: use the fields below
-    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2;
+    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2, tuned_fetch = 1;
     // Copy of the world description: rt_scene_set_params rebuilds from it.
     std::vector<RtMaterialDesc> w_materials;
     std::vector<RtEntityDesc> w_entities;
@@ -510,6 +510,7 @@ struct WfConfig {
     int sort = 1;
     int profile = 0;   // per-kernel events instead of the graph
     int layout = 2;    // BVH records of extend/occlude: 2 or 4 wide
+    int fetch = 1;     // 1 one ray per thread, 2 persistent warps with dynamic fetch (two-wide only)
 };
 
 int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st) {
@@ -665,6 +666,16 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     int blk = cfg.block;
     bool l4 = cfg.layout == 4;
     for (const HostReq& q : reqs) l4 = l4 && q.scene->host.max_stack4 <= kStack;
+    bool pt = !l4 && cfg.fetch == 2;
+    unsigned gpt_e = 1, gpt_o = 1;
+    if (pt) {
+        int sms = 148, nb_e = 1, nb_o = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_e, rt::k_wf_extend_pt<kStack>, blk, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_o, rt::k_wf_occlude_pt<kStack>, blk, 0);
+        gpt_e = (unsigned)std::max(1, nb_e * sms);
+        gpt_o = (unsigned)std::max(1, nb_o * sms);
+    }
     unsigned gs = (unsigned)((nslots + blk - 1) / blk);
     unsigned gsh = (unsigned)((cap + blk - 1) / blk);
     unsigned g256 = (unsigned)((nslots + 255) / 256);
@@ -675,6 +686,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         rt::k_wf_regen<<<g256, 256, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[1], stream);
         if (l4) rt::k_wf_extend<kStack, true><<<gs, blk, 0, stream>>>(a);
+        else if (pt) rt::k_wf_extend_pt<kStack><<<gpt_e, blk, 0, stream>>>(a);
         else rt::k_wf_extend<kStack, false><<<gs, blk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[2], stream);
         if (sort) {
@@ -685,6 +697,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         rt::k_wf_shade<<<gs, blk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[4], stream);
         if (l4) rt::k_wf_occlude<kStack, true><<<gsh, blk, 0, stream>>>(a);
+        else if (pt && a.opaque) rt::k_wf_occlude_pt<kStack><<<gpt_o, blk, 0, stream>>>(a);
         else rt::k_wf_occlude<kStack, false><<<gsh, blk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[5], stream);
     };
@@ -809,11 +822,13 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
         cfg.block = sc->tuned_block;
         cfg.sort = sc->tuned_sort;
         cfg.layout = sc->tuned_layout;
+        cfg.fetch = sc->tuned_fetch;
     }
     if (p->wavefront_size > 0) cfg.slots = p->wavefront_size;
     if (p->block_size > 0) cfg.block = p->block_size;
     if (p->sort_materials >= 0) cfg.sort = p->sort_materials;
     if (p->node_layout == 2 || p->node_layout == 4) cfg.layout = p->node_layout;
+    if (p->ray_fetch == 1 || p->ray_fetch == 2) cfg.fetch = p->ray_fetch;
     cfg.profile = p->profile_kernels != 0;
     if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
         return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
@@ -1175,11 +1190,13 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
             cfg.block = s0->tuned_block;
             cfg.sort = s0->tuned_sort;
             cfg.layout = s0->tuned_layout;
+            cfg.fetch = s0->tuned_fetch;
         }
         if (common->wavefront_size > 0) cfg.slots = common->wavefront_size;
         if (common->block_size > 0) cfg.block = common->block_size;
         if (common->sort_materials >= 0) cfg.sort = common->sort_materials;
         if (common->node_layout == 2 || common->node_layout == 4) cfg.layout = common->node_layout;
+        if (common->ray_fetch == 1 || common->ray_fetch == 2) cfg.fetch = common->ray_fetch;
         rc = wf_render(hq, cfg, st);
     }
     for (int i = 0; i < n; i++) {
@@ -1227,6 +1244,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
                     p.block_size = blocks[bi];
                     p.sort_materials = so;
                     p.node_layout = layouts[li];
+                    p.ray_fetch = 1;
                     RtStats s1{};
                     rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
                     if (rc == RT_OK && s1.kernel_ms < best_ms) {
@@ -1237,6 +1255,23 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
                         pick.layout = layouts[li];
                     }
                 }
+    if (rc == RT_OK && pick.layout == 2) {   // then the persistent dynamic-fetch kernels on the winner
+        RtRenderParams p = *params;
+        p.kernel = RT_KERNEL_WAVEFRONT;
+        p.spp = spp;
+        p.count_work = 0;
+        p.wavefront_size = pick.slots;
+        p.block_size = pick.block;
+        p.sort_materials = pick.sort;
+        p.node_layout = 2;
+        p.ray_fetch = 2;
+        RtStats s1{};
+        rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
+        if (rc == RT_OK && s1.kernel_ms < best_ms) {
+            best_ms = s1.kernel_ms;
+            pick.fetch = 2;
+        }
+    }
     cudaFree(d_film);
     if (rc != RT_OK) return rc;
     sc->tuned = 1;
@@ -1244,6 +1279,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
     sc->tuned_block = pick.block;
     sc->tuned_sort = pick.sort;
     sc->tuned_layout = pick.layout;
+    sc->tuned_fetch = pick.fetch;
     if (best) {
         *best = *params;
         best->kernel = RT_KERNEL_WAVEFRONT;
@@ -1251,6 +1287,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
         best->block_size = pick.block;
         best->sort_materials = pick.sort;
         best->node_layout = pick.layout;
+        best->ray_fetch = pick.fetch;
     }
     return RT_OK;
 }

@@ -71,6 +71,9 @@ struct WfCtl {
     unsigned long long total;   // total work ids
     int live;                   // slots alive or done after the last regen
     int overflow;               // shadow queue overflow (never expected: sized by the host)
+    // (the host reads next, then live and overflow as one 8-byte copy: keep them adjacent)
+    unsigned ext_next;          // persistent extend: next slot to fetch
+    unsigned occ_next;          // persistent occlude: next shadow record to fetch
     int hist[256];              // material histogram (sorting)
 };
 
@@ -224,17 +227,8 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
     atomicAdd(&a.ctl->live, 1);
 }
 
-template <int STACK, bool L4>
-__global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nslots) return;
-    float4 d = a.P.d[i];
-    if (!(fbits(d.w) & PF_ALIVE)) return;
-    float4 o = a.P.o[i];
-    int req = fbits(a.P.pre[i].w);
-    const SceneView& s = a.views[a.reqs[req].scene];
-    Hit h;
-    trace<false, STACK, L4>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf, h, nullptr, a.err);
+// Stores slot i's closest hit and, when sorting, its material key.
+RT_D void extend_store(const WfArgs& a, int i, int req, const SceneView& s, const Hit& h) {
     int packed = h.kind == HIT_NONE ? 0 : ((h.kind << 30) | h.slot);
     a.P.hit[i] = make_float4(h.t, h.u, h.v, ibits(packed));
     if (a.sort) {   // material key for the counting sort
@@ -247,6 +241,73 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
         // one atomic per distinct key in the warp (__match_any_sync groups lanes)
         unsigned grp = __match_any_sync(__activemask(), key);
         if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&a.ctl->hist[key], __popc(grp));
+    }
+}
+
+// One thread per slot.
+template <int STACK, bool L4>
+__global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nslots) return;
+    float4 d = a.P.d[i];
+    if (!(fbits(d.w) & PF_ALIVE)) return;
+    float4 o = a.P.o[i];
+    int req = fbits(a.P.pre[i].w);
+    const SceneView& s = a.views[a.reqs[req].scene];
+    Hit h;
+    trace<false, STACK, L4>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf, h, nullptr, a.err);
+    extend_store(a, i, req, s, h);
+}
+
+// Persistent form with dynamic ray fetch (Aila and Laine 2009): a grid sized
+// to fill the GPU once walks rays in rounds (Walker::step). Between rounds,
+// once kRefill lanes of a warp have finished (or all of them), the finished
+// lanes take the next slots from a global counter, so a few long rays no
+// longer keep a warp whose other lanes are done. The rays, their walks and
+// their results are those of the one-thread-per-slot kernel.
+constexpr int kRefill = 8;
+
+template <int STACK>
+__global__ void __launch_bounds__(256) k_wf_extend_pt(WfArgs a) {
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    Walker<false, STACK> w;
+    int slot = -1, req = 0;
+    bool exhausted = false;
+    for (;;) {
+        bool idle = slot < 0 && !exhausted;
+        unsigned need = __ballot_sync(full, idle);
+        unsigned busy = __ballot_sync(full, slot >= 0);
+        if (!need && !busy) break;
+        if (need && (__popc(need) >= kRefill || !busy)) {
+            int leader = __ffs(need) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(&a.ctl->ext_next, (unsigned)__popc(need));
+            base = __shfl_sync(full, base, leader);
+            if (idle) {
+                unsigned i = base + (unsigned)__popc(need & ((1u << lane) - 1u));
+                if (i >= (unsigned)a.nslots) {
+                    exhausted = true;
+                } else {
+                    float4 d = a.P.d[i];
+                    if (fbits(d.w) & PF_ALIVE) {
+                        float4 o = a.P.o[i];
+                        req = fbits(a.P.pre[i].w);
+                        slot = (int)i;
+                        w.start(a.views[a.reqs[req].scene], v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf,
+                                nullptr, false, 0);
+                    }
+                }
+            }
+            continue;
+        }
+        if (slot >= 0) {
+            const SceneView& s = a.views[a.reqs[req].scene];
+            if (w.step(s, nullptr, a.err)) {
+                extend_store(a, slot, req, s, w.best);
+                slot = -1;
+            }
+        }
     }
 }
 
@@ -339,6 +400,56 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
     wf_store_media(a, i, R, ps);
 }
 
+// Persistent any-hit for opaque batches (the walk is one any-hit traversal):
+// the dynamic-fetch scheme of k_wf_extend_pt over the shadow queue.
+template <int STACK>
+__global__ void __launch_bounds__(256) k_wf_occlude_pt(WfArgs a) {
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    int n = min(*a.S.count, a.S.capacity);
+    Walker<true, STACK> w;
+    int rec = -1;
+    bool exhausted = false;
+    for (;;) {
+        bool idle = rec < 0 && !exhausted;
+        unsigned need = __ballot_sync(full, idle);
+        unsigned busy = __ballot_sync(full, rec >= 0);
+        if (!need && !busy) break;
+        if (need && (__popc(need) >= kRefill || !busy)) {
+            int leader = __ffs(need) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(&a.ctl->occ_next, (unsigned)__popc(need));
+            base = __shfl_sync(full, base, leader);
+            if (idle) {
+                unsigned j = base + (unsigned)__popc(need & ((1u << lane) - 1u));
+                if (j >= (unsigned)n) {
+                    exhausted = true;
+                } else {
+                    float4 o = a.S.o[j], d = a.S.d[j], c = a.S.c[j];
+                    rec = (int)j;
+                    w.start(a.views[fbits(c.w)], v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, o.w, nullptr, false, 0);
+                }
+            }
+            continue;
+        }
+        if (rec >= 0) {
+            float4 c = a.S.c[rec];
+            if (w.step(a.views[fbits(c.w)], nullptr, a.err)) {
+                if (w.best.kind == HIT_NONE) {   // visible: transmittance 1
+                    int packed = fbits(a.S.d[rec].w);
+                    int slot = packed >> 1;
+                    float4* dst = (packed & 1) ? (a.P.la + slot) : (a.P.lp + slot);
+                    float* f = reinterpret_cast<float*>(dst);
+                    atomicAdd(f, c.x);
+                    atomicAdd(f + 1, c.y);
+                    atomicAdd(f + 2, c.z);
+                }
+                rec = -1;
+            }
+        }
+    }
+}
+
 template <int STACK, bool L4>
 __global__ void __launch_bounds__(256) k_wf_occlude(WfArgs a) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -365,6 +476,8 @@ __global__ void k_wf_reset(WfArgs a) {
     if (t == 0) {
         *a.S.count = 0;
         a.ctl->live = 0;
+        a.ctl->ext_next = 0;
+        a.ctl->occ_next = 0;
     }
     if (a.sort)
         for (int k = t; k <= a.nkeys; k += blockDim.x) a.ctl->hist[k] = 0;

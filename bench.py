@@ -266,12 +266,14 @@ def profile_frame(args):
     abi.check(lib.rt_scene_create(pw.ref(), C.byref(scene)), "rt_scene_create")
     kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
     p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=256,
-                          sort_materials=1, node_layout=args.node_layout, profile_kernels=int(args.split))
+                          sort_materials=1, node_layout=args.node_layout, ray_fetch=args.ray_fetch,
+                          profile_kernels=int(args.split))
     film = np.zeros((3, H, W), np.float32)
     st = abi.RtStats()
     for i in range(2):
         abi.check(lib.rt_render(scene, C.byref(p), film.ctypes.data_as(C.c_void_p), C.byref(st)), "rt_render")
-        line = {"frame": i, "kernel": args.kernel, "node_layout": args.node_layout, "spp": args.spp,
+        line = {"frame": i, "kernel": args.kernel, "node_layout": args.node_layout, "ray_fetch": args.ray_fetch,
+                "spp": args.spp,
                 "kernel_ms": st.kernel_ms, "Msamples_per_s": W * H * args.spp / st.kernel_ms / 1e3,
                 "iterations": st.iterations, "launches": st.kernel_launches}
         if args.split:
@@ -453,6 +455,8 @@ def main():
     ap.add_argument("--node-layout", type=int, default=2, choices=[2, 4],
                     help="BVH records for --profile-frame: two-wide or four-wide")
     ap.add_argument("--split", action="store_true", help="--profile-frame: per-kernel event times")
+    ap.add_argument("--ray-fetch", type=int, default=1, choices=[1, 2],
+                    help="--profile-frame: one ray per thread (1) or persistent dynamic fetch (2)")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
     ap.add_argument("--gradcheck", action="store_true",
                     help="adjoint gradients against central finite differences (C4, C5) and exit")
@@ -486,7 +490,8 @@ def main():
         best = abi.RtRenderParams()
         abi.check(lib.rt_autotune(scene, C.byref(params), C.byref(best)), "rt_autotune")
         tuned = {"wavefront_size": best.wavefront_size, "block_size": best.block_size,
-                 "sort_materials": best.sort_materials, "node_layout": best.node_layout}
+                 "sort_materials": best.sort_materials, "node_layout": best.node_layout,
+                 "ray_fetch": best.ray_fetch}
     film = torch.empty((3, H, W), dtype=torch.float32, device="cuda")
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 

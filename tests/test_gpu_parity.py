@@ -432,3 +432,22 @@ def test_four_wide_layout_renders_like_two_wide(throughput_world_small, volume_w
             np.testing.assert_allclose(imgs[0], imgs[1], rtol=1e-4, atol=1e-6)
         finally:
             s.close()
+
+
+def test_persistent_fetch_renders_like_one_ray_per_thread(throughput_world_small, volume_world):
+    """Persistent extend/occlude warps that refill finished lanes walk the same
+    rays as one thread per ray: same images up to the order of the float
+    additions (opaque scene: both kernels persistent; glass: extend only)."""
+    for world in (throughput_world_small, volume_world):
+        s = Scene(world)
+        try:
+            imgs = []
+            for fetch in (1, 2):
+                p = abi.render_params(64, 48, 64, 12, kernel=abi.KERNEL_WAVEFRONT, wavefront_size=1 << 15,
+                                      node_layout=2, ray_fetch=fetch)
+                img, st = s.render(p)
+                assert st.samples == 64 * 48 * 64
+                imgs.append(img)
+            np.testing.assert_allclose(imgs[0], imgs[1], rtol=1e-4, atol=1e-6)
+        finally:
+            s.close()
