@@ -186,15 +186,20 @@ RT_D int find_request(const WfRequest* reqs, int n, unsigned long long id) {
 }
 
 __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
+    // Work ids come from the global counter with one atomic per block (a
+    // ballot prefix over the block's free slots), and the live count with one
+    // more: a per-warp atomic on one address serialised in L2.
+    __shared__ int s_warp[8];   // blockDim 256: per-warp free-slot offsets
+    __shared__ unsigned long long s_base;
+    __shared__ int s_live;
+    const unsigned full = 0xffffffffu;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nslots) return;
-    float4 d = a.P.d[i];
-    int flags = fbits(d.w);
-    if (flags & PF_ALIVE) {
-        atomicAdd(&a.ctl->live, 1);
-        return;
-    }
-    if (flags & PF_DONE) {   // resolve the finished sample into its film
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    bool in = i < a.nslots;
+    int flags = in ? fbits(a.P.d[i].w) : 0;
+    bool alive = in && (flags & PF_ALIVE);
+    bool need = in && !alive;
+    if (need && (flags & PF_DONE)) {   // resolve the finished sample into its film
         int req = fbits(a.P.pre[i].w);
         const WfRequest& R = a.reqs[req];
         PathState ps;
@@ -207,24 +212,45 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
         atomicAdd(R.accum + plane + k, L.y);
         atomicAdd(R.accum + 2 * plane + k, L.z);
     }
-    unsigned long long id = wagg_next(&a.ctl->next);
-    if (id >= a.ctl->total) {
-        a.P.d[i].w = ibits(0);
-        return;
+    unsigned m = __ballot_sync(full, need);
+    if (lane == 0) s_warp[wid] = __popc(m);
+    if (threadIdx.x == 0) s_live = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            int c = s_warp[w];
+            s_warp[w] = tot;
+            tot += c;
+        }
+        s_base = tot ? atomicAdd(&a.ctl->next, (unsigned long long)tot) : 0ull;
     }
-    int req = find_request(a.reqs, a.nreq, id);
-    const WfRequest& R = a.reqs[req];
-    long long local = (long long)(id - (unsigned long long)R.begin);
-    long long npix = (long long)R.ww * R.wh;
-    int s = (int)(local / npix);
-    int p = (int)(local % npix);
-    int lx = p % R.ww, ly = p / R.ww;
-    PathState ps;
-    path_init(ps, R.rc, R.x0 + lx, R.y0 + ly, (uint32_t)(R.spp0 + s));
-    int alive = path_alive(ps);
-    wf_store(a, i, ps, wf_flags(ps, alive), req, lx | (ly << 16));
-    wf_store_media(a, i, R, ps);
-    atomicAdd(&a.ctl->live, 1);
+    __syncthreads();
+    bool live = alive;
+    if (need) {
+        unsigned long long id = s_base + (unsigned long long)(s_warp[wid] + __popc(m & ((1u << lane) - 1u)));
+        if (id >= a.ctl->total) {
+            a.P.d[i].w = ibits(0);
+        } else {
+            int req = find_request(a.reqs, a.nreq, id);
+            const WfRequest& R = a.reqs[req];
+            long long local = (long long)(id - (unsigned long long)R.begin);
+            long long npix = (long long)R.ww * R.wh;
+            int s = (int)(local / npix);
+            int p = (int)(local % npix);
+            int lx = p % R.ww, ly = p / R.ww;
+            PathState ps;
+            path_init(ps, R.rc, R.x0 + lx, R.y0 + ly, (uint32_t)(R.spp0 + s));
+            int al = path_alive(ps);
+            wf_store(a, i, ps, wf_flags(ps, al), req, lx | (ly << 16));
+            wf_store_media(a, i, R, ps);
+            live = true;
+        }
+    }
+    int wl = __popc(__ballot_sync(full, live));
+    if (lane == 0 && wl) atomicAdd(&s_live, wl);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_live) atomicAdd(&a.ctl->live, s_live);
 }
 
 // Stores slot i's closest hit and, when sorting, its material key.
@@ -344,6 +370,7 @@ __global__ void k_wf_scatter(WfArgs a) {
     a.P.order[base + rank] = i;
 }
 
+// Shadow sink of the wavefront: queue the ray with its contribution.
 // Shadow sink of the wavefront: queue the ray with its contribution.
 struct QueueShadows : NoAdjoint {
     const WfArgs* a;
