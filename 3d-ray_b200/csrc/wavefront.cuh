@@ -393,7 +393,11 @@ struct QueueShadows : NoAdjoint {
     RT_D void skipped(V3, V3, float) {}
 };
 
-__global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
+// Minimum resident blocks of 256 for shade (a register budget); a build knob.
+#ifndef RT_SHADE_MIN_BLOCKS
+#define RT_SHADE_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int i;
     if (a.sort) {
