@@ -160,34 +160,46 @@ def oracle_scene(rt, world):
     return binding.OracleScene(rt.abi.PackedWorld(world))
 
 
-def cpu_baseline(rt, world, budget_s=12.0, osc=None):
-    """Times the oracle on a bounded pixel window of the same frame (the scene
-    build, like the reference's, is outside the timing)."""
+def cpu_baseline(rt, world, budget_s=12.0, osc=None, runs=5):
+    """Times the oracle on a bounded sample of the same frame (the scene build,
+    like the reference's, is outside the timing): full-width pixel rows spread
+    evenly over the frame's height, so the sample has the frame's mix of cheap
+    and expensive pixels. An untimed warm-up, then the median of `runs` timed
+    passes, sized so the passes take about budget_s together."""
     own = osc is None
     if own:
         osc = oracle_scene(rt, world)
     cores = os.cpu_count() or 1
-    win_w, win_h = 64, 16
-    # Calibrate with a small window, then size the window for ~budget_s.
-    p = rt.abi.render_params(W, H, SPP, DEPTH, pixel_x0=W // 2 - win_w // 2, pixel_y0=H // 2 - win_h // 2,
-                             window_w=win_w, window_h=win_h)
+
+    def row(y):
+        return rt.abi.render_params(W, H, SPP, DEPTH, pixel_x0=0, pixel_y0=y, window_w=W, window_h=1)
+
+    # warm-up and calibration on two rows
+    cal = [row(H // 3), row(2 * H // 3)]
     t = time.perf_counter()
-    osc.render(p, threads=cores)
-    dt = time.perf_counter() - t
-    rate = win_w * win_h * SPP / dt
-    rows = int(max(16, min(H // 2, budget_s * rate / (win_w * 4 * SPP))))
-    win_w2, win_h2 = win_w * 4, rows
-    p = rt.abi.render_params(W, H, SPP, DEPTH, pixel_x0=W // 2 - win_w2 // 2, pixel_y0=H // 2 - win_h2 // 2,
-                             window_w=win_w2, window_h=win_h2)
-    t = time.perf_counter()
-    osc.render(p, threads=cores)
-    dt = time.perf_counter() - t
-    samples = win_w2 * win_h2 * SPP
+    for p in cal:
+        osc.render(p, threads=cores)
+    rate = 2 * W * SPP / (time.perf_counter() - t)
+    nrows = int(max(2, min(64, budget_s / runs * rate / (W * SPP))))
+    rows = [row(int((k + 0.5) * H / nrows)) for k in range(nrows)]
+    times = []
+    for _ in range(runs):
+        t = time.perf_counter()
+        for p in rows:
+            osc.render(p, threads=cores)
+        times.append(time.perf_counter() - t)
+    dt = statistics.median(times)
+    samples = nrows * W * SPP
     if own:
         osc.close()
-    return {"value": samples / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{win_w2}x{win_h2} centre pixels of the 1920x1080 frame at {SPP} spp, depth {DEPTH} "
-                      f"({samples} samples, {dt:.1f} s)"}
+    try:
+        import cpuinfo
+        model = cpuinfo.get_cpu_info().get("brand_raw", "")
+    except Exception:
+        model = ""
+    return {"value": samples / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "cpu": model,
+            "sample": f"{nrows} full-width rows evenly spread over the 1920x1080 frame at {SPP} spp, depth {DEPTH} "
+                      f"({samples} samples per pass; median of {runs} passes after a warm-up, {dt:.2f} s each)"}
 
 
 def run_reference(args):
@@ -281,6 +293,63 @@ def profile_frame(args):
                         occlude_ms=st.occlude_ms)
         print(json.dumps(line), flush=True)
     lib.rt_scene_destroy(scene)
+
+
+def c1_side(rt, lib, abi):
+    """C1: the Cornell box at 256x256, 64 spp, depth 8: the plain megakernel
+    and the autotuned wavefront (device time, third of three renders), and the
+    oracle on all host cores over a 256x64 band (median of 3)."""
+    world = rt.scenes.cornell()
+    pw = abi.PackedWorld(world)
+    h = C.c_void_p()
+    abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
+    film = np.zeros((3, 256, 256), np.float32)
+    out = {"workload": "cornell 256x256 64spp depth 8"}
+    base = abi.render_params(256, 256, 64, 8, kernel=abi.KERNEL_WAVEFRONT)
+    best = abi.RtRenderParams()
+    abi.check(lib.rt_autotune(h, C.byref(base), C.byref(best)), "rt_autotune")
+    for name, kern in (("megakernel", abi.KERNEL_MEGAKERNEL), ("wavefront", abi.KERNEL_WAVEFRONT)):
+        p = abi.render_params(256, 256, 64, 8, kernel=kern)
+        st = abi.RtStats()
+        for _ in range(3):
+            abi.check(lib.rt_render(h, C.byref(p), film.ctypes.data_as(C.c_void_p), C.byref(st)), "c1")
+        out[name] = 256 * 256 * 64 / st.kernel_ms / 1e3
+    lib.rt_scene_destroy(h)
+    osc = oracle_scene(rt, world)
+    p = abi.render_params(256, 256, 64, 8, pixel_x0=0, pixel_y0=96, window_w=256, window_h=64)
+    cores = os.cpu_count() or 1
+    osc.render(p, threads=cores)
+    ts = []
+    for _ in range(3):
+        t = time.perf_counter()
+        osc.render(p, threads=cores)
+        ts.append(time.perf_counter() - t)
+    osc.close()
+    out["cpu_port"] = 256 * 64 * 64 / statistics.median(ts) / 1e6
+    out["unit"] = UNIT
+    out["cores"] = cores
+    return out
+
+
+def batched_side(rt):
+    """C3 (32 requests of uneven resolution, spp and depth over the icosphere
+    field and the Cornell box) and C5 (eight 512x512 views of the box with the
+    medium and the glass sphere, 512 spp, depth 16), each as one persistent
+    batched wavefront launch; device time."""
+    out = {}
+    reqs = rt.scenes.batch_requests()
+    films, st = rt.render_batch(reqs, [rt.scenes.throughput_scene(), rt.scenes.cornell()])
+    n = sum(r["width"] * r["height"] * r["spp"] for r in reqs)
+    out["c3_batch"] = {"requests": len(reqs), "samples": n, "seconds": st.kernel_ms / 1e3,
+                       "msamples_per_s": n / st.kernel_ms / 1e3, "launches": st.kernel_launches}
+    reqs5 = [dict(scene=0, width=512, height=512, spp=512, max_depth=16, camera=c)
+             for c in rt.scenes.volume_views()]
+    films, st = rt.render_batch(reqs5, [rt.scenes.cornell_volume()])
+    n = sum(r["width"] * r["height"] * r["spp"] for r in reqs5)
+    out["c5_views"] = {"views": len(reqs5), "samples": n, "seconds": st.kernel_ms / 1e3,
+                       "msamples_per_s": n / st.kernel_ms / 1e3,
+                       "finite": bool(all(np.isfinite(f).all() for f in films))}
+    return out
 
 
 def gradcheck(args):
@@ -393,7 +462,7 @@ def fit(args):
         th[e_idx] = ev
         return th
 
-    res = 256
+    res = args.res
     ds.set_params(vec(truth_s, truth_e))
     tp = abi.render_params(res, res, 1024, 8, kernel=abi.KERNEL_WAVEFRONT, spp_offset=1 << 24)
     target = ds.render(tp)
@@ -438,7 +507,7 @@ def fit(args):
         "radiance_rel_err_init": list(map(float, np.abs(init_e / truth_e - 1))),
         "radiance_rel_err_final": list(map(float, np.abs(final_e / truth_e - 1))),
         "seconds": wall, "adjoint_ms_per_step": adj_ms / steps,
-        "loss_curve_every_20": [float(h) for h in hist[::20]]}), flush=True)
+        "loss_curve": [float(h) for h in hist[::max(1, steps // 10)]]}), flush=True)
     ds.close()
 
 
@@ -458,6 +527,7 @@ def main():
     ap.add_argument("--ray-fetch", type=int, default=1, choices=[1, 2],
                     help="--profile-frame: one ray per thread (1) or persistent dynamic fetch (2)")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
+    ap.add_argument("--res", type=int, default=256, help="--fit: square image size")
     ap.add_argument("--gradcheck", action="store_true",
                     help="adjoint gradients against central finite differences (C4, C5) and exit")
     ap.add_argument("--profile-frame", action="store_true",
@@ -603,13 +673,13 @@ def main():
     # project micro-benchmark (L2-only float4 streams over a 32 MiB buffer).
     l2_peak = C.c_double(0.0)
     if lib.rt_probe_l2_bandwidth(dev, 32 << 20, 64, C.byref(l2_peak)) == abi.RT_OK:
-        l2 = {"peak": l2_peak.value, "unit": "GB/s", "peak_source": "rt_probe_l2_bandwidth (32 MiB, 64 passes)",
-              "bytes_per_launch": l2_bytes}
+        l2r = {"peak": l2_peak.value, "unit": "GB/s", "peak_source": "rt_probe_l2_bandwidth (32 MiB, 64 passes)",
+               "bytes_per_launch": l2_bytes}
         if l2_bytes and "kernel_ms_per_step" in roof:
             per_launch_s = roof["kernel_ms_per_step"][roof["kernel"][5:]] / 1e3 / max(roof["launches_per_step"], 1)
-            l2["achieved"] = l2_bytes / per_launch_s / 1e9
-            l2["frac"] = l2["achieved"] / l2_peak.value
-        roof["l2"] = l2
+            l2r["achieved"] = l2_bytes / per_launch_s / 1e9
+            l2r["frac"] = l2r["achieved"] / l2_peak.value
+        roof["l2"] = l2r
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -628,6 +698,8 @@ def main():
         line["plain_kernel"] = {"value": mv, "unit": UNIT, "ms_per_step": mt, "speedup_wavefront": value / mv}
         if rank == 0:
             line["time_to_relmse_1e-3"] = time_to_relmse(rt, lib, abi)
+            line.update(batched_side(rt))
+            line["c1"] = c1_side(rt, lib, abi)
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rt, world)
     lib.rt_scene_destroy(scene)
