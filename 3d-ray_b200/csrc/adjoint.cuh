@@ -409,22 +409,6 @@ RT_D V3 clamp_lum_vjp(V3 cin, float mx, V3 g) {
     return r * keep;
 }
 
-// A BSDF derivative the replay records and evaluates at the end of the
-// sample (AdjointSink::flush): the dual-number code then runs in one phase,
-// with the warp converged, instead of interleaved with the path's own code.
-struct AdjEvent {
-    V3 V, L;           // view direction and the light (NEE) or scattered direction
-    V3 n, tg, bt;      // the surface frame inputs of shading_frame
-    V3 w;              // gradient weight per channel
-    V3 att_pre;        // scatter: attenuation before Russian roulette (score terms)
-    V3 null_dir;       // legacy scatter: the direction of the null sample
-    float cw;          // sampled scatter: |cos| / pdf
-    int mat;
-    int kind;          // -1: NEE (EvaluateDirect); else the SCATTER_* mode
-    int lobe, null_lobe;
-};
-constexpr int kAdjEvents = 8;
-
 // Per-thread adjoint state of one replayed sample, and the replay sink.
 struct AdjointSink {
     const SceneView* s;
@@ -447,9 +431,6 @@ struct AdjointSink {
     int sh_n;
     int sh_mat[8];
     float sh_len[8];       // >= 0: absorption length inside sh_mat; < 0: a crossing of sh_mat's surface
-    // deferred BSDF derivatives of this sample
-    AdjEvent evb[kAdjEvents];
-    int nev;
 
     RT_D void add(int i, float v) {
         if (v == 0.0f || !isfinite(v)) return;
@@ -617,68 +598,21 @@ struct AdjointSink {
         if (m.emission.z > 0.0f) add(b + 2, g.z / m.emission.z);
     }
 
-    // Evaluates one recorded derivative for every selected BSDF slot.
-    RT_NI void process(const AdjEvent& e) {
-        const Material& m = s->materials[e.mat];
-        Surface rec;
-        rec.n = e.n;
-        rec.tangent = e.tg;
-        rec.bitangent = e.bt;
-        rec.material = e.mat;
-        unsigned bits = mmask[e.mat] & ((1u << kAdjBsdfDirs) - 1u);
-        const float* p = params + e.mat * kAdjPerMat;
-        for (; bits; bits &= bits - 1u) {
-            int k = __ffs(bits) - 1;
-            DMat dm = dual_material(*s, m, p, k);
-            V3 da;
-            if (e.kind < 0) {
-                da = dpart(eval_direct_dual(*s, m, dm, rec, e.L, e.V));
-            } else if (e.kind == SCATTER_SAMPLED) {
-                da = dpart(eval_dual(*s, m, dm, rec, e.V, e.L)) * e.cw;
-            } else {
-                da = dpart(lobe_att_dual(*s, m, dm, rec, e.V, e.L, e.lobe));
-                float sc = 0.0f;
-                if (e.lobe >= 0 && e.lobe <= LOBE_CLEARCOAT && dm.pl[e.lobe].v < lobe_floor(e.lobe))
-                    sc += dlog(dm.pl[e.lobe]);
-                if (e.kind == SCATTER_LEGACY) sc += null_sample_score(m, dm, rec, e.V, e.null_lobe, e.null_dir);
-                da = da + e.att_pre * sc;
-            }
-            add(e.mat * kAdjPerMat + k, dot(e.w, da));
-        }
-    }
-    RT_D void record(const AdjEvent& e) {
-        if (nev < kAdjEvents) evb[nev++] = e;
-        else process(e);
-    }
-    // The end of a sample's replay: evaluate the recorded derivatives.
-    RT_NI void flush() {
-        for (int i = 0; i < nev; i++) process(evb[i]);
-        nev = 0;
-    }
-
     RT_NI void nee_surface(const PathState& ps, int li, const Material& m, const Surface& rec, V3 L, V3 V,
                            float term, V3 coef, float dist, V3 tr_m, int to_la) {
         if (!sh_added) return;
         nee_common(ps, li, dist, to_la);
         // the term is coef * (f_direct * term) * tr_m * tr: differentiate f_direct
-        if (!(mmask[rec.material] & ((1u << kAdjBsdfDirs) - 1u))) return;
+        unsigned bits = mmask[rec.material] & ((1u << kAdjBsdfDirs) - 1u);
+        if (!bits) return;
         V3 w = gain(ps, to_la) * coef * tr_m * sh_tr * term;
         if (is_zero(w)) return;
-        AdjEvent e;
-        e.V = V;
-        e.L = L;
-        e.n = rec.n;
-        e.tg = rec.tangent;
-        e.bt = rec.bitangent;
-        e.w = w;
-        e.att_pre = v3(0.0f);
-        e.null_dir = v3(0.0f);
-        e.cw = 0.0f;
-        e.mat = rec.material;
-        e.kind = -1;
-        e.lobe = -1;
-        e.null_lobe = -1;
-        record(e);
+        const float* p = params + rec.material * kAdjPerMat;
+        for (; bits; bits &= bits - 1u) {
+            int k = __ffs(bits) - 1;
+            DMat dm = dual_material(*s, m, p, k);
+            add(rec.material * kAdjPerMat + k, dot(w, dpart(eval_direct_dual(*s, m, dm, rec, L, V))));
+        }
     }
     RT_D void nee_medium(const PathState& ps, int li, float dist, int to_la) {
         if (sh_added) nee_common(ps, li, dist, to_la);
@@ -702,21 +636,22 @@ struct AdjointSink {
                       att_pre.z != 0.0f ? gs.z / att_pre.z : 0.0f);
         }
         if (is_zero(coef)) return;
-        AdjEvent e;
-        e.V = V;
-        e.L = dir;
-        e.n = rec.n;
-        e.tg = rec.tangent;
-        e.bt = rec.bitangent;
-        e.w = coef;
-        e.att_pre = att_pre;
-        e.null_dir = null_dir;
-        e.cw = mode == SCATTER_SAMPLED ? fabsf(dot(rec.n, dir)) / pdf : 1.0f;
-        e.mat = rec.material;
-        e.kind = mode;
-        e.lobe = lobe;
-        e.null_lobe = null_lobe;
-        record(e);
+        float cw = 1.0f;
+        if (mode == SCATTER_SAMPLED) cw = fabsf(dot(rec.n, dir)) / pdf;
+        const float* p = params + rec.material * kAdjPerMat;
+        for (; bits; bits &= bits - 1u) {
+            int k = __ffs(bits) - 1;
+            DMat dm = dual_material(*s, m, p, k);
+            V3 da = mode == SCATTER_SAMPLED ? dpart(eval_dual(*s, m, dm, rec, V, dir)) * cw
+                                            : dpart(lobe_att_dual(*s, m, dm, rec, V, dir, lobe));
+            if (mode != SCATTER_SAMPLED) {
+                float sc = 0.0f;
+                if (lobe >= 0 && lobe <= LOBE_CLEARCOAT && dm.pl[lobe].v < lobe_floor(lobe)) sc += dlog(dm.pl[lobe]);
+                if (mode == SCATTER_LEGACY) sc += null_sample_score(m, dm, rec, V, null_lobe, null_dir);
+                da = da + att_pre * sc;
+            }
+            add(rec.material * kAdjPerMat + k, dot(coef, da));
+        }
     }
 };
 

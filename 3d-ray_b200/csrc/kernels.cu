@@ -217,7 +217,6 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(rt::SceneView s, rt::RenderC
         adj.abs_mat = -1;
         adj.sh_added = 0;
         adj.sh_n = 0;
-        adj.nev = 0;
         V3 A = ps.lp, X = rt::v3(0.0f), C = rt::v3(0.0f);
         if (ps.clamp_mode) {
             X = ps.att0 * rt::sanitize(ps.la);
@@ -244,7 +243,6 @@ __global__ void __launch_bounds__(kBlock) k_adjoint(rt::SceneView s, rt::RenderC
             rt::traverse<false, STACK>(s, ps.o, ps.d, rt::kEps, rt::kInf, h, nullptr, err);
             if (!rt::shade_vertex(s, rc, ps, h, adj)) break;
         }
-        adj.flush();
     }
     if (a.use_local) {   // warp sums of the per-thread accumulators
         int lane = threadIdx.x & 31;

@@ -277,7 +277,7 @@ def profile_frame(args):
     scene = C.c_void_p()
     abi.check(lib.rt_scene_create(pw.ref(), C.byref(scene)), "rt_scene_create")
     kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
-    p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=256,
+    p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=args.block,
                           sort_materials=1, node_layout=args.node_layout, ray_fetch=args.ray_fetch,
                           profile_kernels=int(args.split))
     film = np.zeros((3, H, W), np.float32)
@@ -524,6 +524,7 @@ def main():
     ap.add_argument("--node-layout", type=int, default=2, choices=[2, 4],
                     help="BVH records for --profile-frame: two-wide or four-wide")
     ap.add_argument("--split", action="store_true", help="--profile-frame: per-kernel event times")
+    ap.add_argument("--block", type=int, default=256, choices=[64, 128, 256], help="--profile-frame: block size")
     ap.add_argument("--ray-fetch", type=int, default=1, choices=[1, 2],
                     help="--profile-frame: one ray per thread (1) or persistent dynamic fetch (2)")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
