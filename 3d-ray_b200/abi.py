@@ -86,7 +86,8 @@ class RtRenderParams(C.Structure):
                 ("kernel", C.c_int32), ("block_size", C.c_int32), ("wavefront_size", C.c_int32),
                 ("sort_materials", C.c_int32), ("pixel_x0", C.c_int32), ("pixel_y0", C.c_int32),
                 ("window_w", C.c_int32), ("window_h", C.c_int32), ("count_work", C.c_int32), ("profile_kernels", C.c_int32),
-                ("node_layout", C.c_int32), ("ray_fetch", C.c_int32)]
+                ("node_layout", C.c_int32), ("ray_fetch", C.c_int32), ("trace_block_size", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class RtStats(C.Structure):

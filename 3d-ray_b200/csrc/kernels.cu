@@ -37,7 +37,7 @@ static_assert(sizeof(RtEntityDesc) == 80, "ABI layout");
 static_assert(sizeof(RtLightDesc) == 88, "ABI layout");
 static_assert(sizeof(RtCameraDesc) == 48, "ABI layout");
 static_assert(sizeof(RtMediumDesc) == 36, "ABI layout");
-static_assert(sizeof(RtRenderParams) == 96, "ABI layout");
+static_assert(sizeof(RtRenderParams) == 104, "ABI layout");
 static_assert(sizeof(RtStats) == 144, "ABI layout");
 static_assert(sizeof(RtBsdfQuery) == 96, "ABI layout");
 static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
@@ -64,7 +64,7 @@ struct RtScene {
     size_t scratch_bytes = 0;
     int* d_err = nullptr;
     int tuned = 0;                 // rt_autotune ran: use the fields below
-    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2, tuned_fetch = 1;
+    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2, tuned_fetch = 1, tuned_tblock = 0;
     // Copy of the world description: rt_scene_set_params rebuilds from it.
     std::vector<RtMaterialDesc> w_materials;
     std::vector<RtEntityDesc> w_entities;
@@ -511,6 +511,7 @@ struct WfConfig {
     int profile = 0;   // per-kernel events instead of the graph
     int layout = 2;    // BVH records of extend/occlude: 2 or 4 wide
     int fetch = 1;     // 1 one ray per thread, 2 persistent warps with dynamic fetch (two-wide only)
+    int tblock = 0;    // block of extend/occlude (0: block)
 };
 
 int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st) {
@@ -664,6 +665,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     CUDA_TRY(cudaStreamSynchronize(stream));   // host vectors above go out of scope
     // One iteration: reset, regen, extend, [scan, scatter], shade, occlude.
     int blk = cfg.block;
+    int tblk = cfg.tblock > 0 ? cfg.tblock : blk;
     bool l4 = cfg.layout == 4;
     for (const HostReq& q : reqs) l4 = l4 && q.scene->host.max_stack4 <= kStack;
     bool pt = !l4 && cfg.fetch == 2;
@@ -671,13 +673,14 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     if (pt) {
         int sms = 148, nb_e = 1, nb_o = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_e, rt::k_wf_extend_pt<kStack>, blk, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_o, rt::k_wf_occlude_pt<kStack>, blk, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_e, rt::k_wf_extend_pt<kStack>, tblk, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_o, rt::k_wf_occlude_pt<kStack>, tblk, 0);
         gpt_e = (unsigned)std::max(1, nb_e * sms);
         gpt_o = (unsigned)std::max(1, nb_o * sms);
     }
     unsigned gs = (unsigned)((nslots + blk - 1) / blk);
-    unsigned gsh = (unsigned)((cap + blk - 1) / blk);
+    unsigned gst = (unsigned)((nslots + tblk - 1) / tblk);
+    unsigned gsh = (unsigned)((cap + tblk - 1) / tblk);
     unsigned g256 = (unsigned)((nslots + 255) / 256);
     // ev (profiling only): boundaries between the kernel groups of one iteration.
     auto launch_iter = [&](cudaEvent_t* ev) {
@@ -685,9 +688,9 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         rt::k_wf_reset<<<1, 256, 0, stream>>>(a);
         rt::k_wf_regen<<<g256, 256, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[1], stream);
-        if (l4) rt::k_wf_extend<kStack, true><<<gs, blk, 0, stream>>>(a);
-        else if (pt) rt::k_wf_extend_pt<kStack><<<gpt_e, blk, 0, stream>>>(a);
-        else rt::k_wf_extend<kStack, false><<<gs, blk, 0, stream>>>(a);
+        if (l4) rt::k_wf_extend<kStack, true><<<gst, tblk, 0, stream>>>(a);
+        else if (pt) rt::k_wf_extend_pt<kStack><<<gpt_e, tblk, 0, stream>>>(a);
+        else rt::k_wf_extend<kStack, false><<<gst, tblk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[2], stream);
         if (sort) {
             rt::k_wf_scan<<<1, 256, 0, stream>>>(a);
@@ -696,9 +699,9 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         if (ev) cudaEventRecord(ev[3], stream);
         rt::k_wf_shade<<<gs, blk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[4], stream);
-        if (l4) rt::k_wf_occlude<kStack, true><<<gsh, blk, 0, stream>>>(a);
-        else if (pt && a.opaque) rt::k_wf_occlude_pt<kStack><<<gpt_o, blk, 0, stream>>>(a);
-        else rt::k_wf_occlude<kStack, false><<<gsh, blk, 0, stream>>>(a);
+        if (l4) rt::k_wf_occlude<kStack, true><<<gsh, tblk, 0, stream>>>(a);
+        else if (pt && a.opaque) rt::k_wf_occlude_pt<kStack><<<gpt_o, tblk, 0, stream>>>(a);
+        else rt::k_wf_occlude<kStack, false><<<gsh, tblk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[5], stream);
     };
     const int batch = 4;
@@ -823,15 +826,19 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
         cfg.sort = sc->tuned_sort;
         cfg.layout = sc->tuned_layout;
         cfg.fetch = sc->tuned_fetch;
+        cfg.tblock = sc->tuned_tblock;
     }
     if (p->wavefront_size > 0) cfg.slots = p->wavefront_size;
     if (p->block_size > 0) cfg.block = p->block_size;
     if (p->sort_materials >= 0) cfg.sort = p->sort_materials;
     if (p->node_layout == 2 || p->node_layout == 4) cfg.layout = p->node_layout;
     if (p->ray_fetch == 1 || p->ray_fetch == 2) cfg.fetch = p->ray_fetch;
+    if (p->trace_block_size > 0) cfg.tblock = p->trace_block_size;
     cfg.profile = p->profile_kernels != 0;
     if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
         return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
+    if (cfg.tblock != 0 && cfg.tblock != 64 && cfg.tblock != 128 && cfg.tblock != 256)
+        return fail(RT_ERR_INVALID_ARG, "trace_block_size must be 64, 128 or 256");
     if (p->window_w > 0 || p->window_h > 0)
         CUDA_TRY(cudaMemsetAsync(d_film, 0, (size_t)3 * p->width * p->height * sizeof(float), sc->stream));
     return wf_render({q}, cfg, st);
@@ -1191,12 +1198,14 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
             cfg.sort = s0->tuned_sort;
             cfg.layout = s0->tuned_layout;
             cfg.fetch = s0->tuned_fetch;
+            cfg.tblock = s0->tuned_tblock;
         }
         if (common->wavefront_size > 0) cfg.slots = common->wavefront_size;
         if (common->block_size > 0) cfg.block = common->block_size;
         if (common->sort_materials >= 0) cfg.sort = common->sort_materials;
         if (common->node_layout == 2 || common->node_layout == 4) cfg.layout = common->node_layout;
         if (common->ray_fetch == 1 || common->ray_fetch == 2) cfg.fetch = common->ray_fetch;
+        if (common->trace_block_size > 0) cfg.tblock = common->trace_block_size;
         rc = wf_render(hq, cfg, st);
     }
     for (int i = 0; i < n; i++) {
@@ -1245,6 +1254,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
                     p.sort_materials = so;
                     p.node_layout = layouts[li];
                     p.ray_fetch = 1;
+                    p.trace_block_size = blocks[bi];
                     RtStats s1{};
                     rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
                     if (rc == RT_OK && s1.kernel_ms < best_ms) {
@@ -1255,7 +1265,29 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
                         pick.layout = layouts[li];
                     }
                 }
-    if (rc == RT_OK && pick.layout == 2) {   // then the persistent dynamic-fetch kernels on the winner
+    pick.tblock = pick.block;
+    // then, on the winner, the block of extend/occlude alone and the
+    // persistent dynamic-fetch kernels
+    for (int bi = 0; bi < 3 && rc == RT_OK; bi++) {
+        if (blocks[bi] == pick.block) continue;
+        RtRenderParams p = *params;
+        p.kernel = RT_KERNEL_WAVEFRONT;
+        p.spp = spp;
+        p.count_work = 0;
+        p.wavefront_size = pick.slots;
+        p.block_size = pick.block;
+        p.sort_materials = pick.sort;
+        p.node_layout = pick.layout;
+        p.ray_fetch = 1;
+        p.trace_block_size = blocks[bi];
+        RtStats s1{};
+        rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
+        if (rc == RT_OK && s1.kernel_ms < best_ms) {
+            best_ms = s1.kernel_ms;
+            pick.tblock = blocks[bi];
+        }
+    }
+    if (rc == RT_OK && pick.layout == 2) {
         RtRenderParams p = *params;
         p.kernel = RT_KERNEL_WAVEFRONT;
         p.spp = spp;
@@ -1265,6 +1297,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
         p.sort_materials = pick.sort;
         p.node_layout = 2;
         p.ray_fetch = 2;
+        p.trace_block_size = pick.tblock;
         RtStats s1{};
         rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
         if (rc == RT_OK && s1.kernel_ms < best_ms) {
@@ -1280,6 +1313,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
     sc->tuned_sort = pick.sort;
     sc->tuned_layout = pick.layout;
     sc->tuned_fetch = pick.fetch;
+    sc->tuned_tblock = pick.tblock;
     if (best) {
         *best = *params;
         best->kernel = RT_KERNEL_WAVEFRONT;
@@ -1288,6 +1322,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
         best->sort_materials = pick.sort;
         best->node_layout = pick.layout;
         best->ray_fetch = pick.fetch;
+        best->trace_block_size = pick.tblock;
     }
     return RT_OK;
 }

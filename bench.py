@@ -277,7 +277,8 @@ def profile_frame(args):
     scene = C.c_void_p()
     abi.check(lib.rt_scene_create(pw.ref(), C.byref(scene)), "rt_scene_create")
     kern = abi.KERNEL_WAVEFRONT if args.kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
-    p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=args.block,
+    p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=256,
+                          trace_block_size=args.block,
                           sort_materials=1, node_layout=args.node_layout, ray_fetch=args.ray_fetch,
                           profile_kernels=int(args.split))
     film = np.zeros((3, H, W), np.float32)
@@ -524,7 +525,8 @@ def main():
     ap.add_argument("--node-layout", type=int, default=2, choices=[2, 4],
                     help="BVH records for --profile-frame: two-wide or four-wide")
     ap.add_argument("--split", action="store_true", help="--profile-frame: per-kernel event times")
-    ap.add_argument("--block", type=int, default=256, choices=[64, 128, 256], help="--profile-frame: block size")
+    ap.add_argument("--block", type=int, default=256, choices=[64, 128, 256],
+                    help="--profile-frame: block size of extend/occlude (the others use 256)")
     ap.add_argument("--ray-fetch", type=int, default=1, choices=[1, 2],
                     help="--profile-frame: one ray per thread (1) or persistent dynamic fetch (2)")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
@@ -562,7 +564,7 @@ def main():
         abi.check(lib.rt_autotune(scene, C.byref(params), C.byref(best)), "rt_autotune")
         tuned = {"wavefront_size": best.wavefront_size, "block_size": best.block_size,
                  "sort_materials": best.sort_materials, "node_layout": best.node_layout,
-                 "ray_fetch": best.ray_fetch}
+                 "ray_fetch": best.ray_fetch, "trace_block_size": best.trace_block_size}
     film = torch.empty((3, H, W), dtype=torch.float32, device="cuda")
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 

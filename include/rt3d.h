@@ -186,6 +186,9 @@ typedef struct RtRenderParams {
     int32_t ray_fetch;              /* wavefront extend/occlude on two-wide records: 1 one ray per
                                        thread, 2 persistent warps refilling finished lanes from a
                                        global counter, 0 the autotuned choice (else 1) */
+    int32_t trace_block_size;       /* block of the wavefront's extend/occlude: 64, 128 or 256;
+                                       0 the autotuned choice (else block_size) */
+    int32_t reserved;
 } RtRenderParams;
 
 /* Counters and timings of one call. */
@@ -298,10 +301,10 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
 
 /* Autotuner: times the wavefront over wavefront size {256K, 1M, 4M} x block
  * {64, 128, 256} x material sort {off, on} x node layout {two-wide,
- * four-wide}, then the persistent dynamic-fetch kernels on the winner, on a
- * bounded slice of `params` (the full window at the spp giving ~16 M
- * samples), keeps the fastest for this scene (used when those params fields
- * are 0 / -1) and returns it. */
+ * four-wide}, then, on the winner, the extend/occlude block {64, 128, 256}
+ * and the persistent dynamic-fetch kernels, on a bounded slice of `params`
+ * (the full window at the spp giving ~16 M samples), keeps the fastest for
+ * this scene (used when those params fields are 0 / -1) and returns it. */
 int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* best);
 
 /* ---- differentiation ----------------------------------------------------- */

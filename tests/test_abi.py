@@ -33,7 +33,7 @@ def test_abi_version(lib):
 
 
 @pytest.mark.parametrize("struct,size", [("RtMaterialDesc", 120), ("RtEntityDesc", 80), ("RtLightDesc", 88),
-                                         ("RtCameraDesc", 48), ("RtMediumDesc", 36), ("RtRenderParams", 96),
+                                         ("RtCameraDesc", 48), ("RtMediumDesc", 36), ("RtRenderParams", 104),
                                          ("RtStats", 144), ("RtBsdfQuery", 96), ("RtBsdfResult", 80),
                                          ("RtRequest", 72), ("RtSceneInfo", 56)])
 def test_struct_sizes(struct, size):
