@@ -63,6 +63,8 @@ struct RtScene {
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     int* d_err = nullptr;
+    float* film = nullptr;         // rt_render's device film, kept between calls
+    size_t film_bytes = 0;
     int tuned = 0;                 // rt_autotune ran: use the fields below
     int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2, tuned_fetch = 1, tuned_tblock = 0;
     // Copy of the world description: rt_scene_set_params rebuilds from it.
@@ -485,7 +487,8 @@ struct HostReq {
 struct WfWorkspace {
     void* mem = nullptr;
     size_t bytes = 0;
-    unsigned long long* pinned = nullptr;   // live / next / overflow read-back
+    unsigned long long* pinned = nullptr;   // two read-back slots of {next, live | overflow}
+    cudaEvent_t polled[2] = {nullptr, nullptr};   // each slot's read-back has landed
 };
 std::mutex g_wf_mu;
 WfWorkspace g_wf_ws[16];
@@ -604,6 +607,9 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     }
     if (!ws.pinned && cudaMallocHost(&ws.pinned, 4 * sizeof(unsigned long long)) != cudaSuccess)
         return fail(RT_ERR_OOM, "pinned read-back allocation failed");
+    for (cudaEvent_t& e : ws.polled)
+        if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return fail(RT_ERR_CUDA, "event creation failed");
     Carve cv{static_cast<char*>(ws.mem)};
     rt::WfArgs a{};
     auto* d_views = cv.take<rt::SceneView>(views.size());
@@ -730,6 +736,13 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     int64_t iters = 0;
     double t_regen = 0, t_extend = 0, t_sort = 0, t_shade = 0, t_occlude = 0;
     int rc = RT_OK;
+    // The poll is pipelined: batch k+1 is queued before the host waits for
+    // batch k's read-back, so the device does not idle while the host turns
+    // around. Replays after the wavefront has drained find no work and write
+    // nothing (the polled batches already ran up to batch-1 of them).
+    // Profiling waits for each batch itself, so its events are read before the
+    // next batch records them again.
+    int cur = 0, waiting = -1;
     CUDA_TRY(cudaEventRecord(s0->ev0, stream));
     for (;;) {
         for (int k = 0; k < batch; k++) {
@@ -742,10 +755,18 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         }
         if (rc != RT_OK) break;
         iters += batch;
-        cudaMemcpyAsync(ws.pinned, &d_ctl->next, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
-        cudaMemcpyAsync(reinterpret_cast<char*>(ws.pinned) + 8, &d_ctl->live, 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                        stream);
-        if (cudaStreamSynchronize(stream) != cudaSuccess) {
+        unsigned long long* slot = ws.pinned + 2 * cur;
+        cudaMemcpyAsync(slot, &d_ctl->next, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(slot + 1, &d_ctl->live, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream);
+        cudaEventRecord(ws.polled[cur], stream);
+        int check = cur;
+        if (!cfg.profile) {
+            check = waiting;
+            waiting = cur;
+            cur ^= 1;
+            if (check < 0) continue;   // first batch: queue the second before waiting
+        }
+        if (cudaEventSynchronize(ws.polled[check]) != cudaSuccess) {
             rc = fail(RT_ERR_CUDA, std::string("wavefront iteration failed: ") + cudaGetErrorString(cudaGetLastError()));
             break;
         }
@@ -760,9 +781,9 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
                 t_occlude += m[4];
             }
         }
-        unsigned long long next = ws.pinned[0];
-        int live = reinterpret_cast<int*>(ws.pinned)[2];
-        int overflow = reinterpret_cast<int*>(ws.pinned)[3];
+        unsigned long long next = ws.pinned[2 * check];
+        int live = reinterpret_cast<int*>(ws.pinned + 2 * check + 1)[0];
+        int overflow = reinterpret_cast<int*>(ws.pinned + 2 * check + 1)[1];
         if (overflow) {
             rc = fail(RT_ERR_BOUNDS, "shadow queue overflow");
             break;
@@ -946,6 +967,7 @@ int rt_scene_destroy(RtScene* sc) {
     for (void* p : sc->allocs) cudaFree(p);
     if (sc->scratch) cudaFree(sc->scratch);
     if (sc->d_err) cudaFree(sc->d_err);
+    if (sc->film) cudaFree(sc->film);
     if (sc->ev0) cudaEventDestroy(sc->ev0);
     if (sc->ev1) cudaEventDestroy(sc->ev1);
     if (sc->stream) cudaStreamDestroy(sc->stream);
@@ -1132,17 +1154,27 @@ int rt_render(RtScene* sc, const RtRenderParams* p, float* out, RtStats* st) {
     std::lock_guard<std::mutex> lk(sc->mu);
     auto t0 = std::chrono::steady_clock::now();
     size_t film_bytes = (size_t)3 * p->width * p->height * sizeof(float);
-    float* d_film = nullptr;
     if (p->width <= 0 || p->height <= 0) return fail(RT_ERR_INVALID_ARG, "bad image size");
     CUDA_TRY(cudaSetDevice(sc->device));
-    if (cudaMalloc(&d_film, film_bytes) != cudaSuccess) return fail(RT_ERR_OOM, "film allocation failed");
-    int rc = render_to_device(sc, p, sc->host.camera, d_film, st);
+    // The device film is kept by the scene and grown when a larger image asks
+    // for it, so repeated renders allocate nothing (cudaFree would also
+    // synchronise the whole device on every call).
+    if (sc->film_bytes < film_bytes) {
+        if (sc->film) cudaFree(sc->film);
+        sc->film = nullptr;
+        sc->film_bytes = 0;
+        if (cudaMalloc(&sc->film, film_bytes) != cudaSuccess) {
+            sc->film = nullptr;
+            return fail(RT_ERR_OOM, "film allocation failed");
+        }
+        sc->film_bytes = film_bytes;
+    }
+    int rc = render_to_device(sc, p, sc->host.camera, sc->film, st);
     if (rc == RT_OK) {
-        if (cudaMemcpyAsync(out, d_film, film_bytes, cudaMemcpyDeviceToHost, sc->stream) != cudaSuccess ||
+        if (cudaMemcpyAsync(out, sc->film, film_bytes, cudaMemcpyDeviceToHost, sc->stream) != cudaSuccess ||
             cudaStreamSynchronize(sc->stream) != cudaSuccess)
             rc = fail(RT_ERR_CUDA, "film copy failed");
     }
-    cudaFree(d_film);
     if (st && rc == RT_OK)
         st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
