@@ -87,7 +87,7 @@ class RtRenderParams(C.Structure):
                 ("sort_materials", C.c_int32), ("pixel_x0", C.c_int32), ("pixel_y0", C.c_int32),
                 ("window_w", C.c_int32), ("window_h", C.c_int32), ("count_work", C.c_int32), ("profile_kernels", C.c_int32),
                 ("node_layout", C.c_int32), ("ray_fetch", C.c_int32), ("trace_block_size", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("ray_groups", C.c_int32)]
 
 
 class RtStats(C.Structure):

@@ -66,7 +66,7 @@ struct RtScene {
     float* film = nullptr;         // rt_render's device film, kept between calls
     size_t film_bytes = 0;
     int tuned = 0;                 // rt_autotune ran: use the fields below
-    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2, tuned_fetch = 1, tuned_tblock = 0;
+    int tuned_slots = 0, tuned_block = 0, tuned_sort = 0, tuned_layout = 2, tuned_fetch = 1, tuned_tblock = 0, tuned_groups = 0;
     // Copy of the world description: rt_scene_set_params rebuilds from it.
     std::vector<RtMaterialDesc> w_materials;
     std::vector<RtEntityDesc> w_entities;
@@ -76,6 +76,46 @@ struct RtScene {
 };
 
 namespace {
+
+// The bounce-ray sort's box: per axis the 1st to 99th percentile of the
+// primitive centroids (triangles, quads, spheres), so that one large primitive
+// such as a ground plane does not stretch the cells over empty space.
+void ray_sort_box(const rt::HostScene& h, rt::SceneView& v) {
+    std::vector<float> c[3];
+    size_t ntri = h.tris.size() / 3;
+    for (int k = 0; k < 3; k++) c[k].reserve(ntri + h.quads.size() + h.spheres.size());
+    for (size_t i = 0; i < ntri; i++) {
+        const float4 &p0 = h.tris[3 * i], &e1 = h.tris[3 * i + 1], &e2 = h.tris[3 * i + 2];
+        c[0].push_back(p0.x + (e1.x + e2.x) / 3.0f);
+        c[1].push_back(p0.y + (e1.y + e2.y) / 3.0f);
+        c[2].push_back(p0.z + (e1.z + e2.z) / 3.0f);
+    }
+    for (const rt::QuadData& q : h.quads) {
+        rt::V3 m = q.q + 0.5f * (q.u + q.v);
+        c[0].push_back(m.x);
+        c[1].push_back(m.y);
+        c[2].push_back(m.z);
+    }
+    for (const rt::SphereData& sp : h.spheres) {
+        c[0].push_back(sp.c.x);
+        c[1].push_back(sp.c.y);
+        c[2].push_back(sp.c.z);
+    }
+    float lo[3] = {0, 0, 0}, scale[3] = {0, 0, 0};
+    for (int k = 0; k < 3; k++) {
+        std::vector<float>& a = c[k];
+        if (a.empty()) continue;
+        size_t i0 = a.size() / 100, i1 = a.size() - 1 - a.size() / 100;
+        std::nth_element(a.begin(), a.begin() + i0, a.end());
+        float l = a[i0];
+        std::nth_element(a.begin(), a.begin() + i1, a.end());
+        float hgh = a[i1];
+        lo[k] = l;
+        scale[k] = hgh > l ? 1.0f / (hgh - l) : 0.0f;
+    }
+    v.sort_lo = rt::v3(lo[0], lo[1], lo[2]);
+    v.sort_scale = rt::v3(scale[0], scale[1], scale[2]);
+}
 
 template <typename T>
 int upload(RtScene* sc, const std::vector<T>& v, const T** out) {
@@ -515,7 +555,19 @@ struct WfConfig {
     int layout = 2;    // BVH records of extend/occlude: 2 or 4 wide
     int fetch = 1;     // 1 one ray per thread, 2 persistent warps with dynamic fetch (two-wide only)
     int tblock = 0;    // block of extend/occlude (0: block)
+    int groups = 0;    // 1 slot order, 2 block-local regrouping, 3 sorted bounce rays; 0 default_groups
 };
+
+// Untuned ray order: the bounce-ray sort, except with a participating medium.
+// There nearly every slot is a bounce ray scattered in mid-air and the scene
+// is small, so the sort's key and rank in shade cost more than the coherence
+// wins back (measured: icosphere field +12%, Cornell box +12%, mixed batch
+// +10%, the medium scene -3%).
+int default_groups(const std::vector<RtScene*>& scenes) {
+    for (const RtScene* sc : scenes)
+        if (sc->host.has_medium) return 1;
+    return 3;
+}
 
 int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st) {
     auto t0 = std::chrono::steady_clock::now();
@@ -587,12 +639,15 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     for (int k = 0; k < 9; k++) add((size_t)nslots * sizeof(float4));
     add((size_t)nslots * sizeof(int));
     add((size_t)nslots * sizeof(int));
+    add((size_t)nslots * sizeof(int));
     if (dielectrics) {
         add((size_t)nslots * sizeof(float4));
         add((size_t)nslots * 8 * sizeof(float));
     }
     for (int k = 0; k < 3; k++) add((size_t)cap * sizeof(float4));
     add(sizeof(int));
+    add((size_t)rt::kRayKeys * sizeof(int));
+    add((size_t)rt::kRayKeys * sizeof(int));
     for (auto& q : wreq) add((size_t)3 * q.ww * q.wh * sizeof(float));
     add(reqs.size() * sizeof(float*));
     add(reqs.size() * sizeof(int) * 2);
@@ -627,6 +682,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     a.P.hit = cv.take<float4>(nslots);
     a.P.order = cv.take<int>(nslots);
     a.P.keys = cv.take<int>(nslots);
+    a.P.rrank = cv.take<int>(nslots);
     if (dielectrics) {
         a.P.ab = cv.take<float4>(nslots);
         a.P.ior = cv.take<float>((size_t)nslots * 8);
@@ -636,6 +692,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     a.S.c = cv.take<float4>(cap);
     a.S.count = cv.take<int>(1);
     a.S.capacity = (int)cap;
+    a.rhist = cv.take<int>(rt::kRayKeys);
+    a.roff = cv.take<int>(rt::kRayKeys);
     std::vector<float*> films(reqs.size());
     std::vector<int> fdims(2 * reqs.size());
     for (size_t r = 0; r < reqs.size(); r++) {
@@ -666,6 +724,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     CUDA_TRY(cudaMemcpyAsync(d_fdims, fdims.data(), fdims.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
     CUDA_TRY(cudaMemsetAsync(a.P.d, 0, (size_t)nslots * sizeof(float4), stream));
     CUDA_TRY(cudaMemsetAsync(a.S.count, 0, sizeof(int), stream));
+    CUDA_TRY(cudaMemsetAsync(a.rhist, 0, (size_t)rt::kRayKeys * sizeof(int), stream));
+    CUDA_TRY(cudaMemsetAsync(a.roff, 0, (size_t)rt::kRayKeys * sizeof(int), stream));
     for (auto& q : wreq) CUDA_TRY(cudaMemsetAsync(q.accum, 0, (size_t)3 * q.ww * q.wh * sizeof(float), stream));
     CUDA_TRY(cudaMemsetAsync(s0->d_err, 0, sizeof(int), stream));
     CUDA_TRY(cudaStreamSynchronize(stream));   // host vectors above go out of scope
@@ -675,6 +735,14 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     bool l4 = cfg.layout == 4;
     for (const HostReq& q : reqs) l4 = l4 && q.scene->host.max_stack4 <= kStack;
     bool pt = !l4 && cfg.fetch == 2;
+    int groups = cfg.groups > 0 ? cfg.groups : default_groups(scenes);
+    a.regroup = groups == 2;
+    a.raysort = groups == 3 && !pt;
+    // 8x8x8 origin cells x 8x8 direction bins: the measured best of the
+    // layouts that fit 15 bits (coarser cells or octant-only directions cost
+    // extend 4-13% on the icosphere field)
+    a.rkey_bits = 3;
+    a.rdir_bits = 6;
     unsigned gpt_e = 1, gpt_o = 1;
     if (pt) {
         int sms = 148, nb_e = 1, nb_o = 1;
@@ -704,6 +772,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         }
         if (ev) cudaEventRecord(ev[3], stream);
         rt::k_wf_shade<<<gs, blk, 0, stream>>>(a);
+        if (a.raysort) rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[4], stream);
         if (l4) rt::k_wf_occlude<kStack, true><<<gsh, tblk, 0, stream>>>(a);
         else if (pt && a.opaque) rt::k_wf_occlude_pt<kStack><<<gpt_o, tblk, 0, stream>>>(a);
@@ -729,7 +798,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
             return fail(RT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
         }
     }
-    int per_iter = 5 + (sort ? 2 : 0);
+    int per_iter = 5 + (sort ? 2 : 0) + (a.raysort ? 1 : 0);
     int max_depth = 1;
     for (auto& q : wreq) max_depth = std::max(max_depth, q.rc.max_depth);
     int64_t limit = (total / nslots + 2) * (int64_t)(max_depth + 2) + 64;
@@ -848,6 +917,7 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
         cfg.layout = sc->tuned_layout;
         cfg.fetch = sc->tuned_fetch;
         cfg.tblock = sc->tuned_tblock;
+        cfg.groups = sc->tuned_groups;
     }
     if (p->wavefront_size > 0) cfg.slots = p->wavefront_size;
     if (p->block_size > 0) cfg.block = p->block_size;
@@ -855,6 +925,7 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
     if (p->node_layout == 2 || p->node_layout == 4) cfg.layout = p->node_layout;
     if (p->ray_fetch == 1 || p->ray_fetch == 2) cfg.fetch = p->ray_fetch;
     if (p->trace_block_size > 0) cfg.tblock = p->trace_block_size;
+    if (p->ray_groups >= 1 && p->ray_groups <= 3) cfg.groups = p->ray_groups;
     cfg.profile = p->profile_kernels != 0;
     if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
         return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
@@ -942,6 +1013,7 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     v.sigma_s = h.sigma_s;
     v.sigma_t = h.sigma_t;
     v.hg_g = h.hg_g;
+    ray_sort_box(h, v);
     sc->opaque = 1;
     sc->dielectrics = 0;
     for (const rt::Material& m : h.materials) {
@@ -1231,6 +1303,7 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
             cfg.layout = s0->tuned_layout;
             cfg.fetch = s0->tuned_fetch;
             cfg.tblock = s0->tuned_tblock;
+            cfg.groups = s0->tuned_groups;
         }
         if (common->wavefront_size > 0) cfg.slots = common->wavefront_size;
         if (common->block_size > 0) cfg.block = common->block_size;
@@ -1238,6 +1311,8 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
         if (common->node_layout == 2 || common->node_layout == 4) cfg.layout = common->node_layout;
         if (common->ray_fetch == 1 || common->ray_fetch == 2) cfg.fetch = common->ray_fetch;
         if (common->trace_block_size > 0) cfg.tblock = common->trace_block_size;
+        if (common->ray_groups >= 1 && common->ray_groups <= 3) cfg.groups = common->ray_groups;
+        cfg.profile = common->profile_kernels != 0;
         rc = wf_render(hq, cfg, st);
     }
     for (int i = 0; i < n; i++) {
@@ -1287,6 +1362,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
                     p.node_layout = layouts[li];
                     p.ray_fetch = 1;
                     p.trace_block_size = blocks[bi];
+                    p.ray_groups = 1;
                     RtStats s1{};
                     rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
                     if (rc == RT_OK && s1.kernel_ms < best_ms) {
@@ -1298,6 +1374,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
                     }
                 }
     pick.tblock = pick.block;
+    pick.groups = 1;   // the passes above ran slot order
     // then, on the winner, the block of extend/occlude alone and the
     // persistent dynamic-fetch kernels
     for (int bi = 0; bi < 3 && rc == RT_OK; bi++) {
@@ -1312,11 +1389,31 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
         p.node_layout = pick.layout;
         p.ray_fetch = 1;
         p.trace_block_size = blocks[bi];
+        p.ray_groups = 1;
         RtStats s1{};
         rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
         if (rc == RT_OK && s1.kernel_ms < best_ms) {
             best_ms = s1.kernel_ms;
             pick.tblock = blocks[bi];
+        }
+    }
+    for (int g = 2; g <= 3 && rc == RT_OK; g++) {   // block-local regrouping, then the bounce-ray sort
+        RtRenderParams p = *params;
+        p.kernel = RT_KERNEL_WAVEFRONT;
+        p.spp = spp;
+        p.count_work = 0;
+        p.wavefront_size = pick.slots;
+        p.block_size = pick.block;
+        p.sort_materials = pick.sort;
+        p.node_layout = pick.layout;
+        p.ray_fetch = 1;
+        p.trace_block_size = pick.tblock;
+        p.ray_groups = g;
+        RtStats s1{};
+        rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
+        if (rc == RT_OK && s1.kernel_ms < best_ms) {
+            best_ms = s1.kernel_ms;
+            pick.groups = g;
         }
     }
     if (rc == RT_OK && pick.layout == 2) {
@@ -1330,6 +1427,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
         p.node_layout = 2;
         p.ray_fetch = 2;
         p.trace_block_size = pick.tblock;
+        p.ray_groups = pick.groups;
         RtStats s1{};
         rc = render_to_device(sc, &p, sc->host.camera, d_film, &s1);
         if (rc == RT_OK && s1.kernel_ms < best_ms) {
@@ -1346,6 +1444,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
     sc->tuned_layout = pick.layout;
     sc->tuned_fetch = pick.fetch;
     sc->tuned_tblock = pick.tblock;
+    sc->tuned_groups = pick.groups;
     if (best) {
         *best = *params;
         best->kernel = RT_KERNEL_WAVEFRONT;
@@ -1355,6 +1454,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
         best->node_layout = pick.layout;
         best->ray_fetch = pick.fetch;
         best->trace_block_size = pick.tblock;
+        best->ray_groups = pick.groups;
     }
     return RT_OK;
 }

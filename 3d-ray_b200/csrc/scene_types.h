@@ -152,6 +152,9 @@ struct SceneView {
     int has_medium;
     V3 sigma_a, sigma_s, sigma_t;
     float hg_g;
+    // Box of the wavefront's bounce-ray sort: origins map to cells of
+    // (o - sort_lo) * sort_scale in [0, 1) (clamped); sort_scale 0 on a flat axis.
+    V3 sort_lo, sort_scale;
 };
 
 }  // namespace rt

@@ -54,8 +54,9 @@ struct WfPaths {
     float4* ab;     // cur_abs.xyz, ior count   (dielectric scenes)
     float* ior;     // 8 per slot                (dielectric scenes)
     float4* hit;    // t, u, v, kind << 30 | slot
-    int* order;     // slot order for shade (material-sorted or identity)
-    int* keys;      // material key per slot (sorting)
+    int* order;     // slot order for shade (material-sorted or identity); for extend under the ray sort
+    int* keys;      // material key per slot (sorting); after shade, the ray sort's key
+    int* rrank;     // ray sort: the slot's rank among the rays of its key
 };
 
 struct WfShadow {
@@ -74,8 +75,14 @@ struct WfCtl {
     // (the host reads next, then live and overflow as one 8-byte copy: keep them adjacent)
     unsigned ext_next;          // persistent extend: next slot to fetch
     unsigned occ_next;          // persistent occlude: next shadow record to fetch
+    unsigned long long iter_first;   // ray sort: the first work id of this iteration
+    int nbounce;                // ray sort: bounce rays shade continued (order[0 .. nbounce))
+    int nbounce_pad;
     int hist[256];              // material histogram (sorting)
 };
+
+// Buckets of the bounce-ray sort.
+constexpr int kRayKeys = 1 << 15;
 
 struct WfArgs {
     const SceneView* views;
@@ -86,6 +93,12 @@ struct WfArgs {
     int sort;
     int nkeys;        // material keys (sum over scenes) for sorting
     const int* key_base;   // per scene: first key
+    int regroup;      // extend/occlude regroup their block's rays by kind (block_group)
+    int raysort;      // extend walks bounce rays sorted by ray_key, then camera rays in pixel order
+    int rkey_bits;    // ray_key: origin cell bits per axis (0 .. 4)
+    int rdir_bits;    // ray_key: direction bits (0, 3: octant, or an even count up to 8)
+    int* rhist;       // kRayKeys: bounce rays per key (filled by shade)
+    int* roff;        // kRayKeys: the keys' first positions in order (the scanned histogram)
     WfPaths P;
     WfShadow S;
     WfCtl* ctl;
@@ -227,6 +240,13 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
     }
     __syncthreads();
     bool live = alive;
+    if (alive && a.raysort) {
+        // a bounce ray shade continued: its key's first position plus the rank
+        // shade's count gave it
+        int pos = a.roff[a.P.keys[i]] + a.P.rrank[i];
+        if (pos < a.ctl->nbounce) a.P.order[pos] = i;
+        else atomicExch(a.err, RT_ERR_BOUNDS);
+    }
     if (need) {
         unsigned long long id = s_base + (unsigned long long)(s_warp[wid] + __popc(m & ((1u << lane) - 1u)));
         if (id >= a.ctl->total) {
@@ -245,12 +265,101 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
             wf_store(a, i, ps, wf_flags(ps, al), req, lx | (ly << 16));
             wf_store_media(a, i, R, ps);
             live = true;
+            if (a.raysort) {   // camera rays after the bounce rays, in work-id (pixel) order
+                long long pos = (long long)a.ctl->nbounce + (long long)(id - a.ctl->iter_first);
+                if (pos < a.nslots) a.P.order[pos] = al ? i : -1;
+                else atomicExch(a.err, RT_ERR_BOUNDS);
+            }
         }
     }
     int wl = __popc(__ballot_sync(full, live));
     if (lane == 0 && wl) atomicAdd(&s_live, wl);
     __syncthreads();
     if (threadIdx.x == 0 && s_live) atomicAdd(&a.ctl->live, s_live);
+}
+
+// Block-local counting partition; blockDim.x is a multiple of 32, at most 256,
+// and every thread of the block calls it. Each thread offers one item of class
+// cls (cls < 0: none). On return s_idx[0 .. n) holds the block's items ordered
+// by class, in thread order within a class, and n is returned.
+template <int NC>
+RT_D int block_group(int item, int cls, int* s_idx, int (*s_cnt)[8], int* s_tot) {
+    static_assert(NC <= 32, "one class per lane of the scanning warp");
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned mine = 0;
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+        unsigned m = __ballot_sync(full, cls == c);
+        if (cls == c) mine = m;
+        if (lane == 0) s_cnt[c][wid] = __popc(m);
+    }
+    __syncthreads();
+    if (wid == 0) {
+        // lane c: the class's count, an exclusive scan over the classes, then
+        // the running offsets of its warps (class-major order)
+        int sum = 0;
+        if (lane < NC)
+            for (int w = 0; w < nw; w++) sum += s_cnt[lane][w];
+        int incl = sum;
+        for (int off = 1; off < 32; off <<= 1) {
+            int v = __shfl_up_sync(full, incl, off);
+            if (lane >= off) incl += v;
+        }
+        int run = incl - sum;
+        if (lane < NC)
+            for (int w = 0; w < nw; w++) {
+                int c = s_cnt[lane][w];
+                s_cnt[lane][w] = run;
+                run += c;
+            }
+        if (lane == 31) *s_tot = incl;   // lanes past NC add nothing: lane 31 holds the total
+    }
+    __syncthreads();
+    if (cls >= 0) s_idx[s_cnt[cls][wid] + __popc(mine & ((1u << lane) - 1u))] = item;
+    __syncthreads();
+    return *s_tot;
+}
+
+RT_D int octant(float x, float y, float z) { return (x < 0.0f) | ((y < 0.0f) << 1) | ((z < 0.0f) << 2); }
+
+// Spreads the low 4 bits of v to bits 0, 3, 6, 9 (a Morton code's axis).
+RT_D unsigned spread3(unsigned v) { return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6); }
+
+// Sort key of a bounce ray (0 .. kRayKeys): the origin's cell in the scene's
+// sort box, cb bits per axis in Morton order, above a direction bin of db
+// bits: none, the octant for 3, else a square grid over the octahedral map of
+// the direction. Rays that share a key start close together in similar
+// directions, so they walk much the same BVH nodes.
+RT_D int ray_key(const SceneView& s, V3 o, V3 d, int cb, int db) {
+    unsigned cell = 0;
+    if (cb > 0) {
+        float n = (float)(1 << cb);
+        V3 u = (o - s.sort_lo) * s.sort_scale;
+        unsigned cx = (unsigned)fminf(fmaxf(u.x * n, 0.0f), n - 1.0f);
+        unsigned cy = (unsigned)fminf(fmaxf(u.y * n, 0.0f), n - 1.0f);
+        unsigned cz = (unsigned)fminf(fmaxf(u.z * n, 0.0f), n - 1.0f);
+        cell = spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
+    }
+    unsigned dir = 0;
+    if (db == 3) {
+        dir = (unsigned)octant(d.x, d.y, d.z);
+    } else if (db > 0) {
+        // octahedral map of the direction onto [-1, 1]^2
+        float l1 = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+        float px = l1 > 0.0f ? d.x / l1 : 0.0f, py = l1 > 0.0f ? d.y / l1 : 0.0f;
+        if (d.z < 0.0f) {
+            float qx = (1.0f - fabsf(py)) * (px < 0.0f ? -1.0f : 1.0f);
+            float qy = (1.0f - fabsf(px)) * (py < 0.0f ? -1.0f : 1.0f);
+            px = qx;
+            py = qy;
+        }
+        float g = (float)(1 << (db / 2));
+        unsigned gx = (unsigned)fminf(fmaxf((px * 0.5f + 0.5f) * g, 0.0f), g - 1.0f);
+        unsigned gy = (unsigned)fminf(fmaxf((py * 0.5f + 0.5f) * g, 0.0f), g - 1.0f);
+        dir = gx | (gy << (db / 2));
+    }
+    return (int)((cell << db) | dir) & (kRayKeys - 1);
 }
 
 // Stores slot i's closest hit and, when sorting, its material key.
@@ -271,10 +380,36 @@ RT_D void extend_store(const WfArgs& a, int i, int req, const SceneView& s, cons
 }
 
 // One thread per slot.
+// One thread per slot. With regroup, the block first reorders its live slots:
+// camera rays, then bounce rays by direction octant. Regen hands a block's free
+// slots consecutive pixels, so its camera rays are coherent, but they sit
+// between the bounce rays of paths still in flight; regrouped, a warp holds
+// one kind of ray and no longer waits on its slowest bounce ray.
 template <int STACK, bool L4>
 __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nslots) return;
+    if (a.raysort) {
+        // order[0 .. nbounce): bounce rays by key; then this iteration's camera rays
+        unsigned long long nx = a.ctl->next < a.ctl->total ? a.ctl->next : a.ctl->total;
+        long long ncam = (long long)nx - (long long)a.ctl->iter_first;
+        long long n = (long long)a.ctl->nbounce + (ncam > 0 ? ncam : 0);
+        if ((long long)i >= n || i >= a.nslots) return;
+        i = a.P.order[i];
+        if (i < 0) return;
+    } else if (a.regroup) {
+        __shared__ int s_idx[256], s_cnt[9][8], s_tot;
+        int cls = -1;
+        if (i < a.nslots) {
+            float4 d = a.P.d[i];
+            int fl = fbits(d.w);
+            if (fl & PF_ALIVE) cls = (fl & PF_FIRST) ? 0 : 1 + octant(d.x, d.y, d.z);
+        }
+        int n = block_group<9>(i, cls, s_idx, s_cnt, &s_tot);
+        if ((int)threadIdx.x >= n) return;
+        i = s_idx[threadIdx.x];
+    } else if (i >= a.nslots) {
+        return;
+    }
     float4 d = a.P.d[i];
     if (!(fbits(d.w) & PF_ALIVE)) return;
     float4 o = a.P.o[i];
@@ -429,6 +564,62 @@ __global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a)
     bool alive = shade_vertex(s, R.rc, ps, h, sink);
     wf_store(a, i, ps, wf_flags(ps, alive), req, pix);
     wf_store_media(a, i, R, ps);
+    if (a.raysort && alive) {   // the continued ray's sort key and its rank in the key's count
+        int key = ray_key(s, ps.o, ps.d, a.rkey_bits, a.rdir_bits);
+        unsigned grp = __match_any_sync(__activemask(), key);
+        int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&a.rhist[key], __popc(grp));
+        base = __shfl_sync(grp, base, leader);
+        a.P.keys[i] = key;
+        a.P.rrank[i] = base + __popc(grp & ((1u << lane) - 1u));
+    }
+}
+
+// Exclusive scan of the bounce-ray key histogram into roff (one block of
+// 1024 threads, a run of kRayKeys / 1024 keys each), clearing the histogram
+// for the next shade; nbounce is the total.
+__global__ void __launch_bounds__(1024) k_wf_rscan(WfArgs a) {
+    constexpr int kPer = kRayKeys / 1024;
+    static_assert(kPer % 4 == 0, "whole int4 runs per thread");
+    __shared__ int s_w[32];
+    const unsigned full = 0xffffffffu;
+    int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    int4* h4 = reinterpret_cast<int4*>(a.rhist) + t * (kPer / 4);
+    int4* o4 = reinterpret_cast<int4*>(a.roff) + t * (kPer / 4);
+    int sum = 0;
+    for (int k = 0; k < kPer / 4; k++) {
+        int4 v = h4[k];
+        sum += v.x + v.y + v.z + v.w;
+    }
+    int incl = sum;
+    for (int off = 1; off < 32; off <<= 1) {
+        int x = __shfl_up_sync(full, incl, off);
+        if (lane >= off) incl += x;
+    }
+    if (lane == 31) s_w[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int x = s_w[lane];
+        for (int off = 1; off < 32; off <<= 1) {
+            int y = __shfl_up_sync(full, x, off);
+            if (lane >= off) x += y;
+        }
+        s_w[lane] = x;
+    }
+    __syncthreads();
+    int base = (w ? s_w[w - 1] : 0) + incl - sum;
+    for (int k = 0; k < kPer / 4; k++) {
+        int4 v = h4[k], r;
+        r.x = base;
+        r.y = r.x + v.x;
+        r.z = r.y + v.y;
+        r.w = r.z + v.z;
+        base = r.w + v.w;
+        o4[k] = r;
+        h4[k] = make_int4(0, 0, 0, 0);
+    }
+    if (t == 1023) a.ctl->nbounce = base;
 }
 
 // Persistent any-hit for opaque batches (the walk is one any-hit traversal):
@@ -485,7 +676,21 @@ template <int STACK, bool L4>
 __global__ void __launch_bounds__(256) k_wf_occlude(WfArgs a) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     int n = min(*a.S.count, a.S.capacity);
-    if (j >= n) return;
+    if (a.regroup) {
+        // shadow rays by direction octant (blocks wholly past the queue leave at once)
+        if ((int)(blockIdx.x * blockDim.x) >= n) return;
+        __shared__ int s_idx[256], s_cnt[8][8], s_tot;
+        int cls = -1;
+        if (j < n) {
+            float4 d = a.S.d[j];
+            cls = octant(d.x, d.y, d.z);
+        }
+        int m = block_group<8>(j, cls, s_idx, s_cnt, &s_tot);
+        if ((int)threadIdx.x >= m) return;
+        j = s_idx[threadIdx.x];
+    } else if (j >= n) {
+        return;
+    }
     float4 o = a.S.o[j], d = a.S.d[j], c = a.S.c[j];
     const SceneView& s = a.views[fbits(c.w)];
     V3 tr = shadow_transmittance<STACK, L4>(s, a.opaque, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, o.w, nullptr,
@@ -509,6 +714,7 @@ __global__ void k_wf_reset(WfArgs a) {
         a.ctl->live = 0;
         a.ctl->ext_next = 0;
         a.ctl->occ_next = 0;
+        a.ctl->iter_first = a.ctl->next;
     }
     if (a.sort)
         for (int k = t; k <= a.nkeys; k += blockDim.x) a.ctl->hist[k] = 0;

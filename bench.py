@@ -280,12 +280,13 @@ def profile_frame(args):
     p = abi.render_params(W, H, args.spp, DEPTH, kernel=kern, wavefront_size=1 << 22, block_size=256,
                           trace_block_size=args.block,
                           sort_materials=1, node_layout=args.node_layout, ray_fetch=args.ray_fetch,
-                          profile_kernels=int(args.split))
+                          ray_groups=args.ray_groups, profile_kernels=int(args.split))
     film = np.zeros((3, H, W), np.float32)
     st = abi.RtStats()
     for i in range(2):
         abi.check(lib.rt_render(scene, C.byref(p), film.ctypes.data_as(C.c_void_p), C.byref(st)), "rt_render")
         line = {"frame": i, "kernel": args.kernel, "node_layout": args.node_layout, "ray_fetch": args.ray_fetch,
+                "ray_groups": args.ray_groups,
                 "spp": args.spp,
                 "kernel_ms": st.kernel_ms, "Msamples_per_s": W * H * args.spp / st.kernel_ms / 1e3,
                 "iterations": st.iterations, "launches": st.kernel_launches}
@@ -529,6 +530,8 @@ def main():
                     help="--profile-frame: block size of extend/occlude (the others use 256)")
     ap.add_argument("--ray-fetch", type=int, default=1, choices=[1, 2],
                     help="--profile-frame: one ray per thread (1) or persistent dynamic fetch (2)")
+    ap.add_argument("--ray-groups", type=int, default=1, choices=[1, 2, 3],
+                    help="--profile-frame: rays in slot order (1), regrouped by kind in each block (2), bounce rays sorted by origin and direction (3)")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
     ap.add_argument("--res", type=int, default=256, help="--fit: square image size")
     ap.add_argument("--gradcheck", action="store_true",
@@ -564,7 +567,8 @@ def main():
         abi.check(lib.rt_autotune(scene, C.byref(params), C.byref(best)), "rt_autotune")
         tuned = {"wavefront_size": best.wavefront_size, "block_size": best.block_size,
                  "sort_materials": best.sort_materials, "node_layout": best.node_layout,
-                 "ray_fetch": best.ray_fetch, "trace_block_size": best.trace_block_size}
+                 "ray_fetch": best.ray_fetch, "trace_block_size": best.trace_block_size,
+                 "ray_groups": best.ray_groups}
     film = torch.empty((3, H, W), dtype=torch.float32, device="cuda")
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 

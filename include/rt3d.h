@@ -188,7 +188,12 @@ typedef struct RtRenderParams {
                                        global counter, 0 the autotuned choice (else 1) */
     int32_t trace_block_size;       /* block of the wavefront's extend/occlude: 64, 128 or 256;
                                        0 the autotuned choice (else block_size) */
-    int32_t reserved;
+    int32_t ray_groups;             /* wavefront extend/occlude on one ray per thread: 1 rays in slot
+                                       order, 2 each block regroups its rays by kind (camera rays,
+                                       then bounce and shadow rays by direction octant), 3 extend
+                                       walks the bounce rays sorted by origin cell and direction,
+                                       then the camera rays in pixel order; 0 the autotuned choice
+                                       (else 3, or 1 when a scene has a participating medium) */
 } RtRenderParams;
 
 /* Counters and timings of one call. */
@@ -301,10 +306,11 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
 
 /* Autotuner: times the wavefront over wavefront size {256K, 1M, 4M} x block
  * {64, 128, 256} x material sort {off, on} x node layout {two-wide,
- * four-wide}, then, on the winner, the extend/occlude block {64, 128, 256}
- * and the persistent dynamic-fetch kernels, on a bounded slice of `params`
- * (the full window at the spp giving ~16 M samples), keeps the fastest for
- * this scene (used when those params fields are 0 / -1) and returns it. */
+ * four-wide}, then, on the winner, the extend/occlude block {64, 128, 256},
+ * the ray regrouping {block-local, sorted bounce rays} and the persistent
+ * dynamic-fetch kernels, on a bounded slice of `params` (the full window at
+ * the spp giving ~16 M samples), keeps the fastest for this scene (used when
+ * those params fields are 0 / -1) and returns it. */
 int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* best);
 
 /* ---- differentiation ----------------------------------------------------- */
