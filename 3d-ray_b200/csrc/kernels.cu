@@ -555,18 +555,19 @@ struct WfConfig {
     int layout = 2;    // BVH records of extend/occlude: 2 or 4 wide
     int fetch = 1;     // 1 one ray per thread, 2 persistent warps with dynamic fetch (two-wide only)
     int tblock = 0;    // block of extend/occlude (0: block)
-    int groups = 0;    // 1 slot order, 2 block-local regrouping, 3 sorted bounce rays; 0 default_groups
+    int groups = 0;    // 1 slot order, 2 block-local regrouping, 3 sorted bounce rays, 4 and shadow rays; 0 default_groups
 };
 
-// Untuned ray order: the bounce-ray sort, except with a participating medium.
-// There nearly every slot is a bounce ray scattered in mid-air and the scene
-// is small, so the sort's key and rank in shade cost more than the coherence
-// wins back (measured: icosphere field +12%, Cornell box +12%, mixed batch
-// +10%, the medium scene -3%).
+// Untuned ray order: bounce and shadow rays sorted, except with a
+// participating medium. There nearly every slot is a bounce ray scattered in
+// mid-air and the scene is small, so the sorts' keys and ranks in shade cost
+// more than the coherence wins back (measured, bounce rays sorted: icosphere
+// field +12%, Cornell box +12%, mixed batch +10%, the medium scene -3%; shadow
+// rays sorted as well: a further +3%, +1% and -3%).
 int default_groups(const std::vector<RtScene*>& scenes) {
     for (const RtScene* sc : scenes)
         if (sc->host.has_medium) return 1;
-    return 3;
+    return 4;
 }
 
 int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st) {
@@ -646,8 +647,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     }
     for (int k = 0; k < 3; k++) add((size_t)cap * sizeof(float4));
     add(sizeof(int));
-    add((size_t)rt::kRayKeys * sizeof(int));
-    add((size_t)rt::kRayKeys * sizeof(int));
+    for (int k = 0; k < 3; k++) add((size_t)cap * sizeof(int));
+    for (int k = 0; k < 4; k++) add((size_t)rt::kRayKeys * sizeof(int));
     for (auto& q : wreq) add((size_t)3 * q.ww * q.wh * sizeof(float));
     add(reqs.size() * sizeof(float*));
     add(reqs.size() * sizeof(int) * 2);
@@ -692,8 +693,13 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     a.S.c = cv.take<float4>(cap);
     a.S.count = cv.take<int>(1);
     a.S.capacity = (int)cap;
+    a.S.key = cv.take<int>(cap);
+    a.S.rank = cv.take<int>(cap);
+    a.S.order = cv.take<int>(cap);
     a.rhist = cv.take<int>(rt::kRayKeys);
     a.roff = cv.take<int>(rt::kRayKeys);
+    a.shist = cv.take<int>(rt::kRayKeys);
+    a.soff = cv.take<int>(rt::kRayKeys);
     std::vector<float*> films(reqs.size());
     std::vector<int> fdims(2 * reqs.size());
     for (size_t r = 0; r < reqs.size(); r++) {
@@ -724,8 +730,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     CUDA_TRY(cudaMemcpyAsync(d_fdims, fdims.data(), fdims.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
     CUDA_TRY(cudaMemsetAsync(a.P.d, 0, (size_t)nslots * sizeof(float4), stream));
     CUDA_TRY(cudaMemsetAsync(a.S.count, 0, sizeof(int), stream));
-    CUDA_TRY(cudaMemsetAsync(a.rhist, 0, (size_t)rt::kRayKeys * sizeof(int), stream));
-    CUDA_TRY(cudaMemsetAsync(a.roff, 0, (size_t)rt::kRayKeys * sizeof(int), stream));
+    for (int* h : {a.rhist, a.roff, a.shist, a.soff})
+        CUDA_TRY(cudaMemsetAsync(h, 0, (size_t)rt::kRayKeys * sizeof(int), stream));
     for (auto& q : wreq) CUDA_TRY(cudaMemsetAsync(q.accum, 0, (size_t)3 * q.ww * q.wh * sizeof(float), stream));
     CUDA_TRY(cudaMemsetAsync(s0->d_err, 0, sizeof(int), stream));
     CUDA_TRY(cudaStreamSynchronize(stream));   // host vectors above go out of scope
@@ -737,7 +743,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     bool pt = !l4 && cfg.fetch == 2;
     int groups = cfg.groups > 0 ? cfg.groups : default_groups(scenes);
     a.regroup = groups == 2;
-    a.raysort = groups == 3 && !pt;
+    a.raysort = groups >= 3 && !pt;
+    a.shadowsort = groups == 4 && !pt;
     // 8x8x8 origin cells x 8x8 direction bins: the measured best of the
     // layouts that fit 15 bits (coarser cells or octant-only directions cost
     // extend 4-13% on the icosphere field)
@@ -756,6 +763,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     unsigned gst = (unsigned)((nslots + tblk - 1) / tblk);
     unsigned gsh = (unsigned)((cap + tblk - 1) / tblk);
     unsigned g256 = (unsigned)((nslots + 255) / 256);
+    unsigned gsh256 = (unsigned)((cap + 255) / 256);
     // ev (profiling only): boundaries between the kernel groups of one iteration.
     auto launch_iter = [&](cudaEvent_t* ev) {
         if (ev) cudaEventRecord(ev[0], stream);
@@ -772,7 +780,11 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         }
         if (ev) cudaEventRecord(ev[3], stream);
         rt::k_wf_shade<<<gs, blk, 0, stream>>>(a);
-        if (a.raysort) rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a);
+        if (a.raysort) rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.rhist, a.roff, &d_ctl->nbounce);
+        if (a.shadowsort) {
+            rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.shist, a.soff, &d_ctl->nshadow);
+            rt::k_wf_sscatter<<<gsh256, 256, 0, stream>>>(a);
+        }
         if (ev) cudaEventRecord(ev[4], stream);
         if (l4) rt::k_wf_occlude<kStack, true><<<gsh, tblk, 0, stream>>>(a);
         else if (pt && a.opaque) rt::k_wf_occlude_pt<kStack><<<gpt_o, tblk, 0, stream>>>(a);
@@ -798,7 +810,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
             return fail(RT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
         }
     }
-    int per_iter = 5 + (sort ? 2 : 0) + (a.raysort ? 1 : 0);
+    int per_iter = 5 + (sort ? 2 : 0) + (a.raysort ? 1 : 0) + (a.shadowsort ? 2 : 0);
     int max_depth = 1;
     for (auto& q : wreq) max_depth = std::max(max_depth, q.rc.max_depth);
     int64_t limit = (total / nslots + 2) * (int64_t)(max_depth + 2) + 64;
@@ -925,7 +937,7 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
     if (p->node_layout == 2 || p->node_layout == 4) cfg.layout = p->node_layout;
     if (p->ray_fetch == 1 || p->ray_fetch == 2) cfg.fetch = p->ray_fetch;
     if (p->trace_block_size > 0) cfg.tblock = p->trace_block_size;
-    if (p->ray_groups >= 1 && p->ray_groups <= 3) cfg.groups = p->ray_groups;
+    if (p->ray_groups >= 1 && p->ray_groups <= 4) cfg.groups = p->ray_groups;
     cfg.profile = p->profile_kernels != 0;
     if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
         return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
@@ -1311,7 +1323,7 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
         if (common->node_layout == 2 || common->node_layout == 4) cfg.layout = common->node_layout;
         if (common->ray_fetch == 1 || common->ray_fetch == 2) cfg.fetch = common->ray_fetch;
         if (common->trace_block_size > 0) cfg.tblock = common->trace_block_size;
-        if (common->ray_groups >= 1 && common->ray_groups <= 3) cfg.groups = common->ray_groups;
+        if (common->ray_groups >= 1 && common->ray_groups <= 4) cfg.groups = common->ray_groups;
         cfg.profile = common->profile_kernels != 0;
         rc = wf_render(hq, cfg, st);
     }
@@ -1397,7 +1409,7 @@ int rt_autotune(RtScene* sc, const RtRenderParams* params, RtRenderParams* best)
             pick.tblock = blocks[bi];
         }
     }
-    for (int g = 2; g <= 3 && rc == RT_OK; g++) {   // block-local regrouping, then the bounce-ray sort
+    for (int g = 2; g <= 4 && rc == RT_OK; g++) {   // block-local regrouping, then the ray sorts
         RtRenderParams p = *params;
         p.kernel = RT_KERNEL_WAVEFRONT;
         p.spp = spp;

@@ -65,6 +65,9 @@ struct WfShadow {
     float4* c;    // contribution.xyz, scene
     int* count;
     int capacity;
+    int* key;     // shadow sort: the record's ray_key
+    int* rank;    // shadow sort: its rank among the records of its key
+    int* order;   // shadow sort: records in key order, for occlude
 };
 
 struct WfCtl {
@@ -77,7 +80,7 @@ struct WfCtl {
     unsigned occ_next;          // persistent occlude: next shadow record to fetch
     unsigned long long iter_first;   // ray sort: the first work id of this iteration
     int nbounce;                // ray sort: bounce rays shade continued (order[0 .. nbounce))
-    int nbounce_pad;
+    int nshadow;                // shadow sort: records counted by key (the queue's count)
     int hist[256];              // material histogram (sorting)
 };
 
@@ -99,6 +102,9 @@ struct WfArgs {
     int rdir_bits;    // ray_key: direction bits (0, 3: octant, or an even count up to 8)
     int* rhist;       // kRayKeys: bounce rays per key (filled by shade)
     int* roff;        // kRayKeys: the keys' first positions in order (the scanned histogram)
+    int shadowsort;   // occlude walks the shadow records sorted by ray_key
+    int* shist;       // kRayKeys: shadow records per key (filled by shade)
+    int* soff;        // kRayKeys: the keys' first positions in S.order
     WfPaths P;
     WfShadow S;
     WfCtl* ctl;
@@ -524,6 +530,16 @@ struct QueueShadows : NoAdjoint {
         a->S.o[j] = make_float4(o.x, o.y, o.z, tmax);
         a->S.d[j] = make_float4(d.x, d.y, d.z, ibits((slot << 1) | to_la));
         a->S.c[j] = make_float4(c.x, c.y, c.z, ibits(scene));
+        if (a->shadowsort) {   // the record's sort key and its rank in the key's count
+            int key = ray_key(a->views[scene], o, d, a->rkey_bits, a->rdir_bits);
+            unsigned grp = __match_any_sync(__activemask(), key);
+            int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&a->shist[key], __popc(grp));
+            base = __shfl_sync(grp, base, leader);
+            a->S.key[j] = key;
+            a->S.rank[j] = base + __popc(grp & ((1u << lane) - 1u));
+        }
     }
     RT_D void skipped(V3, V3, float) {}
 };
@@ -576,50 +592,63 @@ __global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a)
     }
 }
 
-// Exclusive scan of the bounce-ray key histogram into roff (one block of
-// 1024 threads, a run of kRayKeys / 1024 keys each), clearing the histogram
-// for the next shade; nbounce is the total.
-__global__ void __launch_bounds__(1024) k_wf_rscan(WfArgs a) {
+// Exclusive scan of a ray-sort key histogram (kRayKeys counts) into off (one
+// block of 1024 threads, a run of kRayKeys / 1024 keys each), clearing the
+// histogram for the next shade; *total receives the sum.
+__global__ void __launch_bounds__(1024) k_wf_rscan(int* hist, int* off, int* total) {
     constexpr int kPer = kRayKeys / 1024;
     static_assert(kPer % 4 == 0, "whole int4 runs per thread");
     __shared__ int s_w[32];
     const unsigned full = 0xffffffffu;
     int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    int4* h4 = reinterpret_cast<int4*>(a.rhist) + t * (kPer / 4);
-    int4* o4 = reinterpret_cast<int4*>(a.roff) + t * (kPer / 4);
+    int4* h4 = reinterpret_cast<int4*>(hist) + t * (kPer / 4);
+    int4* o4 = reinterpret_cast<int4*>(off) + t * (kPer / 4);
+    int4 v[kPer / 4];
     int sum = 0;
+#pragma unroll
     for (int k = 0; k < kPer / 4; k++) {
-        int4 v = h4[k];
-        sum += v.x + v.y + v.z + v.w;
+        v[k] = h4[k];
+        sum += v[k].x + v[k].y + v[k].z + v[k].w;
     }
     int incl = sum;
-    for (int off = 1; off < 32; off <<= 1) {
-        int x = __shfl_up_sync(full, incl, off);
-        if (lane >= off) incl += x;
+    for (int o = 1; o < 32; o <<= 1) {
+        int x = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += x;
     }
     if (lane == 31) s_w[w] = incl;
     __syncthreads();
     if (w == 0) {
         int x = s_w[lane];
-        for (int off = 1; off < 32; off <<= 1) {
-            int y = __shfl_up_sync(full, x, off);
-            if (lane >= off) x += y;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(full, x, o);
+            if (lane >= o) x += y;
         }
         s_w[lane] = x;
     }
     __syncthreads();
     int base = (w ? s_w[w - 1] : 0) + incl - sum;
+#pragma unroll
     for (int k = 0; k < kPer / 4; k++) {
-        int4 v = h4[k], r;
+        int4 r;
         r.x = base;
-        r.y = r.x + v.x;
-        r.z = r.y + v.y;
-        r.w = r.z + v.z;
-        base = r.w + v.w;
+        r.y = r.x + v[k].x;
+        r.z = r.y + v[k].y;
+        r.w = r.z + v[k].z;
+        base = r.w + v[k].w;
         o4[k] = r;
         h4[k] = make_int4(0, 0, 0, 0);
     }
-    if (t == 1023) a.ctl->nbounce = base;
+    if (t == 1023) *total = base;
+}
+
+// Shadow sort: each queued record goes to its key's offset plus its rank.
+__global__ void k_wf_sscatter(WfArgs a) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = min(*a.S.count, a.S.capacity);
+    if (j >= n) return;
+    int pos = a.soff[a.S.key[j]] + a.S.rank[j];
+    if (pos < n) a.S.order[pos] = j;
+    else atomicExch(a.err, RT_ERR_BOUNDS);
 }
 
 // Persistent any-hit for opaque batches (the walk is one any-hit traversal):
@@ -676,7 +705,10 @@ template <int STACK, bool L4>
 __global__ void __launch_bounds__(256) k_wf_occlude(WfArgs a) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     int n = min(*a.S.count, a.S.capacity);
-    if (a.regroup) {
+    if (a.shadowsort) {
+        if (j >= n) return;
+        j = a.S.order[j];
+    } else if (a.regroup) {
         // shadow rays by direction octant (blocks wholly past the queue leave at once)
         if ((int)(blockIdx.x * blockDim.x) >= n) return;
         __shared__ int s_idx[256], s_cnt[8][8], s_tot;

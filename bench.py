@@ -530,8 +530,8 @@ def main():
                     help="--profile-frame: block size of extend/occlude (the others use 256)")
     ap.add_argument("--ray-fetch", type=int, default=1, choices=[1, 2],
                     help="--profile-frame: one ray per thread (1) or persistent dynamic fetch (2)")
-    ap.add_argument("--ray-groups", type=int, default=1, choices=[1, 2, 3],
-                    help="--profile-frame: rays in slot order (1), regrouped by kind in each block (2), bounce rays sorted by origin and direction (3)")
+    ap.add_argument("--ray-groups", type=int, default=1, choices=[1, 2, 3, 4],
+                    help="--profile-frame: rays in slot order (1), regrouped by kind in each block (2), bounce rays sorted by origin and direction (3), bounce and shadow rays sorted (4)")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
     ap.add_argument("--res", type=int, default=256, help="--fit: square image size")
     ap.add_argument("--gradcheck", action="store_true",

@@ -192,8 +192,9 @@ typedef struct RtRenderParams {
                                        order, 2 each block regroups its rays by kind (camera rays,
                                        then bounce and shadow rays by direction octant), 3 extend
                                        walks the bounce rays sorted by origin cell and direction,
-                                       then the camera rays in pixel order; 0 the autotuned choice
-                                       (else 3, or 1 when a scene has a participating medium) */
+                                       then the camera rays in pixel order, 4 as 3 and occlude walks
+                                       the shadow rays sorted the same way; 0 the autotuned choice
+                                       (else 4, or 1 when a scene has a participating medium) */
 } RtRenderParams;
 
 /* Counters and timings of one call. */
@@ -307,10 +308,11 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
 /* Autotuner: times the wavefront over wavefront size {256K, 1M, 4M} x block
  * {64, 128, 256} x material sort {off, on} x node layout {two-wide,
  * four-wide}, then, on the winner, the extend/occlude block {64, 128, 256},
- * the ray regrouping {block-local, sorted bounce rays} and the persistent
- * dynamic-fetch kernels, on a bounded slice of `params` (the full window at
- * the spp giving ~16 M samples), keeps the fastest for this scene (used when
- * those params fields are 0 / -1) and returns it. */
+ * the ray order {block-local regrouping, sorted bounce rays, sorted bounce
+ * and shadow rays} and the persistent dynamic-fetch kernels, on a bounded
+ * slice of `params` (the full window at the spp giving ~16 M samples), keeps
+ * the fastest for this scene (used when those params fields are 0 / -1) and
+ * returns it. */
 int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* best);
 
 /* ---- differentiation ----------------------------------------------------- */

@@ -455,10 +455,11 @@ def test_persistent_fetch_renders_like_one_ray_per_thread(throughput_world_small
 
 def test_regrouped_rays_render_like_slot_order(throughput_world_small, volume_world):
     """Extend/occlude blocks that regroup their rays by kind (camera rays, then
-    bounce and shadow rays by direction octant), and an extend that walks the
+    bounce and shadow rays by direction octant), an extend that walks the
     bounce rays sorted by origin cell and direction then the camera rays in
-    pixel order, trace the same rays as slot order, at every trace block size
-    and on both layouts: same images up to the order of the float additions."""
+    pixel order, and an occlude that walks the shadow records sorted the same
+    way, trace the same rays as slot order, at every trace block size and on
+    both layouts: same images up to the order of the float additions."""
     for world in (throughput_world_small, volume_world):
         s = Scene(world)
         try:
@@ -468,7 +469,7 @@ def test_regrouped_rays_render_like_slot_order(throughput_world_small, volume_wo
                 assert st.samples == 64 * 48 * 64
                 return img
             base = render(node_layout=2, ray_groups=1)
-            for g in (2, 3):
+            for g in (2, 3, 4):
                 for tb in (64, 128, 256):
                     np.testing.assert_allclose(render(node_layout=2, ray_groups=g, trace_block_size=tb), base,
                                                rtol=1e-4, atol=1e-6)
