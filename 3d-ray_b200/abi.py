@@ -75,7 +75,8 @@ class RtWorldDesc(C.Structure):
                 ("entities", C.POINTER(RtEntityDesc)), ("num_entities", C.c_int32),
                 ("tri_verts", C.POINTER(C.c_float)), ("num_tris", C.c_int64),
                 ("lights", C.POINTER(RtLightDesc)), ("num_lights", C.c_int32),
-                ("geometry_light_samples", C.c_int32), ("camera", RtCameraDesc), ("medium", RtMediumDesc)]
+                ("geometry_light_samples", C.c_int32), ("camera", RtCameraDesc), ("medium", RtMediumDesc),
+                ("tri_normals", C.POINTER(C.c_float)), ("tri_uvs", C.POINTER(C.c_float))]
 
 
 class RtRenderParams(C.Structure):
@@ -204,9 +205,17 @@ class PackedWorld:
             med.sigma_a = _f3(world.medium["sigma_a"])
             med.sigma_s = _f3(world.medium["sigma_s"])
             med.g = float(world.medium["g"])
+        fp = C.POINTER(C.c_float)
+        self.normals = self.uvs = None
+        if getattr(world, "tri_normals", None) is not None:
+            self.normals = np.ascontiguousarray(world.tri_normals, np.float32).reshape(-1)
+            self.uvs = np.ascontiguousarray(world.tri_uvs, np.float32).reshape(-1)
+            assert self.normals.size == 9 * world.num_tris and self.uvs.size == 6 * world.num_tris
         self.desc = RtWorldDesc(self.mats, nm, self.ents, ne,
-                                self.tris.ctypes.data_as(C.POINTER(C.c_float)), world.num_tris,
-                                self.lights, nl, int(world.geometry_light_samples), camera_desc(world.camera), med)
+                                self.tris.ctypes.data_as(fp), world.num_tris,
+                                self.lights, nl, int(world.geometry_light_samples), camera_desc(world.camera), med,
+                                self.normals.ctypes.data_as(fp) if self.normals is not None else fp(),
+                                self.uvs.ctypes.data_as(fp) if self.uvs is not None else fp())
 
     def ref(self):
         return C.byref(self.desc)

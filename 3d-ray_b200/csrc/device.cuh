@@ -174,13 +174,28 @@ RT_D bool entity_test(const SceneView& s, int e, V3 o, V3 d, float tmin, float t
     return true;
 }
 
+// Three-input min / max (PTX min.f32 and max.f32 with three sources, sm_100):
+// one instruction for what fminf(a, fminf(b, c)) computes in two. Neither
+// rounds, and both skip a NaN source as fminf / fmaxf do, so the value is the
+// same.
+RT_D float fmin3(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+RT_D float fmax3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 // Slab test of one child box; te receives max(tmin, entry distance).
 RT_D bool box_hit_te(float lx, float ly, float lz, float hx, float hy, float hz, V3 o, V3 inv, float tmin,
                      float tmax, float& te) {   // Core/AABB.cs:28-52
     float t0x = (lx - o.x) * inv.x, t0y = (ly - o.y) * inv.y, t0z = (lz - o.z) * inv.z;
     float t1x = (hx - o.x) * inv.x, t1y = (hy - o.y) * inv.y, t1z = (hz - o.z) * inv.z;
-    te = fmaxf(tmin, fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))));
-    float tx = fminf(tmax, fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z))));
+    te = fmax3(tmin, fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z)));
+    float tx = fmin3(tmax, fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z)));
     return tx >= te;
 }
 
@@ -614,8 +629,18 @@ RT_D Surface make_surface(const SceneView& s, const Hit& h, V3 o, V3 d) {
         V3 n = v3(a0.w, a1.w, a2.w);
         r.front = dot(d, n) < 0.0f;   // HitRecord.SetFaceNormal
         r.n = r.front ? n : -n;
-        r.tangent = length_sq(e1) > 0.0f ? normalize(e1) : v3(1.0f, 0.0f, 0.0f);
-        r.bitangent = length_sq(e2) > 0.0f ? normalize(e2) : v3(0.0f, 0.0f, 1.0f);
+        int si = s.tri_smooth ? s.tri_smooth[h.slot] : -1;
+        if (si >= 0) {   // SmoothTriangle.Hit (Geometry/SmoothTriangle.cs:166-197)
+            const SmoothTri& st = s.smooth[si];
+            float w0 = 1.0f - h.u - h.v;
+            V3 sn = normalize(w0 * st.n0 + h.u * st.n1 + h.v * st.n2);
+            r.n = r.front ? sn : -sn;   // the face normal decides the side
+            r.tangent = st.tangent;
+            r.bitangent = st.bitangent;
+        } else {
+            r.tangent = length_sq(e1) > 0.0f ? normalize(e1) : v3(1.0f, 0.0f, 0.0f);
+            r.bitangent = length_sq(e2) > 0.0f ? normalize(e2) : v3(0.0f, 0.0f, 1.0f);
+        }
         r.entity = s.tri_entity[h.slot];
         r.prim = s.tri_local[h.slot];
     } else if (h.kind == HIT_QUAD) {
@@ -1270,8 +1295,15 @@ RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, i
             float r1 = sqrtf(x1);
             float u = 1.0f - r1;
             float v = x2 * r1;
-            sp = t.v0 + u * t.e1 + v * t.e2;
-            ln = t.normal;
+            if (t.smooth >= 0) {   // SmoothTriangle.SampleAt (:219-230)
+                const SmoothTri& st = s.smooth[t.smooth];
+                float w0 = 1.0f - u - v;
+                sp = w0 * t.v0 + u * st.v1 + v * st.v2;
+                ln = normalize(w0 * st.n0 + u * st.n1 + v * st.n2);
+            } else {
+                sp = t.v0 + u * t.e1 + v * t.e2;
+                ln = t.normal;
+            }
             area = l.rep_area;
         }
         V3 tl = sp - p;
@@ -1377,6 +1409,12 @@ RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
         if (err || h.kind == HIT_NONE) return 0.0f;
         const float4* tp = s.tris + 3 * h.slot;
         V3 n = v3(__ldg(tp).w, __ldg(tp + 1).w, __ldg(tp + 2).w);
+        int si = s.tri_smooth ? s.tri_smooth[h.slot] : -1;
+        if (si >= 0) {   // the hit record's normal is the interpolated one
+            const SmoothTri& st = s.smooth[si];
+            float w0 = 1.0f - h.u - h.v;
+            n = normalize(w0 * st.n0 + h.u * st.n1 + h.v * st.n2);
+        }
         float cl = fabsf(dot(-wi, n));
         if (cl < 1e-6f) return 0.0f;
         float d2 = h.t * h.t;

@@ -42,6 +42,7 @@ static_assert(sizeof(RtStats) == 144, "ABI layout");
 static_assert(sizeof(RtBsdfQuery) == 96, "ABI layout");
 static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
 static_assert(sizeof(RtRequest) == 72, "ABI layout");
+static_assert(sizeof(RtWorldDesc) == 168, "ABI layout");
 static_assert(sizeof(RtSceneInfo) == 56, "ABI layout");
 
 constexpr int kStack = 64;       // traversal stack entries per thread
@@ -70,7 +71,7 @@ struct RtScene {
     // Copy of the world description: rt_scene_set_params rebuilds from it.
     std::vector<RtMaterialDesc> w_materials;
     std::vector<RtEntityDesc> w_entities;
-    std::vector<float> w_tris;
+    std::vector<float> w_tris, w_normals, w_uvs;
     std::vector<RtLightDesc> w_lights;
     RtWorldDesc w{};
 };
@@ -979,11 +980,17 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
         sc->w_entities.assign(world->entities, world->entities + world->num_entities);
         if (world->num_tris > 0 && world->tri_verts)
             sc->w_tris.assign(world->tri_verts, world->tri_verts + world->num_tris * 9);
+        if (world->num_tris > 0 && world->tri_normals)
+            sc->w_normals.assign(world->tri_normals, world->tri_normals + world->num_tris * 9);
+        if (world->num_tris > 0 && world->tri_uvs)
+            sc->w_uvs.assign(world->tri_uvs, world->tri_uvs + world->num_tris * 6);
         if (world->num_lights > 0 && world->lights)
             sc->w_lights.assign(world->lights, world->lights + world->num_lights);
         sc->w.materials = sc->w_materials.data();
         sc->w.entities = sc->w_entities.data();
         sc->w.tri_verts = sc->w_tris.empty() ? nullptr : sc->w_tris.data();
+        sc->w.tri_normals = sc->w_normals.empty() ? nullptr : sc->w_normals.data();
+        sc->w.tri_uvs = sc->w_uvs.empty() ? nullptr : sc->w_uvs.data();
         sc->w.lights = sc->w_lights.empty() ? nullptr : sc->w_lights.data();
     }
     if (rc != RT_OK) {
@@ -1008,6 +1015,8 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     r = r ? r : upload(sc, h.materials, &v.materials);
     r = r ? r : upload(sc, h.lights, &v.lights);
     r = r ? r : upload(sc, h.light_tris, &v.light_tris);
+    r = r ? r : upload(sc, h.smooth, &v.smooth);
+    r = r ? r : upload(sc, h.tri_smooth, &v.tri_smooth);
     r = r ? r : upload(sc, h.emitter_light, &v.emitter_light);
     r = r ? r : upload(sc, h.lut_e, &v.lut_e);
     r = r ? r : upload(sc, h.lut_eavg, &v.lut_eavg);

@@ -110,6 +110,18 @@ struct Light {
 struct LightTri {
     V3 v0, e1, e2, normal;
     float cum_area;
+    int smooth;   // index into SceneView::smooth, or -1 (flat)
+};
+
+// Shading data of a smooth triangle (Geometry/SmoothTriangle.cs:67-138): the
+// normalised vertex normals, the UV-gradient tangent frame, the vertex UVs and
+// the original v1, v2 (SampleAt weights the vertices themselves, not v0 plus
+// the edges).
+struct SmoothTri {
+    V3 n0, n1, n2;
+    V3 tangent, bitangent;
+    V3 v1, v2;
+    float uv[6];
 };
 
 struct Camera {
@@ -141,6 +153,8 @@ struct SceneView {
     const Material* materials;
     const Light* lights;
     const LightTri* light_tris;
+    const SmoothTri* smooth;
+    const int* tri_smooth;      // per triangle: index into smooth or -1; null when no triangle is smooth
     const int* emitter_light;   // material -> light index or -1
     const float* lut_e;         // 32 x 32, mu-major
     const float* lut_eavg;      // 32

@@ -409,6 +409,60 @@ Material make_material(const RtMaterialDesc& d, const float* eavg) {
     return m;
 }
 
+namespace {
+
+// Vertex normals of world triangle i, or nullptr when it is a flat Triangle
+// (no normal array, or all nine floats zero).
+const float* smooth_normals(const RtWorldDesc* w, int64_t i) {
+    if (!w->tri_normals) return nullptr;
+    const float* nn = w->tri_normals + i * 9;
+    for (int k = 0; k < 9; k++)
+        if (nn[k] != 0.0f) return nn;
+    return nullptr;
+}
+
+// The SmoothTriangle constructor (Geometry/SmoothTriangle.cs:67-126) for world
+// triangle i: normalised vertex normals and the tangent frame from the UV
+// gradients, with the edge fallback for a degenerate mapping. Returns false
+// for a flat triangle.
+bool make_smooth(const RtWorldDesc* w, int64_t i, SmoothTri& st) {
+    const float* nn = smooth_normals(w, i);
+    if (!nn) return false;
+    const float* p = w->tri_verts + i * 9;
+    V3 v0 = v3(p[0], p[1], p[2]), v1 = v3(p[3], p[4], p[5]), v2 = v3(p[6], p[7], p[8]);
+    st.n0 = normalize(v3(nn[0], nn[1], nn[2]));
+    st.n1 = normalize(v3(nn[3], nn[4], nn[5]));
+    st.n2 = normalize(v3(nn[6], nn[7], nn[8]));
+    const float def_uv[6] = {0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 1.0f};   // the no-UV constructor (:133-139)
+    const float* uv = w->tri_uvs ? w->tri_uvs + i * 6 : def_uv;
+    for (int k = 0; k < 6; k++) st.uv[k] = uv[k];
+    V3 e1 = v1 - v0, e2 = v2 - v0;
+    float d1x = uv[2] - uv[0], d1y = uv[3] - uv[1];
+    float d2x = uv[4] - uv[0], d2y = uv[5] - uv[1];
+    float det = d1x * d2y - d2x * d1y;
+    bool uv_frame = false;
+    if (std::fabs(det) > 1e-8f) {
+        float inv = 1.0f / det;
+        V3 t = inv * (d2y * e1 - d1y * e2);
+        V3 b = inv * ((-d2x) * e1 + d1x * e2);
+        float tl = length(t), bl = length(b);
+        if (tl > 1e-8f && bl > 1e-8f) {
+            st.tangent = t / tl;
+            st.bitangent = b / bl;
+            uv_frame = true;
+        }
+    }
+    if (!uv_frame) {
+        st.tangent = normalize(e1);
+        st.bitangent = normalize(e2);
+    }
+    st.v1 = v1;
+    st.v2 = v2;
+    return true;
+}
+
+}  // namespace
+
 int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
     if (!w || w->num_materials <= 0 || w->num_entities <= 0 || !w->materials || !w->entities) {
         err = "world needs at least one material and one entity";
@@ -443,6 +497,17 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             if (d.count <= 0 || d.first < 0 || d.first + d.count > w->num_tris || !w->tri_verts) {
                 err = "entity " + std::to_string(e) + ": triangle range out of bounds";
                 return RT_ERR_INVALID_ARG;
+            }
+            for (int64_t t = d.first; t < d.first + d.count; t++) {
+                const float* nn = smooth_normals(w, t);
+                if (!nn) continue;
+                for (int k = 0; k < 3; k++) {
+                    V3 n = v3(nn[3 * k], nn[3 * k + 1], nn[3 * k + 2]);
+                    if (!std::isfinite(n.x) || !std::isfinite(n.y) || !std::isfinite(n.z) || length_sq(n) == 0.0f) {
+                        err = "triangle " + std::to_string(t) + ": a vertex normal is zero or not finite";
+                        return RT_ERR_INVALID_ARG;
+                    }
+                }
             }
             mesh_ids.push_back(e);
         } else if (d.kind != RT_ENT_QUAD && d.kind != RT_ENT_SPHERE) {
@@ -556,8 +621,16 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             sc.tris.push_back(float4{e2.x, e2.y, e2.z, n.z});
             sc.tri_entity.push_back(e);
             sc.tri_local.push_back(local);
+            SmoothTri st;
+            if (make_smooth(w, d.first + local, st)) {
+                sc.tri_smooth.push_back((int)sc.smooth.size());
+                sc.smooth.push_back(st);
+            } else {
+                sc.tri_smooth.push_back(-1);
+            }
         }
     }
+    if (sc.smooth.empty()) sc.tri_smooth.clear();
     // Worst-case traversal stack: one far child per interior level of each
     // tree, plus up to 4 pending entities of a top-level fat leaf.
     sc.max_stack = top_depth + 4 + max_blas_depth + 1;
@@ -767,6 +840,12 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
                 float a = 0.5f * length(cross(v1 - v0, v2 - v0));
                 sum += a;
                 lt.cum_area = sum;
+                lt.smooth = -1;
+                SmoothTri st;
+                if (make_smooth(w, d.first + t, st)) {   // SmoothTriangle.SampleAt (:219-230)
+                    lt.smooth = (int)sc.smooth.size();
+                    sc.smooth.push_back(st);
+                }
                 sc.light_tris.push_back(lt);
             }
             l.rep_area = sum;

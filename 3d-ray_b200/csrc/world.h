@@ -31,6 +31,8 @@ struct HostScene {
     std::vector<Material> materials;
     std::vector<Light> lights;
     std::vector<LightTri> light_tris;
+    std::vector<SmoothTri> smooth;
+    std::vector<int> tri_smooth;   // per triangle (traversal order); empty when no triangle is smooth
     std::vector<int> emitter_light;
     std::vector<float> lut_e, lut_eavg;
     RtCameraDesc camera{};

@@ -66,6 +66,10 @@ class World:
     material_names: list = dataclasses.field(default_factory=list)
     entities: list = dataclasses.field(default_factory=list)
     tri_verts: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 9), np.float32))
+    # smooth triangles (SmoothTriangle): per triangle n0, n1, n2 (zeros for a
+    # flat one) and uv0, uv1, uv2; None while no triangle is smooth
+    tri_normals: np.ndarray | None = None
+    tri_uvs: np.ndarray | None = None
     lights: list = dataclasses.field(default_factory=list)
     geometry_light_samples: int = 1
     camera: dict = dataclasses.field(default_factory=dict)
@@ -87,11 +91,37 @@ class World:
         self.entities.append(dict(kind=ENT_SPHERE, material=material, center=tuple(map(float, center)),
                                   radius=float(radius), name=name))
 
-    def add_mesh(self, tris: np.ndarray, material: int, name=""):
+    def add_mesh(self, tris: np.ndarray, material: int, name="", normals=None, uvs=None, path=None):
+        """A mesh entity of world-space triangles [n, 9]. With `normals`
+        ([n, 9] vertex normals) its triangles are smooth, with `uvs` ([n, 6])
+        their tangent frame follows the UV mapping; `path` records the OBJ the
+        triangles came from."""
         tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+        n = tris.shape[0]
         first = self.tri_verts.shape[0]
         self.tri_verts = np.concatenate([self.tri_verts, tris], 0) if first else tris.copy()
-        self.entities.append(dict(kind=ENT_MESH, material=material, first=first, count=tris.shape[0], name=name))
+        if normals is not None or self.tri_normals is not None:
+            nn = np.zeros((n, 9), np.float32) if normals is None else \
+                np.ascontiguousarray(normals, np.float32).reshape(n, 9)
+            uu = np.tile(np.array([0, 0, 1, 0, 0, 1], np.float32), (n, 1)) if uvs is None else \
+                np.ascontiguousarray(uvs, np.float32).reshape(n, 6)
+            if self.tri_normals is None:
+                self.tri_normals = np.zeros((first, 9), np.float32)
+                self.tri_uvs = np.tile(np.array([0, 0, 1, 0, 0, 1], np.float32), (first, 1))
+            self.tri_normals = np.concatenate([self.tri_normals, nn], 0)
+            self.tri_uvs = np.concatenate([self.tri_uvs, uu], 0)
+        self.entities.append(dict(kind=ENT_MESH, material=material, first=first, count=n, name=name,
+                                  path=path))
+
+    def add_obj(self, path: str, material: int, name=""):
+        """A mesh entity loaded from an OBJ file the way the reference's
+        ObjLoader does without subdivision (see objfile.load_obj); returns the
+        loader's warnings."""
+        from . import objfile
+        m = objfile.load_obj(path)
+        self.add_mesh(m.tris, material, name=name or os.path.basename(path), normals=m.normals, uvs=m.uvs,
+                      path=path)
+        return m.warnings
 
     @property
     def num_tris(self) -> int:
@@ -230,6 +260,38 @@ def cornell_sphere(params: dict | None = None, shadow_samples: int = 1) -> World
     return w
 
 
+def smooth_icosphere(level: int, center, radius: float, with_uvs: bool = True):
+    """Triangles [n, 9] of a level-`level` icosphere of `radius` around
+    `center`, its exact vertex normals [n, 9] (smooth triangles) and, with
+    `with_uvs`, a longitude/latitude mapping [n, 6] (else None)."""
+    v, f = icosphere(level)
+    tris = (v * float(radius) + np.asarray(center, np.float64))[f].reshape(-1, 9).astype(np.float32)
+    normals = v[f].reshape(-1, 9).astype(np.float32)
+    uvs = None
+    if with_uvs:
+        lon = np.arctan2(v[:, 2], v[:, 0]) / (2 * math.pi) + 0.5
+        lat = np.arcsin(np.clip(v[:, 1], -1, 1)) / math.pi + 0.5
+        uvs = np.stack([lon, lat], 1)[f].reshape(-1, 6).astype(np.float32)
+    return tris, normals, uvs
+
+
+def cornell_smooth(shadow_samples: int = 1) -> World:
+    """Smooth triangles (SmoothTriangle) in the Cornell box: a UV-mapped
+    smooth icosphere with an anisotropic metallic Disney material in place of
+    the tall box (its shading normal and UV tangent frame both matter) and a
+    small smooth emissive icosphere, a geometry light whose samples and pdf
+    use the interpolated normal."""
+    w = cornell(shadow_samples, tall_box=False)
+    w.name = "cornell-smooth"
+    aniso = w.add_material("aniso", disney((0.8, 0.6, 0.3), roughness=0.3, metallic=0.7, anisotropic=0.8))
+    tris, nn, uv = smooth_icosphere(3, (370, 100, 350), 100.0)
+    w.add_mesh(tris, aniso, name="smooth_sphere", normals=nn, uvs=uv)
+    glow = w.add_material("glow", emissive((6.0, 5.0, 3.0), 1.0))
+    tris, nn, _ = smooth_icosphere(1, (150, 380, 300), 35.0, with_uvs=False)
+    w.add_mesh(tris, glow, name="smooth_light", normals=nn)
+    return w
+
+
 def cornell_volume(shadow_samples: int = 1, density: float = 1.0) -> World:
     """C5: homogeneous medium (sigma_t 0.02 per unit times `density`, albedo
     0.8, HG g 0.6) filling the box, and a dielectric sphere (IOR 1.5,
@@ -333,8 +395,9 @@ def batch_requests(n: int = 32, seed: int = DEFAULT_REQUEST_SEED, radius: float 
 # --- reference-compatible YAML + OBJ ------------------------------------------
 
 def write_yaml(world: World, out_dir: str, name: str | None = None) -> str:
-    """Writes `<name>.yaml` plus one OBJ per mesh entity (world-space vertices,
-    no normals -> flat Triangle faces in ObjLoader.BuildTrianglesDirect)."""
+    """Writes `<name>.yaml` plus one OBJ per mesh entity (world-space vertices;
+    smooth meshes with their vertex normals and UVs, which ObjLoader turns into
+    SmoothTriangle faces, flat ones without, which it turns into Triangle)."""
     import yaml
 
     name = name or world.name or "scene"
@@ -367,14 +430,18 @@ def write_yaml(world: World, out_dir: str, name: str | None = None) -> str:
             ents.append(dict(name=e["name"] or f"e{i}", type="sphere", center=list(e["center"]),
                              radius=e["radius"], material=mname))
         else:
+            from . import objfile
             fn = f"{name}_{i}.obj"
-            tris = world.tri_verts[e["first"]:e["first"] + e["count"]].reshape(-1, 3, 3)
-            with open(os.path.join(out_dir, fn), "w") as f:
-                for t in tris:
-                    for p in t:
-                        f.write(f"v {p[0]:.9g} {p[1]:.9g} {p[2]:.9g}\n")
-                for k in range(tris.shape[0]):
-                    f.write(f"f {3 * k + 1} {3 * k + 2} {3 * k + 3}\n")
+            sl = slice(e["first"], e["first"] + e["count"])
+            nn = uv = None
+            if world.tri_normals is not None:
+                smooth = np.any(world.tri_normals[sl] != 0.0, axis=1)
+                if smooth.any() and not smooth.all():
+                    raise ValueError(f"mesh entity {i} mixes flat and smooth triangles, which one OBJ cannot "
+                                     "express (ObjLoader drops a partial normal channel)")
+                if smooth.all():
+                    nn, uv = world.tri_normals[sl], world.tri_uvs[sl]
+            objfile.write_obj(os.path.join(out_dir, fn), world.tri_verts[sl], nn, uv)
             ents.append(dict(name=e["name"] or f"e{i}", type="mesh", path=fn, material=mname))
     lights = []
     for l in world.lights:

@@ -150,6 +150,14 @@ typedef struct RtWorldDesc {
     int32_t geometry_light_samples;   /* ShadowSamples of derived geometry lights */
     RtCameraDesc camera;
     RtMediumDesc medium;
+    /* Smooth triangles (Geometry/SmoothTriangle.cs, what ObjLoader.cs:355-395
+     * builds for faces with vertex normals): null, or 9 floats per triangle,
+     * the vertex normals n0, n1, n2 (normalised on load). All nine zero marks
+     * a flat Triangle. */
+    const float*          tri_normals;
+    /* null, or 6 floats per triangle: uv0, uv1, uv2 of a smooth triangle, for
+     * its UV-gradient tangent frame (null: (0,0), (1,0), (0,1)). */
+    const float*          tri_uvs;
 } RtWorldDesc;
 
 /* ---- render parameters: the Renderer constructor (Renderer.cs:300-319) --- */

@@ -268,10 +268,42 @@ struct Hittable {
     virtual AABB bbox() const = 0;
 };
 
-struct Triangle : Hittable {   // Geometry/Triangle.cs
+struct Triangle : Hittable {   // Geometry/Triangle.cs, or SmoothTriangle.cs when smooth
     V3 v0, v1, v2, e1, e2, normal, tangent, bitangent;
     float area;
     int material, entity, prim;
+    bool smooth = false;
+    V3 n0{}, n1{}, n2{};
+    float uv[6] = {0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 1.0f};
+    // SmoothTriangle constructor (SmoothTriangle.cs:67-126): normalised vertex
+    // normals, vertex UVs (the no-UV constructor's (0,0), (1,0), (0,1) when
+    // uvs is null) and the tangent frame from the UV gradients, with the edge
+    // fallback for a degenerate mapping. The face normal, area and edges are
+    // the flat triangle's.
+    void make_smooth(const float* nn, const float* uvs) {
+        smooth = true;
+        n0 = normalize(v3(nn[0], nn[1], nn[2]));
+        n1 = normalize(v3(nn[3], nn[4], nn[5]));
+        n2 = normalize(v3(nn[6], nn[7], nn[8]));
+        if (uvs)
+            for (int k = 0; k < 6; k++) uv[k] = uvs[k];
+        float d1x = uv[2] - uv[0], d1y = uv[3] - uv[1];
+        float d2x = uv[4] - uv[0], d2y = uv[5] - uv[1];
+        float det = d1x * d2y - d2x * d1y;
+        if (std::fabs(det) > 1e-8f) {
+            float inv = 1.0f / det;
+            V3 t = inv * (d2y * e1 - d1y * e2);
+            V3 b = inv * ((-d2x) * e1 + d1x * e2);
+            float tl = length(t), bl = length(b);
+            if (tl > 1e-8f && bl > 1e-8f) {
+                tangent = t / tl;
+                bitangent = b / bl;
+                return;
+            }
+        }
+        tangent = normalize(e1);
+        bitangent = normalize(e2);
+    }
     Triangle(V3 a, V3 b, V3 c, int mat, int ent, int pr) : v0(a), v1(b), v2(c), material(mat), entity(ent), prim(pr) {
         e1 = v1 - v0;   // Triangle.cs:35-47
         e2 = v2 - v0;
@@ -298,7 +330,17 @@ struct Triangle : Hittable {   // Geometry/Triangle.cs
         if (t < tmin || t > tmax) return false;
         rec.t = t;
         rec.p = r.at(t);
-        rec.set_face_normal(r, normal);
+        if (smooth) {   // SmoothTriangle.cs:166-197: interpolated normal, face normal decides the side
+            float w0 = 1.0f - u - v;
+            V3 sn = normalize(w0 * n0 + u * n1 + v * n2);
+            rec.front = dot(r.d, normal) < 0.0f;
+            rec.n = rec.front ? sn : -sn;
+        } else {
+            rec.set_face_normal(r, normal);
+        }
+        // The barycentrics, for both kinds: a smooth triangle's record holds
+        // the interpolated UV instead, which only texture lookups read, and
+        // textures are constant on this path.
         rec.u = u;
         rec.v = v;
         rec.tangent = tangent;
@@ -318,6 +360,12 @@ struct Triangle : Hittable {   // Geometry/Triangle.cs
         float r1 = std::sqrt(xi1);
         u = 1.0f - r1;
         v = xi2 * r1;
+        if (smooth) {   // SmoothTriangle.SampleAt (:219-230): weights on the vertices themselves
+            float w0 = 1.0f - u - v;
+            p = w0 * v0 + u * v1 + v * v2;
+            n = normalize(w0 * n0 + u * n1 + v * n2);
+            return;
+        }
         p = v0 + u * e1 + v * e2;
         n = normal;
     }
@@ -2240,6 +2288,12 @@ int or_scene_create(const RtWorldDesc* w, void** out) {
                 const float* p = w->tri_verts + (ed.first + t) * 9;
                 m->tris.emplace_back(new Triangle(v3(p[0], p[1], p[2]), v3(p[3], p[4], p[5]), v3(p[6], p[7], p[8]),
                                                   ed.material, e, (int)t));
+                if (w->tri_normals) {   // ObjLoader.BuildTrianglesDirect: a face with normals is smooth
+                    const float* nn = w->tri_normals + (ed.first + t) * 9;
+                    bool any = false;
+                    for (int k = 0; k < 9; k++) any = any || nn[k] != 0.0f;
+                    if (any) m->tris.back()->make_smooth(nn, w->tri_uvs ? w->tri_uvs + (ed.first + t) * 6 : nullptr);
+                }
             }
             m->finish();
             h = m.get();
