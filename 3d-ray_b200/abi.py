@@ -108,6 +108,11 @@ class RtSceneInfo(C.Structure):
                 ("pad", C.c_int32), ("device_bytes", C.c_int64)]
 
 
+class RtCapture(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("beauty_a", "beauty_b", "albedo_a", "albedo_b", "normal_a", "normal_b",
+                                          "depth_a", "depth_b")]
+
+
 class RtRequest(C.Structure):
     _fields_ = [("scene", C.c_int32), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("max_depth", C.c_int32), ("pad", C.c_int32), ("camera", RtCameraDesc)]
@@ -263,6 +268,7 @@ def load(path: str | None = None):
                                        P, C.c_int64]),
         "rt_render": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtStats)]),
         "rt_render_device": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtStats)]),
+        "rt_render_capture": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtCapture), C.POINTER(RtStats)]),
         "rt_render_device_noalloc": (C.c_int, [P, C.POINTER(RtRenderParams), P, C.POINTER(RtStats)]),
         "rt_render_batch": (C.c_int, [P, C.c_int32, P, C.c_int32, C.POINTER(RtRenderParams), P,
                                       C.POINTER(RtStats)]),

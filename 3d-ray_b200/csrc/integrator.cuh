@@ -247,6 +247,20 @@ struct NoAdjoint {
     // The vertex attenuation: att_pre before Russian roulette, att after. For
     // the legacy path, the lobe and direction of the null sample before it.
     RT_D void scatter(const PathState&, const Material&, const Surface&, V3, V3, int, int, float, V3, V3, int, V3) {}
+
+    // Capture hooks (the AOV probe, Renderer.cs:1051-1054, 1139-1145,
+    // 1271-1277, 1657-1662, 1716-1724, 1849-1850). None of them draws from
+    // the sampler, so a capturing render traces the same paths.
+    // The closest hit of the current ray (d its direction).
+    RT_D void aov_ray(const Hit&, V3) {}
+    // A medium scattering event at distance t along direction d.
+    RT_D void aov_medium(float, V3) {}
+    // The ray left the scene (black flat sky).
+    RT_D void aov_miss() {}
+    // The surface ShadeSurface is about to shade.
+    RT_D void aov_surface(V3, const Material&) {}
+    // The bounce decision: a delta lobe with attenuation f, or a non-delta one.
+    RT_D void aov_bounce(bool, V3) {}
 };
 
 // One vertex of TraceRay given the closest hit of the current ray: the
@@ -258,6 +272,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
                                              Sink& sink) {
     bool hit = h.kind != HIT_NONE;
     V3 beta_s = ps.beta;
+    sink.aov_ray(h, ps.d);
     if (s.has_medium) {
         float tmax = hit ? h.t : 1e30f;
         float tmed;
@@ -265,6 +280,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         bool sc = medium_sample(s, tmax, ps.rng, tmed, mb);
         if (sc) {
             V3 p = ps.o + ps.d * tmed;
+            sink.aov_medium(tmed, ps.d);
             sink.segment(ps, tmed, SEG_MEDIUM_SCATTER);
             ps.w = ps.w * bl_factor(ps.cur_abs, tmed) * mb;
             nee_medium(s, rc, ps, p, ps.d, sink);
@@ -296,11 +312,15 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         ps.w = ps.w * mb;
         beta_s = ps.beta * mb;
     }
-    if (!hit) return false;   // black flat sky: SampleSky returns 0
+    if (!hit) {   // black flat sky: SampleSky returns 0
+        sink.aov_miss();
+        return false;
+    }
     sink.segment(ps, h.t, SEG_ABSORPTION);
     ps.w = ps.w * bl_factor(ps.cur_abs, h.t);
     Surface rec = make_surface(s, h, ps.o, ps.d);
     const Material& m = s.materials[rec.material];
+    sink.aov_surface(rec.n, m);
     int to_la = ps.clamp_mode;
     if (m.type != 0) {   // Emissive: Emit (front face only), no NEE, no scatter
         if (rec.front && (m.emission.x > 0.0f || m.emission.y > 0.0f || m.emission.z > 0.0f)) {
@@ -327,6 +347,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
             if (a <= 0.0f || bs.pdf <= 0.0f) return false;
             att = bs.f * a / bs.pdf;
         }
+        sink.aov_bounce(bs.is_delta, bs.f);
         next_beta = beta_s * att;
         V3 att_pre = att;
         if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
@@ -347,6 +368,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         V3 sdir;
         int lobe;
         if (!bsdf_scatter(s, m, rec, ps.d, rel_eta, ps.rng, att, sdir, lobe)) return false;
+        sink.aov_bounce(false, att);   // Disney's IsDeltaScatter is false
         next_beta = beta_s * att;
         V3 att_pre = att;
         if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
@@ -412,6 +434,95 @@ __device__ V3 trace_sample(const SceneView& s, const RenderConst& rc, int px, in
         traverse<false, STACK>(s, ps.o, ps.d, kEps, kInf, h, COUNT ? &cnt->closest : nullptr, err);
         if (!shade_vertex(s, rc, ps, h, sink)) break;
     }
+    return path_resolve(ps, rc);
+}
+
+// The AOV probe of one camera path (Renderer.cs:776-815): depth at the camera
+// ray's first surface hit; albedo and normal at the first non-delta surface,
+// with a specular chain's tint folded into weight; a medium scatter commits
+// white with no normal, a miss the (black) sky.
+struct AovProbe {
+    bool pending, have_depth, camera;
+    float depth;
+    V3 weight, tent_albedo, tent_normal, albedo, normal;
+    RT_D void reset() {
+        pending = true;
+        have_depth = false;
+        camera = true;
+        depth = -1.0f;
+        weight = v3(1.0f);
+        tent_albedo = v3(1.0f);
+        tent_normal = v3(0.0f);
+        albedo = v3(0.0f);
+        normal = v3(0.0f);
+    }
+    RT_D void commit() {
+        albedo = weight * tent_albedo;
+        normal = tent_normal;
+        pending = false;
+    }
+    RT_D void commit_as(V3 a, V3 n) {
+        albedo = weight * a;
+        normal = n;
+        pending = false;
+    }
+};
+
+RT_D V3 clamp01(V3 v) {   // Vector3.Clamp(v, Zero, One)
+    return v3(fminf(fmaxf(v.x, 0.0f), 1.0f), fminf(fmaxf(v.y, 0.0f), 1.0f), fminf(fmaxf(v.z, 0.0f), 1.0f));
+}
+
+// The megakernel's shadow sink plus the capture hooks on a probe.
+template <int STACK>
+struct CaptureShadows : InlineShadows<STACK> {
+    AovProbe* probe;
+    RT_D void aov_ray(const Hit& h, V3 d) {
+        AovProbe& p = *probe;
+        if (p.camera && h.kind != HIT_NONE && p.pending && !p.have_depth) {   // :1657-1662
+            p.depth = h.t * length(d);
+            p.have_depth = true;
+        }
+        p.camera = false;
+    }
+    RT_D void aov_medium(float t, V3 d) {   // :1716-1724
+        AovProbe& p = *probe;
+        if (!p.pending) return;
+        if (!p.have_depth) {
+            p.depth = t * length(d);
+            p.have_depth = true;
+        }
+        p.commit_as(v3(1.0f), v3(0.0f));
+    }
+    RT_D void aov_miss() {   // :1849-1850, a black flat sky
+        if (probe->pending) probe->commit_as(v3(0.0f), v3(0.0f));
+    }
+    RT_D void aov_surface(V3 n, const Material& m) {   // :1051-1054
+        if (!probe->pending) return;
+        probe->tent_normal = n;
+        probe->tent_albedo = clamp01(m.base);   // AovAlbedo: baseColor, or an Emissive's colour
+    }
+    RT_D void aov_bounce(bool delta, V3 f) {   // :1139-1145, 1271-1277
+        if (!probe->pending) return;
+        if (delta) probe->weight = probe->weight * clamp01(f);
+        else probe->commit();
+    }
+};
+
+// trace_sample with the probe: returns the clamped sample radiance and leaves
+// the path's committed features in *probe.
+template <int STACK>
+__device__ V3 trace_capture(const SceneView& s, const RenderConst& rc, int px, int py, uint32_t sample_index,
+                            AovProbe* probe, int* err) {
+    PathState ps;
+    path_init(ps, rc, px, py, sample_index);
+    probe->reset();
+    CaptureShadows<STACK> sink{{{}, &s, rc.opaque, nullptr, err}, probe};
+    while (path_alive(ps)) {
+        Hit h;
+        traverse<false, STACK>(s, ps.o, ps.d, kEps, kInf, h, nullptr, err);
+        if (!shade_vertex(s, rc, ps, h, sink)) break;
+    }
+    if (probe->pending) probe->commit();   // CaptureAccumulator.Add (:835-837)
     return path_resolve(ps, rc);
 }
 

@@ -43,6 +43,7 @@ static_assert(sizeof(RtBsdfQuery) == 96, "ABI layout");
 static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
 static_assert(sizeof(RtRequest) == 72, "ABI layout");
 static_assert(sizeof(RtWorldDesc) == 168, "ABI layout");
+static_assert(sizeof(RtCapture) == 64, "ABI layout");
 static_assert(sizeof(RtSceneInfo) == 56, "ABI layout");
 
 constexpr int kStack = 64;       // traversal stack entries per thread
@@ -195,6 +196,93 @@ __global__ void k_resolve(const float* partial, int nchunks, int ww, int wh, int
         for (int k = 1; k < nchunks; k++) a += partial[(size_t)k * 3 * plane + (size_t)c * plane + i];
         film[c * fplane + fi] = a / (float)spp;
     }
+}
+
+// Capturing megakernel (Renderer.Render with RenderCaptureOptions.Full): the
+// megakernel plus the AOV probe and the even/odd sample halves of
+// CaptureAccumulator (Renderer.cs:817-856). Per chunk and pixel it writes
+// kCapSums partial sums, plane after plane: beauty, beauty A, beauty B,
+// albedo A, albedo B, normal A, normal B (3 each), then depth A, depth B and
+// the A and B depth counts.
+constexpr int kCapSums = 25;
+template <int STACK>
+__global__ void __launch_bounds__(kBlock) k_render_capture(rt::SceneView s, rt::RenderConst rc, int ww, int wh,
+                                                            int spp0, int per_chunk, int spp, float* partial,
+                                                            int* err) {
+    int lx = blockIdx.x * 16 + (threadIdx.x & 15);
+    int ly = blockIdx.y * 8 + (threadIdx.x >> 4);
+    int chunk = blockIdx.z;
+    if (lx >= ww || ly >= wh) return;
+    int sb = chunk * per_chunk;
+    int se = min(sb + per_chunk, spp);
+    V3 sum = rt::v3(0.0f), sa = rt::v3(0.0f), sbv = rt::v3(0.0f);
+    V3 aa = rt::v3(0.0f), ab = rt::v3(0.0f), na = rt::v3(0.0f), nb = rt::v3(0.0f);
+    float da = 0.0f, db = 0.0f, ca = 0.0f, cb = 0.0f;
+    rt::AovProbe probe;
+    for (int si = sb; si < se; si++) {
+        V3 l = rt::trace_capture<STACK>(s, rc, lx, ly, (uint32_t)(spp0 + si), &probe, err);
+        sum = sum + l;
+        if ((si & 1) == 0) {   // A: even samples of the call
+            sa = sa + l;
+            aa = aa + probe.albedo;
+            na = na + probe.normal;
+            if (probe.have_depth) {
+                da += probe.depth;
+                ca += 1.0f;
+            }
+        } else {
+            sbv = sbv + l;
+            ab = ab + probe.albedo;
+            nb = nb + probe.normal;
+            if (probe.have_depth) {
+                db += probe.depth;
+                cb += 1.0f;
+            }
+        }
+    }
+    size_t plane = (size_t)ww * wh;
+    float* out = partial + (size_t)chunk * kCapSums * plane + (size_t)ly * ww + lx;
+    const V3 v[7] = {sum, sa, sbv, aa, ab, na, nb};
+    for (int k = 0; k < 7; k++) {
+        out[(3 * k) * plane] = v[k].x;
+        out[(3 * k + 1) * plane] = v[k].y;
+        out[(3 * k + 2) * plane] = v[k].z;
+    }
+    out[21 * plane] = da;
+    out[22 * plane] = db;
+    out[23 * plane] = ca;
+    out[24 * plane] = cb;
+}
+
+// The capture's means (RenderBuffers: CaptureAccumulator.Store, Renderer.cs:
+// 858-882): A holds ceil(n/2) samples, B floor(n/2), and B mirrors A when
+// n == 1; a depth half with no hit is -1. Writes 23 planes: beauty, beauty A,
+// beauty B, albedo A, albedo B, normal A, normal B (3 each), depth A, depth B.
+__global__ void k_resolve_capture(const float* partial, int nchunks, int ww, int wh, int spp, float* outp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int plane = ww * wh;
+    if (i >= plane) return;
+    float acc[kCapSums];
+    for (int k = 0; k < kCapSums; k++) {
+        float a = partial[(size_t)k * plane + i];
+        for (int c = 1; c < nchunks; c++) a += partial[(size_t)c * kCapSums * plane + (size_t)k * plane + i];
+        acc[k] = a;
+    }
+    int n_a = (spp + 1) / 2, n_b = spp / 2;
+    auto put = [&](int p, float x) { outp[(size_t)p * plane + i] = x; };
+    for (int c = 0; c < 3; c++) {
+        put(c, acc[c] / (float)spp);   // cumulativeColor / actualSamples
+        for (int q = 0; q < 3; q++) {  // beauty, albedo, normal halves
+            float ma = acc[3 + 6 * q + c] / (float)n_a;
+            float mb = n_b > 0 ? acc[6 + 6 * q + c] / (float)n_b : ma;
+            put(3 + 6 * q + c, ma);
+            put(6 + 6 * q + c, mb);
+        }
+    }
+    float dA = acc[23] > 0.0f ? acc[21] / acc[23] : -1.0f;
+    float dB = n_b > 0 ? (acc[24] > 0.0f ? acc[22] / acc[24] : -1.0f) : dA;
+    put(21, dA);
+    put(22, dB);
 }
 
 // Path-replay adjoint: one thread per (pixel, sample) work item, samples
@@ -1135,6 +1223,62 @@ int rt_render_device(RtScene* sc, const RtRenderParams* p, float* d_film, RtStat
     if (!sc || !d_film) return fail(RT_ERR_INVALID_ARG, "null argument");
     std::lock_guard<std::mutex> lk(sc->mu);
     return render_to_device(sc, p, sc->host.camera, d_film, st);
+}
+
+int rt_render_capture(RtScene* sc, const RtRenderParams* p, float* out, const RtCapture* cap, RtStats* st) {
+    if (!sc || !p || !out || !cap) return fail(RT_ERR_INVALID_ARG, "null argument");
+    if (p->window_w > 0 || p->window_h > 0 || p->pixel_x0 != 0 || p->pixel_y0 != 0)
+        return fail(RT_ERR_INVALID_ARG, "a capturing render covers the whole frame");
+    if (p->count_work) return fail(RT_ERR_INVALID_ARG, "count_work is not available with capture");
+    std::lock_guard<std::mutex> lk(sc->mu);
+    auto t0 = std::chrono::steady_clock::now();
+    int rc_ = validate_params(sc, p);
+    if (rc_ != RT_OK) return rc_;
+    CUDA_TRY(cudaSetDevice(sc->device));
+    rt::RenderConst rc = make_rc(sc, p, sc->host.camera);
+    int ww = p->width, wh = p->height;
+    int64_t npix = (int64_t)ww * wh;
+    int64_t target = 148LL * 2048 * 2;
+    int nchunks = (int)std::min<int64_t>(p->spp, std::max<int64_t>(1, (target + npix - 1) / npix));
+    int per_chunk = (p->spp + nchunks - 1) / nchunks;
+    nchunks = (p->spp + per_chunk - 1) / per_chunk;
+    size_t partial_bytes = (size_t)nchunks * kCapSums * npix * sizeof(float);
+    size_t out_bytes = (size_t)23 * npix * sizeof(float);
+    rc_ = ensure_scratch(sc, partial_bytes + out_bytes);
+    if (rc_ != RT_OK) return rc_;
+    float* partial = static_cast<float*>(sc->scratch);
+    float* res = reinterpret_cast<float*>(static_cast<char*>(sc->scratch) + partial_bytes);
+    CUDA_TRY(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream));
+    dim3 grid((ww + 15) / 16, (wh + 7) / 8, nchunks);
+    CUDA_TRY(cudaEventRecord(sc->ev0, sc->stream));
+    k_render_capture<kStack><<<grid, kBlock, 0, sc->stream>>>(sc->view, rc, ww, wh, p->spp_offset, per_chunk, p->spp,
+                                                              partial, sc->d_err);
+    k_resolve_capture<<<(unsigned)((npix + 255) / 256), 256, 0, sc->stream>>>(partial, nchunks, ww, wh, p->spp, res);
+    CUDA_TRY(cudaEventRecord(sc->ev1, sc->stream));
+    CUDA_TRY(cudaGetLastError());
+    // the planes the caller asked for, in the result's plane order
+    float* const dst[9] = {out, cap->beauty_a, cap->beauty_b, cap->albedo_a, cap->albedo_b,
+                           cap->normal_a, cap->normal_b, cap->depth_a, cap->depth_b};
+    const int first[9] = {0, 3, 6, 9, 12, 15, 18, 21, 22};
+    for (int k = 0; k < 9; k++) {
+        if (!dst[k]) continue;
+        size_t nb = (size_t)(k < 7 ? 3 : 1) * npix * sizeof(float);
+        CUDA_TRY(cudaMemcpyAsync(dst[k], res + (size_t)first[k] * npix, nb, cudaMemcpyDeviceToHost, sc->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(sc->stream));
+    rc_ = check_err(sc);
+    if (rc_ != RT_OK) return rc_;
+    if (st) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+        st->kernel_ms = ms;
+        st->samples = (uint64_t)npix * (uint64_t)p->spp;
+        st->kernel_launches = 2;
+        st->rr_min_bounces = rc.rr_min_bounces;
+        st->rr_min_survival = rc.rr_min_survival;
+        st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return RT_OK;
 }
 
 }  // extern "C"

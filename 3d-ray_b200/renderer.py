@@ -26,11 +26,81 @@ LIGHT_STRATEGY = {"all": 0}
 KERNELS = {"megakernel": abi.KERNEL_MEGAKERNEL, "wavefront": abi.KERNEL_WAVEFRONT}
 
 
+@dataclasses.dataclass(frozen=True)
+class RenderCaptureOptions:
+    """Which side buffers a render captures (Rendering/RenderBuffers.cs:9-23)."""
+    capture_beauty_halves: bool = False
+    capture_aovs: bool = False
+
+    @property
+    def any(self) -> bool:
+        return self.capture_beauty_halves or self.capture_aovs
+
+
+RenderCaptureOptions.NONE = RenderCaptureOptions()
+RenderCaptureOptions.FULL = RenderCaptureOptions(True, True)
+
+
+@dataclasses.dataclass
+class RenderBuffers:
+    """Linear-HDR frame data of a capturing render (RenderBuffers.cs:50-169):
+    every quantity split by sample-index parity into A (the ceil(n/2) even
+    samples) and B (the floor(n/2) odd ones), each a mean; B mirrors A when
+    n == 1. Depth is the world-space distance to the camera ray's first hit,
+    -1 where no sample of the half hit geometry. Colour planes are [3, H, W],
+    depth [H, W]."""
+    width: int
+    height: int
+    sample_count: np.ndarray     # [H * W] int32 (uniform)
+    samples_a: int
+    samples_b: int
+    beauty: np.ndarray
+    beauty_a: np.ndarray
+    beauty_b: np.ndarray
+    albedo_a: np.ndarray | None = None
+    albedo_b: np.ndarray | None = None
+    normal_a: np.ndarray | None = None
+    normal_b: np.ndarray | None = None
+    depth_a: np.ndarray | None = None
+    depth_b: np.ndarray | None = None
+
+    @property
+    def has_aovs(self) -> bool:
+        return self.albedo_a is not None
+
+    def combine_halves(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        """(nA * A + nB * B) / n (:101-118)."""
+        n = self.samples_a + self.samples_b
+        if self.samples_b == 0:
+            return a.copy()
+        wa = np.float32(np.float32(self.samples_a) / np.float32(n))
+        wb = np.float32(np.float32(self.samples_b) / np.float32(n))
+        return (wa * a.astype(np.float32) + wb * b.astype(np.float32)).astype(np.float32)
+
+    def combine_depth_halves(self) -> np.ndarray:
+        """Sentinel-aware depth combination (:125-150)."""
+        if self.depth_a is None:
+            raise ValueError("Depth AOV was not captured.")
+        n = self.samples_a + self.samples_b
+        wa = np.float32(np.float32(self.samples_a) / np.float32(n)) if n > 0 else np.float32(1.0)
+        wb = np.float32(np.float32(1.0) - wa)
+        a, b = self.depth_a.astype(np.float32), self.depth_b.astype(np.float32)
+        both = a * wa + b * wb if self.samples_b else a
+        out = np.where(a < 0, np.where(b < 0, np.float32(-1.0), b), np.where(b < 0, a, both))
+        return out.astype(np.float32)
+
+    def raw_beauty_variance(self) -> np.ndarray:
+        """((A - B) / 2)^2 per channel (:157-168)."""
+        d = np.float32(0.5) * (self.beauty_a.astype(np.float32) - self.beauty_b.astype(np.float32))
+        return (d * d).astype(np.float32)
+
+
 @dataclasses.dataclass
 class RenderResult:
     pixels: np.ndarray        # [H, W, 3] display RGB in [0, 1]
     beauty: np.ndarray        # [3, H, W] linear HDR (mean of clamped samples)
     stats: dict
+    buffers: RenderBuffers | None = None
 
 
 class Renderer:
@@ -89,13 +159,29 @@ class Renderer:
         return dict(wavefront_size=best.wavefront_size, block_size=best.block_size,
                     sort_materials=best.sort_materials)
 
-    def render(self, width: int, height: int, **kw) -> RenderResult:
+    def render(self, width: int, height: int, capture: RenderCaptureOptions | None = None, **kw) -> RenderResult:
+        """Renderer.Render(w, h[, RenderCaptureOptions]). A capture runs the
+        plain megakernel (rt_render_capture) and fills `buffers`."""
         p = self.params(width, height, **kw)
         beauty = np.zeros((3, height, width), np.float32)
         st = abi.RtStats()
-        abi.check(self._lib.rt_render(self._scene, C.byref(p), abi.ptr(beauty), C.byref(st)), "rt_render")
+        bufs = None
+        if capture is not None and capture.any:
+            planes = {k: np.zeros((3, height, width), np.float32) for k in ("beauty_a", "beauty_b")}
+            if capture.capture_aovs:
+                for k in ("albedo_a", "albedo_b", "normal_a", "normal_b"):
+                    planes[k] = np.zeros((3, height, width), np.float32)
+                for k in ("depth_a", "depth_b"):
+                    planes[k] = np.zeros((height, width), np.float32)
+            cap = abi.RtCapture(**{k: v.ctypes.data for k, v in planes.items()})
+            abi.check(self._lib.rt_render_capture(self._scene, C.byref(p), abi.ptr(beauty), C.byref(cap),
+                                                  C.byref(st)), "rt_render_capture")
+            bufs = RenderBuffers(width, height, np.full(width * height, self.spp, np.int32), (self.spp + 1) // 2,
+                                 self.spp // 2, beauty, **planes)
+        else:
+            abi.check(self._lib.rt_render(self._scene, C.byref(p), abi.ptr(beauty), C.byref(st)), "rt_render")
         return RenderResult(self.tone_map_to_display(beauty), beauty,
-                            {f: getattr(st, f) for f, _ in abi.RtStats._fields_})
+                            {f: getattr(st, f) for f, _ in abi.RtStats._fields_}, bufs)
 
     def tone_map_to_display(self, beauty: np.ndarray) -> np.ndarray:
         """Renderer.ToneMapToDisplay (:741): exposure, ACES, gamma on the GPU."""

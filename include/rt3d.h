@@ -313,6 +313,33 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
                     const RtRequest* requests, int32_t n,
                     const RtRenderParams* common, float* const* outs, RtStats* stats);
 
+/* Capture planes of a capturing render (Rendering/RenderBuffers.cs): the
+ * linear-HDR even/odd sample halves the denoiser's variance estimate needs,
+ * and the first-non-delta-hit AOVs, each split the same way. A holds the
+ * ceil(n/2) even samples of the call, B the floor(n/2) odd ones (B mirrors A
+ * when n == 1); each is a mean. Colour planes are 3*W*H floats (planar),
+ * depth W*H (world-space distance; -1 where no sample of the half hit
+ * geometry). Host pointers, each null to skip its plane. */
+typedef struct RtCapture {
+    float* beauty_a;
+    float* beauty_b;
+    float* albedo_a;
+    float* albedo_b;
+    float* normal_a;
+    float* normal_b;
+    float* depth_a;
+    float* depth_b;
+} RtCapture;
+
+/* Renderer.Render(w, h, RenderCaptureOptions.Full) (Renderer.cs:522-733 with
+ * the AOV probe :755-856): the beauty film as rt_render plus the planes of
+ * `capture`. It always runs the plain megakernel (params->kernel is ignored)
+ * over the whole frame; a render window or count_work is RT_ERR_INVALID_ARG.
+ * The capture draws nothing from the sampler, so the beauty film equals
+ * rt_render's megakernel film up to the order of the per-pixel sums. */
+int rt_render_capture(RtScene* scene, const RtRenderParams* params, float* hdr_rgb_planar,
+                      const RtCapture* capture, RtStats* stats);
+
 /* Autotuner: times the wavefront over wavefront size {256K, 1M, 4M} x block
  * {64, 128, 256} x material sort {off, on} x node layout {two-wide,
  * four-wide}, then, on the winner, the extend/occlude block {64, 128, 256},

@@ -49,6 +49,7 @@ def lib():
             ("or_trace_any", C.c_int, [P, P, C.c_int64, P]),
             ("or_bsdf_batch", C.c_int, [P, P, C.c_int64, P]),
             ("or_render", C.c_int, [P, P, P, C.c_int32, P]),
+            ("or_render_capture", C.c_int, [P, P, P, C.c_int32]),
         ]:
             f = getattr(L, name)
             f.restype = res
@@ -170,6 +171,19 @@ class OracleScene:
         out = np.zeros(queries.shape[0], result_dtype)
         lib().or_bsdf_batch(self.h, _p(queries), queries.shape[0], _p(out))
         return out
+
+    def render_capture(self, params, threads: int | None = None) -> dict:
+        """A capturing render of the whole frame: dict of beauty, beauty_a,
+        beauty_b, albedo_a, albedo_b, normal_a, normal_b ([3, H, W]) and
+        depth_a, depth_b ([H, W])."""
+        W, H = params.width, params.height
+        out = np.zeros((23, H, W), np.float32)
+        nt = threads or os.cpu_count() or 1
+        lib().or_render_capture(self.h, C.cast(C.pointer(params), C.c_void_p), _p(out), nt)
+        names = ["beauty", "beauty_a", "beauty_b", "albedo_a", "albedo_b", "normal_a", "normal_b"]
+        d = {n: out[3 * k:3 * k + 3] for k, n in enumerate(names)}
+        d["depth_a"], d["depth_b"] = out[21], out[22]
+        return d
 
     def render(self, params, threads: int | None = None, counters: bool = False):
         """Returns (planar [3,H,W] float32 film, counters dict or None)."""

@@ -1879,6 +1879,42 @@ static inline V3 sanitize(V3 c) {   // Renderer.cs:917-923
     return vmax(c, v3(0.0f));
 }
 
+// The AOV probe of the camera path being traced (Renderer.cs:755-815), one
+// per thread like the reference's [ThreadStatic] t_aovProbe; null while not
+// capturing, so every hook is one test.
+struct AovProbe {
+    bool pending = false, have_depth = false, camera = false;
+    float depth = -1.0f;
+    V3 weight{}, tent_albedo{}, tent_normal{}, albedo{}, normal{};
+    void reset() {
+        pending = true;
+        have_depth = false;
+        camera = true;
+        depth = -1.0f;
+        weight = v3(1.0f);
+        tent_albedo = v3(1.0f);
+        tent_normal = v3(0.0f);
+        albedo = v3(0.0f);
+        normal = v3(0.0f);
+    }
+    void commit() {
+        albedo = weight * tent_albedo;
+        normal = tent_normal;
+        pending = false;
+    }
+    void commit_as(V3 a, V3 n) {
+        albedo = weight * a;
+        normal = n;
+        pending = false;
+    }
+};
+static thread_local AovProbe* t_probe = nullptr;
+
+static inline V3 clamp01(V3 v) {   // Renderer.Clamp01: Vector3.Clamp(v, Zero, One)
+    return v3(std::fmin(std::fmax(v.x, 0.0f), 1.0f), std::fmin(std::fmax(v.y, 0.0f), 1.0f),
+              std::fmin(std::fmax(v.z, 0.0f), 1.0f));
+}
+
 struct Tracer {
     const Scene& sc;
     RenderCfg cfg;
@@ -2014,6 +2050,10 @@ struct Tracer {
     V3 shade_surface(const Ray& ray, HitRecord& rec, int depth, float prev_pdf, bool prev_delta, V3 cur_abs,
                      V3 beta, IorStack& iors) const {
         const Material& m = sc.mats[rec.material];
+        if (t_probe && t_probe->pending) {   // AOV tentative surface (:1051-1054): AovAlbedo is the colour
+            t_probe->tent_normal = rec.n;
+            t_probe->tent_albedo = clamp01(v3(m.d.base_color[0], m.d.base_color[1], m.d.base_color[2]));
+        }
         V3 emitted = v3(0.0f);
         if (m.is_emissive()) {   // Emissive.Emit (:86-90)
             if (rec.front) {
@@ -2041,6 +2081,10 @@ struct Tracer {
                 float a = std::fabs(ndwo);
                 if (a <= 0.0f || s.pdf <= 0.0f) return emitted + direct;
                 att = s.f * a / s.pdf;
+            }
+            if (t_probe && t_probe->pending) {   // AOV first-non-delta decision (:1271-1277)
+                if (s.is_delta) t_probe->weight = t_probe->weight * clamp01(s.f);
+                else t_probe->commit();
             }
             bool killed;
             V3 nb;
@@ -2073,6 +2117,7 @@ struct Tracer {
         V3 att, dir;
         int lobe2;
         if (bsdf.scatter_internal(ray.d, rec, att, dir, lobe2)) {
+            if (t_probe && t_probe->pending) t_probe->commit();   // (:1139-1145); Disney is not delta-scatter
             bool killed;
             V3 nb;
             V3 r = rr_and_recurse(att, beta, depth, emitted, direct, killed, nb);
@@ -2107,7 +2152,15 @@ struct Tracer {
         }
         bool hit = sc.world_hit(ray, kEps, kInf, rec);
         t_counting = saved;
+        if (t_probe) {   // AOV depth: the camera ray's first surface hit (:1657-1662)
+            if (t_probe->camera && hit && t_probe->pending && !t_probe->have_depth) {
+                t_probe->depth = rec.t * length(ray.d);
+                t_probe->have_depth = true;
+            }
+            t_probe->camera = false;
+        }
         if (!sc.has_medium) {
+            if (!hit && t_probe && t_probe->pending) t_probe->commit_as(v3(0.0f), v3(0.0f));   // black sky (:1849)
             V3 res = !hit ? v3(0.0f) : shade_surface(ray, rec, depth, prev_pdf, prev_delta, cur_abs, beta, iors);
             return beer_lambert(res, cur_abs, hit ? rec.t : INFINITY);
         }
@@ -2117,6 +2170,13 @@ struct Tracer {
         bool scattered = medium_sample(tmax, tmed, mb);
         if (scattered) {
             V3 p = ray.o + ray.d * tmed;
+            if (t_probe && t_probe->pending) {   // AOV at a medium scatter (:1716-1724)
+                if (!t_probe->have_depth) {
+                    t_probe->depth = tmed * length(ray.d);
+                    t_probe->have_depth = true;
+                }
+                t_probe->commit_as(v3(1.0f), v3(0.0f));
+            }
             V3 lnee = direct_lighting_medium(p, ray.d);
             V3 lind = v3(0.0f);
             V3 mthr = beta * mb;
@@ -2140,6 +2200,7 @@ struct Tracer {
             }
             return beer_lambert(mb * (lnee + lind), cur_abs, tmed);
         }
+        if (!hit && t_probe && t_probe->pending) t_probe->commit_as(v3(0.0f), v3(0.0f));   // black sky (:1849)
         V3 so = !hit ? v3(0.0f)
                      : mb * shade_surface(ray, rec, depth, prev_pdf, prev_delta, cur_abs, beta * mb, iors);
         return beer_lambert(so, cur_abs, hit ? rec.t : INFINITY);
@@ -2167,6 +2228,73 @@ static V3 render_pixel(const Scene& sc, const Tracer& tr, int i, int j, int widt
         cum += smp;
     }
     return cum;
+}
+
+// render_pixel with CaptureAccumulator (Renderer.cs:817-882): the even/odd
+// halves of the clamped samples and of the probe's features. Writes the
+// pixel's means into the 23-value record `o` (beauty, beauty A, beauty B,
+// albedo A, albedo B, normal A, normal B, depth A, depth B).
+static void render_pixel_capture(const Scene& sc, const Tracer& tr, int i, int j, int width, int height, int spp,
+                                 int spp_offset, float* o) {
+    V3 cum = v3(0.0f), sa = v3(0.0f), sb = v3(0.0f), aa = v3(0.0f), ab = v3(0.0f), na = v3(0.0f), nb = v3(0.0f);
+    float da = 0.0f, db = 0.0f;
+    int ca = 0, cb = 0;
+    AovProbe probe;
+    t_probe = &probe;
+    uint32_t seed = (uint32_t)(i * 73856093) ^ (uint32_t)(j * 19349663);
+    for (int s = 0; s < spp; s++) {
+        begin_pixel_sample(seed, (uint32_t)(spp_offset + s));
+        float ju = random_float();
+        float jv = random_float();
+        float u = ((float)i + ju) / (float)width;
+        float v = ((float)(height - j - 1) + jv) / (float)height;
+        V3 target = sc.cam_llc + u * sc.cam_h + v * sc.cam_v;
+        Ray ray(sc.cam_origin, target - sc.cam_origin);
+        IorStack iors;
+        probe.reset();
+        V3 smp = tr.trace(ray, tr.cfg.max_depth, 0.0f, true, iors, v3(0.0f), v3(1.0f));
+        end_pixel_sample();
+        smp = tr.clamp_radiance(smp);
+        cum += smp;
+        if (probe.pending) probe.commit();
+        if ((s & 1) == 0) {
+            sa += smp;
+            aa += probe.albedo;
+            na += probe.normal;
+            if (probe.have_depth) {
+                da += probe.depth;
+                ca++;
+            }
+        } else {
+            sb += smp;
+            ab += probe.albedo;
+            nb += probe.normal;
+            if (probe.have_depth) {
+                db += probe.depth;
+                cb++;
+            }
+        }
+    }
+    t_probe = nullptr;
+    int n_a = (spp + 1) / 2, n_b = spp / 2;
+    auto put3 = [&](int at, V3 c) {
+        o[at] = c.x;
+        o[at + 1] = c.y;
+        o[at + 2] = c.z;
+    };
+    put3(0, cum / (float)spp);
+    V3 ma = sa / (float)n_a;
+    put3(3, ma);
+    put3(6, n_b > 0 ? sb / (float)n_b : ma);
+    V3 a2 = aa / (float)n_a;
+    put3(9, a2);
+    put3(12, n_b > 0 ? ab / (float)n_b : a2);
+    V3 n2 = na / (float)n_a;
+    put3(15, n2);
+    put3(18, n_b > 0 ? nb / (float)n_b : n2);
+    float dA = ca > 0 ? da / (float)ca : -1.0f;
+    o[21] = dA;
+    o[22] = n_b > 0 ? (cb > 0 ? db / (float)cb : -1.0f) : dA;
 }
 
 }  // namespace oracle
@@ -2597,6 +2725,46 @@ int or_bsdf_batch(void* s, const RtBsdfQuery* q, int64_t n, RtBsdfResult* out) {
 // 16x16 tiles (Renderer.cs:530-585). out: planar 3*W*H (only the window is
 // written). counters[7]: node visits, tri tests, other tests, closest rays,
 // shadow rays, segments, samples.
+// A capturing render (Renderer.Render with RenderCaptureOptions.Full) of the
+// whole frame: out holds 23 planes of W*H floats, in the order of
+// render_pixel_capture's record.
+int or_render_capture(void* s, const RtRenderParams* p, float* out, int32_t threads) {
+    Scene* sc = static_cast<Scene*>(s);
+    int W = p->width, H = p->height;
+    build_camera(*sc, sc->cam_desc, (float)W / (float)H);
+    Tracer tr{*sc, {}};
+    tr.cfg.max_depth = p->max_depth;
+    tr.cfg.max_radiance = p->max_sample_radiance > 0.0f ? p->max_sample_radiance : 10.0f;
+    float icf = p->indirect_clamp_factor >= 0.0f ? p->indirect_clamp_factor : 0.25f;
+    tr.cfg.indirect_max = tr.cfg.max_radiance * std::fmax(0.0f, icf);
+    tr.cfg.mis_power = p->mis_heuristic == RT_MIS_POWER;
+    tr.cfg.rr_min_bounces = p->rr_min_bounces >= 0 ? p->rr_min_bounces : sc->rr_min_bounces;
+    tr.cfg.rr_min_survival = p->rr_min_bounces >= 0 ? p->rr_min_survival : sc->rr_min_survival;
+    const int T = 16;
+    int tx = (W + T - 1) / T, ty = (H + T - 1) / T;
+    std::atomic<int> next(0);
+    size_t plane = (size_t)W * (size_t)H;
+    auto worker = [&]() {
+        for (;;) {
+            int tile = next.fetch_add(1);
+            if (tile >= tx * ty) break;
+            int px0 = (tile % tx) * T, py0 = (tile / tx) * T;
+            for (int j = py0; j < std::min(py0 + T, H); j++)
+                for (int i = px0; i < std::min(px0 + T, W); i++) {
+                    float rec[23];
+                    render_pixel_capture(*sc, tr, i, j, W, H, p->spp, p->spp_offset, rec);
+                    for (int k = 0; k < 23; k++) out[(size_t)k * plane + (size_t)j * W + i] = rec[k];
+                }
+        }
+    };
+    int nt = std::max(1, (int)threads);
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
 int or_render(void* s, const RtRenderParams* p, float* out, int32_t threads, uint64_t* counters) {
     Scene* sc = static_cast<Scene*>(s);
     int W = p->width, H = p->height;
