@@ -58,7 +58,7 @@ class RtLightDesc(C.Structure):
     _fields_ = [("type", C.c_int32), ("shadow_samples", C.c_int32), ("proxy_material", C.c_int32),
                 ("pad", C.c_int32), ("corner", F3), ("u", F3), ("v", F3), ("color", F3),
                 ("intensity", C.c_float), ("soft_radius", C.c_float), ("direction", F3),
-                ("angular_radius_deg", C.c_float)]
+                ("angular_radius_deg", C.c_float), ("center", F3), ("radius", C.c_float)]
 
 
 class RtCameraDesc(C.Structure):
@@ -200,6 +200,9 @@ class PackedWorld:
             if l["type"] == scenes.LIGHT_AREA:
                 d.corner, d.u, d.v = _f3(l["corner"]), _f3(l["u"]), _f3(l["v"])
                 d.soft_radius = float(l.get("soft_radius", 0.0))
+            elif l["type"] == scenes.LIGHT_SPHERE:
+                d.center = _f3(l["center"])
+                d.radius = float(l["radius"])
             else:
                 d.direction = _f3(l["direction"])
                 d.angular_radius_deg = float(l.get("angular_radius_deg", 0.0))

@@ -518,7 +518,8 @@ struct AdjointSink {
         V3 gx = gain(ps, to_la) * sh_x;
         if (is_zero(gx)) return;
         const Light& l = s->lights[li];
-        if ((l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH) && l.emissive_material >= 0) {
+        if ((l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH || l.type == LIGHT_GEOM_SPHERE) &&
+            l.emissive_material >= 0) {
             int b = l.emissive_material * kAdjPerMat;
             if (l.emission.x > 0.0f) add(b + 0, gx.x / l.emission.x);
             if (l.emission.y > 0.0f) add(b + 1, gx.y / l.emission.y);

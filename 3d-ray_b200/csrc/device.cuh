@@ -1255,6 +1255,38 @@ struct LightSample {
     float ray_tmax;
 };
 
+// A direction in the cone of half-angle acos(cos_max) around w, uniform in
+// solid angle (Sphere.SampleSolidAngleCore, Sphere.cs:160-169; SphereLight
+// :87-96), through LocalToWorld (Sphere.cs:230-246).
+RT_D V3 cone_dir(V3 w, float cos_max, float xi1, float xi2) {
+    float ct = 1.0f - xi1 * (1.0f - cos_max);
+    float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+    float phi = 2.0f * kPi * xi2;
+    V3 loc = v3(st * cosf(phi), st * sinf(phi), ct);
+    V3 uu, vv;
+    tangent_frame(w, uu, vv);
+    V3 res = loc.x * uu + loc.y * vv + loc.z * w;
+    float l2 = length_sq(res);
+    return l2 > 1e-8f ? res / sqrtf(l2) : w;
+}
+
+// Sphere.SolidAnglePdf (Sphere.cs:205-226) and SphereLight.PdfSolidAngle
+// (SphereLight.cs:179-200), the same function of the cone.
+RT_D float sphere_cone_pdf(V3 center, float radius, V3 p, V3 wi) {
+    V3 tc = center - p;
+    float d2 = length_sq(tc);
+    float r2 = radius * radius;
+    if (d2 <= r2) return 1.0f / (4.0f * kPi);   // observer inside: uniform sphere
+    float cmax = sqrtf(fmaxf(0.0f, 1.0f - r2 / d2));
+    float wl = length(wi);
+    if (wl < kEps) return 0.0f;
+    V3 wd = tc / sqrtf(d2);
+    float ct = dot(wi, wd) / wl;
+    if (ct < cmax) return 0.0f;
+    float sa = 2.0f * kPi * (1.0f - cmax);
+    return sa > kEps ? 1.0f / sa : 0.0f;
+}
+
 // Draws the light sample (all RNG draws happen here, before any shadow test):
 // GeometryLight.ComputeAreaSample (GeometryLight.cs:149-190),
 // AreaLight.IlluminateAndTestStratified (AreaLight.cs:129-178),
@@ -1330,6 +1362,115 @@ RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, i
         r.color = l.emission * atten;
         return r;
     }
+    if (l.type == LIGHT_GEOM_SPHERE) {   // GeometryLight.ComputeSolidAngleSample (:202-238)
+        int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
+        float xi1 = ((float)su + rng.next()) * l.inv_sqrt;   // Sphere.SampleSolidAngleStratified
+        float xi2 = ((float)sv + rng.next()) * l.inv_sqrt;
+        V3 tc = l.center - p;
+        float d2c = length_sq(tc);
+        float r2 = l.radius * l.radius;
+        V3 sp, ln;
+        float pdf;
+        if (d2c <= r2) {   // observer inside: uniform sphere (two more draws)
+            V3 pu = random_unit_vector(rng);
+            sp = l.center + pu * l.radius;
+            ln = pu;
+            pdf = 1.0f / (4.0f * kPi);
+        } else {
+            float dc = sqrtf(d2c);
+            V3 wd = tc / dc;
+            float cmax = sqrtf(fmaxf(0.0f, 1.0f - r2 / d2c));
+            V3 dw = cone_dir(wd, cmax, xi1, xi2);
+            V3 oc = p - l.center;
+            float b = dot(oc, dw);
+            float c = length_sq(oc) - r2;
+            float disc = b * b - c;
+            float t;
+            if (disc <= 0.0f) {
+                t = -b;   // tangent ray: the foot of the perpendicular
+            } else {
+                float sq = sqrtf(disc);
+                t = -b - sq;
+                if (t < kEps) t = -b + sq;
+            }
+            sp = p + t * dw;
+            ln = normalize(sp - l.center);
+            float sa = 2.0f * kPi * (1.0f - cmax);
+            pdf = sa > kEps ? 1.0f / sa : 0.0f;
+        }
+        if (pdf <= 0.0f) {
+            r.occluded = 1;
+            r.dir = v3(0.0f, 1.0f, 0.0f);
+            return r;
+        }
+        V3 tl = sp - p;
+        float d2 = length_sq(tl);
+        if (d2 < kEps * kEps) {
+            r.occluded = 1;
+            r.dir = v3(0.0f, 1.0f, 0.0f);
+            return r;
+        }
+        float dist = sqrtf(d2);
+        V3 dir = tl / dist;
+        r.dir = dir;
+        r.dist = dist;
+        float cl = fmaxf(0.0f, dot(-dir, ln));
+        if (cl <= 0.0f) return r;   // not in shadow, zero colour
+        V3 so = offset_origin(p, sn);
+        r.has_ray = 1;
+        r.ray_o = so;
+        r.ray_tmax = length(sp - so) - kEps;
+        float atten = 1.0f / (pdf * (float)l.shadow_samples);
+        r.color = l.emission * atten;
+        return r;
+    }
+    if (l.type == LIGHT_SPHERE) {   // SphereLight.IlluminateAndTestStratified (:72-141)
+        V3 tc = l.center - p;
+        float d2c = length_sq(tc);
+        if (d2c < kEps * kEps) {
+            r.occluded = 1;
+            r.dir = v3(0.0f, 1.0f, 0.0f);
+            return r;
+        }
+        float dc = sqrtf(d2c);
+        V3 wd = tc / dc;
+        float s2 = l.radius * l.radius / d2c;
+        float cmax = s2 >= 1.0f ? -1.0f : sqrtf(1.0f - s2);
+        int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
+        float xi1 = ((float)su + rng.next()) * l.inv_sqrt;
+        float xi2 = ((float)sv + rng.next()) * l.inv_sqrt;
+        V3 dw = cone_dir(wd, cmax, xi1, xi2);
+        V3 oc = p - l.center;
+        float b = dot(oc, dw);
+        float c = length_sq(oc) - l.radius * l.radius;
+        float disc = b * b - c;
+        r.dir = dw;
+        if (disc < 0.0f) {
+            r.occluded = 1;
+            r.dist = length(l.center + normalize(dw) * l.radius - p);
+            return r;
+        }
+        float sq = sqrtf(disc);
+        float t = -b - sq;
+        if (t < kEps) t = -b + sq;
+        if (t < kEps) {
+            r.occluded = 1;
+            return r;
+        }
+        V3 sp = p + t * dw;
+        r.dist = t;
+        V3 ln = (sp - l.center) / l.radius;
+        float cl = fmaxf(0.0f, dot(-dw, ln));
+        if (cl <= 0.0f) return r;   // not in shadow, zero colour
+        V3 so = offset_origin(p, sn);
+        r.has_ray = 1;
+        r.ray_o = so;
+        r.ray_tmax = length(sp - so) - kEps;
+        float sa = 2.0f * kPi * (1.0f - cmax);
+        float atten = l.intensity * sa / (float)l.shadow_samples;
+        r.color = l.color * atten;
+        return r;
+    }
     if (l.type == LIGHT_AREA) {
         int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
         float ru = ((float)su + rng.next()) * l.inv_sqrt;
@@ -1402,6 +1543,7 @@ RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
         if (l.rep_area < 1e-12f) return 0.0f;
         return d2 / (l.rep_area * cl);
     }
+    if (l.type == LIGHT_GEOM_SPHERE || l.type == LIGHT_SPHERE) return sphere_cone_pdf(l.center, l.radius, p, wi);
     if (l.type == LIGHT_GEOM_MESH) {   // ray cast against the emitter mesh alone
         Hit h;
         int err = 0;

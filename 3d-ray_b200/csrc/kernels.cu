@@ -34,7 +34,7 @@ int fail(int code, const std::string& msg) {
 
 static_assert(sizeof(RtMaterialDesc) == 120, "ABI layout");
 static_assert(sizeof(RtEntityDesc) == 80, "ABI layout");
-static_assert(sizeof(RtLightDesc) == 88, "ABI layout");
+static_assert(sizeof(RtLightDesc) == 104, "ABI layout");
 static_assert(sizeof(RtCameraDesc) == 48, "ABI layout");
 static_assert(sizeof(RtMediumDesc) == 36, "ABI layout");
 static_assert(sizeof(RtRenderParams) == 104, "ABI layout");

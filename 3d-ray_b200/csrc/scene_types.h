@@ -84,7 +84,14 @@ struct Material {
     float alpha_iso, e_avg;            // sqrt(ax*ay), E_avg(alpha_iso)
 };
 
-enum : int { LIGHT_GEOM_QUAD = 0, LIGHT_GEOM_MESH = 1, LIGHT_AREA = 3, LIGHT_DIRECTIONAL = 4 };
+enum : int {
+    LIGHT_GEOM_QUAD = 0,
+    LIGHT_GEOM_MESH = 1,
+    LIGHT_GEOM_SPHERE = 2,   // an emissive sphere: GeometryLight with cone sampling
+    LIGHT_AREA = 3,
+    LIGHT_DIRECTIONAL = 4,
+    LIGHT_SPHERE = 5,        // SphereLight
+};
 
 struct Light {
     int type;
@@ -104,6 +111,8 @@ struct Light {
     float intensity, area, soft_radius;
     V3 direction;
     float angular_radius, cos_angular, solid_angle;
+    V3 center;           // sphere lights (geometry or SphereLight)
+    float radius;
 };
 
 // Emissive-mesh triangles in source order with the area CDF (Mesh.cs:98-107).

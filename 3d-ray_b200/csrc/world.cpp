@@ -206,9 +206,10 @@ void build_mesh(const float* tv, int64_t count, MeshBuild& mb) {
 }
 
 float light_power(const Light& l, const Box& bounds) {
-    if (l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH)   // GeometryLight.cs:116-120
+    if (l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH || l.type == LIGHT_GEOM_SPHERE)   // GeometryLight.cs:116-120
         return kPi * l.rep_area * luminance(l.emission);
     if (l.type == LIGHT_AREA) return kPi * l.area * luminance(l.color) * l.intensity;   // AreaLight.cs:111
+    if (l.type == LIGHT_SPHERE) return 4.0f * kPi * luminance(l.color) * l.intensity;   // SphereLight.cs:79-80
     V3 ext = bounds.mx - bounds.mn;                                                     // DirectionalLight.cs:82-88
     float radius = 0.5f * length(ext);
     float cs = kPi * radius * radius;
@@ -794,6 +795,19 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             l.sqrt_samples = (int)std::ceil(std::sqrt((float)l.shadow_samples));
             l.inv_sqrt = 1.0f / (float)l.sqrt_samples;
             l.is_delta = disc ? 0 : 1;
+        } else if (d.type == RT_LIGHT_SPHERE) {   // SphereLight.cs:54-68
+            l.type = LIGHT_SPHERE;
+            l.center = v3(d.center[0], d.center[1], d.center[2]);
+            l.radius = std::fmax(d.radius, kEps);
+            l.shadow_samples = d.shadow_samples > 0 ? d.shadow_samples : 4;
+            l.sqrt_samples = (int)std::ceil(std::sqrt((float)l.shadow_samples));
+            l.inv_sqrt = 1.0f / (float)l.sqrt_samples;
+            l.is_delta = 0;
+            l.emissive_material = d.proxy_material;
+            if (d.proxy_material >= w->num_materials) {
+                err = "sphere light proxy material out of range";
+                return RT_ERR_INVALID_ARG;
+            }
         } else {
             err = "light " + std::to_string(i) + ": unsupported type";
             return RT_ERR_UNSUPPORTED;
@@ -849,20 +863,27 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
                 sc.light_tris.push_back(lt);
             }
             l.rep_area = sum;
-        } else {
-            err = "entity " + std::to_string(e) + ": emissive spheres (cone-sampled lights) are outside the GPU path";
-            return RT_ERR_UNSUPPORTED;
+        } else {   // a sphere: GeometryLight's cone sampling (ISolidAngleSamplable, GeometryLight.cs:94)
+            l.type = LIGHT_GEOM_SPHERE;
+            const SphereData& sp = sc.spheres[sc.entities[e].index];
+            l.center = sp.c;
+            l.radius = sp.r;
+            l.rep_area = 4.0f * kPi * sp.r * sp.r;   // Sphere.SurfaceArea (Sphere.cs:78)
         }
         sc.lights.push_back(l);
     }
     // --- emitter -> light map (Renderer.cs:409-425)
     sc.emitter_light.assign((size_t)w->num_materials, -1);
-    for (size_t i = 0; i < sc.lights.size(); i++)
-        if (sc.lights[i].type == LIGHT_GEOM_QUAD || sc.lights[i].type == LIGHT_GEOM_MESH)
+    for (size_t i = 0; i < sc.lights.size(); i++) {
+        int t = sc.lights[i].type;
+        if (t == LIGHT_GEOM_QUAD || t == LIGHT_GEOM_MESH || t == LIGHT_GEOM_SPHERE)
             sc.emitter_light[sc.lights[i].emissive_material] = (int)i;
-    for (size_t i = 0; i < sc.lights.size(); i++)
-        if (sc.lights[i].type == LIGHT_AREA && sc.lights[i].emissive_material >= 0)
+    }
+    for (size_t i = 0; i < sc.lights.size(); i++) {   // then every light's proxy, in list order
+        int t = sc.lights[i].type;
+        if ((t == LIGHT_AREA || t == LIGHT_SPHERE) && sc.lights[i].emissive_material >= 0)
             sc.emitter_light[sc.lights[i].emissive_material] = (int)i;
+    }
     // --- RR classifier (Renderer.cs:361-378; ComputeFiniteSceneBounds :475-500)
     Box bounds;
     {

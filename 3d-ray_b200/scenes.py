@@ -36,6 +36,7 @@ ENT_SPHERE = 1
 ENT_MESH = 2
 LIGHT_AREA = 0
 LIGHT_DIRECTIONAL = 1
+LIGHT_SPHERE = 2
 
 DEFAULT_SCENE_SEED = 0x3D7A1
 DEFAULT_REQUEST_SEED = 0xC0FFEE
@@ -90,6 +91,16 @@ class World:
     def add_sphere(self, center, radius, material: int, name=""):
         self.entities.append(dict(kind=ENT_SPHERE, material=material, center=tuple(map(float, center)),
                                   radius=float(radius), name=name))
+
+    def add_sphere_light(self, center, radius, color, intensity, shadow_samples=4, name=""):
+        """A SphereLight with its visible emissive proxy sphere, appended to the
+        objects as SceneLoader.CreateSphereLight does (SceneLoader.cs:3592-3634)."""
+        proxy = self.add_material(f"{name or 'sphere_light'}_proxy",
+                                  emissive(color, intensity, is_light_proxy=True))
+        self.add_sphere(center, radius, proxy, name=f"{name or 'sphere_light'}_proxy")
+        self.lights.append(dict(type=LIGHT_SPHERE, center=tuple(map(float, center)), radius=float(radius),
+                                color=tuple(map(float, color)), intensity=float(intensity),
+                                shadow_samples=int(shadow_samples), proxy_material=proxy))
 
     def add_mesh(self, tris: np.ndarray, material: int, name="", normals=None, uvs=None, path=None):
         """A mesh entity of world-space triangles [n, 9]. With `normals`
@@ -292,6 +303,21 @@ def cornell_smooth(shadow_samples: int = 1) -> World:
     return w
 
 
+def cornell_spheres(shadow_samples: int = 1) -> World:
+    """Spherical emitters in the Cornell box: an emissive sphere (a
+    GeometryLight sampled in its solid-angle cone) beside the ceiling quad,
+    and a SphereLight with its proxy, both seen directly and through a
+    metallic sphere."""
+    w = cornell(shadow_samples, tall_box=False)
+    w.name = "cornell-spheres"
+    glow = w.add_material("glow_sphere", emissive((8.0, 6.0, 2.0), 1.0))
+    w.add_sphere((140, 420, 350), 40.0, glow, name="glow_sphere")
+    metal = w.add_material("metal", disney((0.9, 0.9, 0.9), roughness=0.25, metallic=1.0))
+    w.add_sphere((380, 100, 380), 100.0, metal, name="metal_sphere")
+    w.add_sphere_light((420, 330, 200), 25.0, (1.0, 0.8, 0.6), 12.0, shadow_samples=4, name="bulb")
+    return w
+
+
 def cornell_volume(shadow_samples: int = 1, density: float = 1.0) -> World:
     """C5: homogeneous medium (sigma_t 0.02 per unit times `density`, albedo
     0.8, HG g 0.6) filling the box, and a dielectric sphere (IOR 1.5,
@@ -447,6 +473,10 @@ def write_yaml(world: World, out_dir: str, name: str | None = None) -> str:
     for l in world.lights:
         if l["type"] == LIGHT_AREA:
             lights.append(dict(type="area", corner=list(l["corner"]), u=list(l["u"]), v=list(l["v"]),
+                               color=list(l["color"]), intensity=l["intensity"],
+                               shadow_samples=l["shadow_samples"]))
+        elif l["type"] == LIGHT_SPHERE:
+            lights.append(dict(type="sphere", position=list(l["center"]), radius=l["radius"],
                                color=list(l["color"]), intensity=l["intensity"],
                                shadow_samples=l["shadow_samples"]))
         else:

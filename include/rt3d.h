@@ -106,6 +106,7 @@ typedef struct RtEntityDesc {
 
 #define RT_LIGHT_AREA        0   /* Lights/AreaLight.cs        */
 #define RT_LIGHT_DIRECTIONAL 1   /* Lights/DirectionalLight.cs */
+#define RT_LIGHT_SPHERE      2   /* Lights/SphereLight.cs      */
 
 /* Explicit lights in YAML order. Geometry lights (Lights/GeometryLight.cs) are
  * derived by the library from emissive, non-proxy entities in entity order and
@@ -114,7 +115,7 @@ typedef struct RtEntityDesc {
 typedef struct RtLightDesc {
     int32_t type;
     int32_t shadow_samples;       /* <= 0: the light type's default */
-    int32_t proxy_material;       /* area light: material index of its proxy, or -1 */
+    int32_t proxy_material;       /* area / sphere light: material index of its proxy, or -1 */
     int32_t pad;
     float corner[3], u[3], v[3];  /* area light parallelogram */
     float color[3];
@@ -122,6 +123,8 @@ typedef struct RtLightDesc {
     float soft_radius;
     float direction[3];           /* directional light travel direction */
     float angular_radius_deg;     /* directional disc; 0 = delta light */
+    float center[3];              /* sphere light */
+    float radius;
 } RtLightDesc;
 
 /* Camera/Camera.cs:26-51 (pinhole when aperture == 0). */

@@ -1537,7 +1537,8 @@ struct Scene;
 static V3 shadow_transmittance(const Scene& sc, const Ray& ray, float tmin, float tmax, int max_bounces = 8);
 
 struct Light {
-    int type = 0;   // 0 geometry-quad, 1 geometry-mesh, 2 geometry-triangle, 3 area, 4 directional
+    int type = 0;   // 0 geometry-quad, 1 geometry-mesh, 2 geometry-triangle, 3 area, 4 directional,
+                    // 5 geometry-sphere (cone sampled), 6 sphere light
     int shadow_samples = 1;
     int sqrt_samples = 1;
     float inv_sqrt = 1.0f;
@@ -1553,6 +1554,8 @@ struct Light {
     float angular_radius = 0.0f, cos_angular = 1.0f, solid_angle = 0.0f;
     V3 rep_point{};
     float rep_area = 0.0f;
+    V3 center{};   // sphere lights
+    float radius = 0.0f;
 };
 
 struct Scene {
@@ -1584,7 +1587,8 @@ struct Scene {
 };
 
 static float light_approx_power(const Light& l, const AABB& bounds, const Scene& sc) {
-    if (l.type <= 2) {   // GeometryLight.ApproximatePower (:116-120)
+    if (l.type == 6) return 4.0f * kPi * luminance(l.color) * l.intensity;   // SphereLight.ApproximatePower (:79-80)
+    if (l.type <= 2 || l.type == 5) {   // GeometryLight.ApproximatePower (:116-120)
         const Material& m = sc.mats[l.emissive_material];
         V3 em = v3(m.d.base_color[0], m.d.base_color[1], m.d.base_color[2]) * std::fmax(m.d.intensity, 0.0f);
         return kPi * l.rep_area * luminance(em);
@@ -1596,9 +1600,143 @@ static float light_approx_power(const Light& l, const AABB& bounds, const Scene&
     return luminance(l.color) * l.intensity * cross_section;
 }
 
+// Sphere.LocalToWorld (Sphere.cs:230-246, the same frame as SphereLight's and
+// DirectionalLight's) of a cone direction: cosTheta = 1 - xi1 (1 - cosMax),
+// phi = 2 pi xi2 (Sphere.cs:160-169, SphereLight.cs:87-96).
+static V3 cone_dir(V3 w, float cos_max, float xi1, float xi2) {
+    float ct = 1.0f - xi1 * (1.0f - cos_max);
+    float st = std::sqrt(std::fmax(0.0f, 1.0f - ct * ct));
+    float phi = 2.0f * kPi * xi2;
+    V3 loc = v3(st * std::cos(phi), st * std::sin(phi), ct);
+    V3 uu, vv;
+    if (w.z < -0.999f) {
+        uu = v3(0, -1, 0);
+        vv = v3(-1, 0, 0);
+    } else {
+        float a = 1.0f / (1.0f + w.z);
+        float b = -w.x * w.y * a;
+        uu = v3(1.0f - w.x * w.x * a, b, -w.x);
+        vv = v3(b, 1.0f - w.y * w.y * a, -w.y);
+    }
+    V3 res = loc.x * uu + loc.y * vv + loc.z * w;
+    float l2 = length_sq(res);
+    return l2 > 1e-8f ? res / std::sqrt(l2) : w;
+}
+
+// Sphere.SolidAnglePdf (:205-226) = SphereLight.PdfSolidAngle (:179-200).
+static float sphere_cone_pdf(V3 center, float radius, V3 p, V3 wi) {
+    V3 tc = center - p;
+    float d2 = length_sq(tc);
+    float r2 = radius * radius;
+    if (d2 <= r2) return 1.0f / (4.0f * kPi);
+    float cmax = std::sqrt(std::fmax(0.0f, 1.0f - r2 / d2));
+    float wl = length(wi);
+    if (wl < kEps) return 0.0f;
+    float dist = std::sqrt(d2);
+    V3 wd = tc / dist;
+    float ct = dot(wi, wd) / wl;
+    if (ct < cmax) return 0.0f;
+    float sa = 2.0f * kPi * (1.0f - cmax);
+    return sa > kEps ? 1.0f / sa : 0.0f;
+}
+
 // GeometryLight.ComputeAreaSample (:149-190) for quads / triangles / meshes,
+// GeometryLight.ComputeSolidAngleSample (:202-238) for spheres,
+// SphereLight.IlluminateAndTestStratified (:72-141),
 // AreaLight.IlluminateAndTestStratified (:129-178), DirectionalLight (:102-160).
 static LightSample illuminate(const Scene& sc, const Light& l, V3 hit_p, V3 surf_n, int s) {
+    if (l.type == 5) {
+        int su = s % l.sqrt_samples, sv = s / l.sqrt_samples;   // Sphere.SampleSolidAngleStratified
+        float inv = 1.0f / (float)l.sqrt_samples;
+        float xi1 = ((float)su + random_float()) * inv;
+        float xi2 = ((float)sv + random_float()) * inv;
+        V3 tc = l.center - hit_p;   // Sphere.SampleSolidAngleCore (:137-200)
+        float dist_sq = length_sq(tc);
+        float r_sq = l.radius * l.radius;
+        V3 sp, nrm;
+        float pdf;
+        if (dist_sq <= r_sq) {
+            V3 pu = random_unit_vector();
+            sp = l.center + pu * l.radius;
+            nrm = pu;
+            pdf = 1.0f / (4.0f * kPi);
+        } else {
+            float dist = std::sqrt(dist_sq);
+            V3 wd = tc / dist;
+            float cmax = std::sqrt(std::fmax(0.0f, 1.0f - r_sq / dist_sq));
+            V3 dw = cone_dir(wd, cmax, xi1, xi2);
+            V3 oc = hit_p - l.center;
+            float b = dot(oc, dw);
+            float c = length_sq(oc) - r_sq;
+            float disc = b * b - c;
+            float t;
+            if (disc <= 0.0f) {
+                t = -b;
+            } else {
+                float sq = std::sqrt(disc);
+                t = -b - sq;
+                if (t < kEps) t = -b + sq;
+            }
+            sp = hit_p + t * dw;
+            nrm = normalize(sp - l.center);
+            float sa = 2.0f * kPi * (1.0f - cmax);
+            pdf = sa > kEps ? 1.0f / sa : 0.0f;
+        }
+        if (pdf <= 0.0f) return {true, v3(0.0f), v3(0, 1, 0), 0.0f};
+        V3 to_l = sp - hit_p;
+        float d2 = length_sq(to_l);
+        if (d2 < kEps * kEps) return {true, v3(0.0f), v3(0, 1, 0), 0.0f};
+        float dist = std::sqrt(d2);
+        V3 dir = to_l / dist;
+        float cos_l = std::fmax(0.0f, dot(-dir, nrm));
+        if (cos_l <= 0.0f) return {false, v3(0.0f), dir, dist};
+        V3 so = offset_origin(hit_p, surf_n);
+        Ray sr(so, dir);
+        float tmax = length(sp - so) - kEps;
+        V3 tr = shadow_transmittance(sc, sr, kEps, tmax);
+        if (near_zero(tr)) return {true, v3(0.0f), dir, dist};
+        const Material& m = sc.mats[l.emissive_material];
+        V3 em = v3(m.d.base_color[0], m.d.base_color[1], m.d.base_color[2]) * std::fmax(m.d.intensity, 0.0f);
+        float atten = 1.0f / (pdf * (float)l.shadow_samples);
+        return {false, em * atten * tr, dir, dist};
+    }
+    if (l.type == 6) {
+        V3 tc = l.center - hit_p;
+        float dist_sq = length_sq(tc);
+        if (dist_sq < kEps * kEps) return {true, v3(0.0f), v3(0, 1, 0), 0.0f};
+        float dist = std::sqrt(dist_sq);
+        V3 wd = tc / dist;
+        float s2 = l.radius * l.radius / dist_sq;
+        float cmax = s2 >= 1.0f ? -1.0f : std::sqrt(1.0f - s2);
+        int su = s % l.sqrt_samples, sv = s / l.sqrt_samples;
+        float xi1 = ((float)su + random_float()) * l.inv_sqrt;
+        float xi2 = ((float)sv + random_float()) * l.inv_sqrt;
+        V3 dw = cone_dir(wd, cmax, xi1, xi2);
+        V3 oc = hit_p - l.center;
+        float b = dot(oc, dw);
+        float c = length_sq(oc) - l.radius * l.radius;
+        float disc = b * b - c;
+        if (disc < 0.0f) {
+            V3 cp = l.center + normalize(dw) * l.radius;
+            return {true, v3(0.0f), dw, length(cp - hit_p)};
+        }
+        float sq = std::sqrt(disc);
+        float t = -b - sq;
+        if (t < kEps) t = -b + sq;
+        if (t < kEps) return {true, v3(0.0f), dw, 0.0f};
+        V3 sp = hit_p + t * dw;
+        V3 ln = (sp - l.center) / l.radius;
+        float cos_l = std::fmax(0.0f, dot(-dw, ln));
+        if (cos_l <= 0.0f) return {false, v3(0.0f), dw, t};
+        V3 so = offset_origin(hit_p, surf_n);
+        Ray sr(so, dw);
+        float tmax = length(sp - so) - kEps;
+        V3 tr = shadow_transmittance(sc, sr, kEps, tmax);
+        if (near_zero(tr)) return {true, v3(0.0f), dw, t};
+        float sa = 2.0f * kPi * (1.0f - cmax);
+        float atten = l.intensity * sa / (float)l.shadow_samples;
+        return {false, l.color * atten * tr, dw, t};
+    }
     if (l.type <= 2) {
         V3 sp, ln;
         float uvx = 0.5f, uvy = 0.5f, area;
@@ -1703,6 +1841,7 @@ static LightSample illuminate(const Scene& sc, const Light& l, V3 hit_p, V3 surf
 
 // ILight.PdfSolidAngle implementations.
 static float light_pdf(const Light& l, V3 p, V3 wi) {
+    if (l.type == 5 || l.type == 6) return sphere_cone_pdf(l.center, l.radius, p, wi);
     if (l.type == 0 || l.type == 1) {   // GeometryLight.PdfSolidAngle area fallback (:254-279)
         Ray r(p, wi);
         HitRecord rec;
@@ -2467,6 +2606,17 @@ int or_scene_create(const RtWorldDesc* w, void** out) {
             l.sqrt_samples = (int)std::ceil(std::sqrt((float)l.shadow_samples));
             l.inv_sqrt = 1.0f / (float)l.sqrt_samples;
             l.is_delta = !disc;
+        } else if (ld.type == RT_LIGHT_SPHERE) {   // SphereLight.cs:54-68
+            l.type = 6;
+            l.center = v3(ld.center[0], ld.center[1], ld.center[2]);
+            l.radius = std::fmax(ld.radius, kEps);
+            l.color = v3(ld.color[0], ld.color[1], ld.color[2]);
+            l.intensity = ld.intensity;
+            l.shadow_samples = ld.shadow_samples > 0 ? ld.shadow_samples : 4;
+            l.sqrt_samples = (int)std::ceil(std::sqrt((float)l.shadow_samples));
+            l.inv_sqrt = 1.0f / (float)l.sqrt_samples;
+            l.is_delta = false;
+            l.emissive_material = ld.proxy_material;
         } else {
             std::snprintf(g_err, sizeof(g_err), "unsupported light type %d", ld.type);
             return -6;
@@ -2506,17 +2656,21 @@ int or_scene_create(const RtWorldDesc* w, void** out) {
             l.type = 1;
             l.mesh = static_cast<const Mesh*>(sc->entity_ptr[e]);
             l.rep_area = l.mesh->total_area;
-        } else {
-            std::snprintf(g_err, sizeof(g_err), "emissive spheres (cone-sampled geometry lights) are not restated");
-            return -6;
+        } else {   // a sphere: cone sampling (ISolidAngleSamplable)
+            l.type = 5;
+            const Sphere* sp = static_cast<const Sphere*>(sc->entity_ptr[e]);
+            l.center = sp->c;
+            l.radius = sp->r;
+            l.rep_area = 4.0f * kPi * sp->r * sp->r;   // Sphere.SurfaceArea
         }
         sc->lights.push_back(l);
     }
     // Emitter -> light map (Renderer.cs:409-425): geometry lights first, then proxies.
     for (size_t li = 0; li < sc->lights.size(); li++)
-        if (sc->lights[li].type <= 2) sc->emitter_to_light[sc->lights[li].emissive_material] = (int)li;
+        if (sc->lights[li].type <= 2 || sc->lights[li].type == 5)
+            sc->emitter_to_light[sc->lights[li].emissive_material] = (int)li;
     for (size_t li = 0; li < sc->lights.size(); li++)
-        if (sc->lights[li].type == 3 && sc->lights[li].emissive_material >= 0)
+        if ((sc->lights[li].type == 3 || sc->lights[li].type == 6) && sc->lights[li].emissive_material >= 0)
             sc->emitter_to_light[sc->lights[li].emissive_material] = (int)li;
     // RR classifier (Renderer.cs:361-378, ComputeFiniteSceneBounds :475-500)
     AABB bounds;

@@ -32,7 +32,7 @@ def test_abi_version(lib):
     assert lib.rt_abi_version() == 1
 
 
-@pytest.mark.parametrize("struct,size", [("RtMaterialDesc", 120), ("RtEntityDesc", 80), ("RtLightDesc", 88),
+@pytest.mark.parametrize("struct,size", [("RtMaterialDesc", 120), ("RtEntityDesc", 80), ("RtLightDesc", 104),
                                          ("RtCameraDesc", 48), ("RtMediumDesc", 36), ("RtRenderParams", 104),
                                          ("RtStats", 144), ("RtBsdfQuery", 96), ("RtBsdfResult", 80),
                                          ("RtRequest", 72), ("RtSceneInfo", 56), ("RtWorldDesc", 168),
