@@ -76,7 +76,8 @@ class RtWorldDesc(C.Structure):
                 ("tri_verts", C.POINTER(C.c_float)), ("num_tris", C.c_int64),
                 ("lights", C.POINTER(RtLightDesc)), ("num_lights", C.c_int32),
                 ("geometry_light_samples", C.c_int32), ("camera", RtCameraDesc), ("medium", RtMediumDesc),
-                ("tri_normals", C.POINTER(C.c_float)), ("tri_uvs", C.POINTER(C.c_float))]
+                ("tri_normals", C.POINTER(C.c_float)), ("tri_uvs", C.POINTER(C.c_float)),
+                ("sky_color", F3), ("sky_light_samples", C.c_int32)]
 
 
 class RtRenderParams(C.Structure):
@@ -223,7 +224,9 @@ class PackedWorld:
                                 self.tris.ctypes.data_as(fp), world.num_tris,
                                 self.lights, nl, int(world.geometry_light_samples), camera_desc(world.camera), med,
                                 self.normals.ctypes.data_as(fp) if self.normals is not None else fp(),
-                                self.uvs.ctypes.data_as(fp) if self.uvs is not None else fp())
+                                self.uvs.ctypes.data_as(fp) if self.uvs is not None else fp(),
+                                _f3(getattr(world, "sky", (0.0, 0.0, 0.0))),
+                                int(getattr(world, "sky_light_samples", 1)))
 
     def ref(self):
         return C.byref(self.desc)

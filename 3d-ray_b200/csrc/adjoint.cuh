@@ -661,7 +661,7 @@ struct AdjointReplay : AdjointSink {
     // the adjoint captures no AOVs
     RT_D void aov_ray(const Hit&, V3) {}
     RT_D void aov_medium(float, V3) {}
-    RT_D void aov_miss() {}
+    RT_D void aov_miss(V3) {}
     RT_D void aov_surface(V3, const Material&) {}
     RT_D void aov_bounce(bool, V3) {}
     RT_D void shadow(PathState& ps, V3 o, V3 d, float tmax, V3 c, int to_la) {

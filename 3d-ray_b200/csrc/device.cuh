@@ -1471,6 +1471,21 @@ RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, i
         r.color = l.color * atten;
         return r;
     }
+    if (l.type == LIGHT_ENV) {   // EnvironmentLight.IlluminateAndTest (:54-90) over FlatSky.ImportanceSample
+        V3 dir = random_unit_vector(rng);
+        const float pdf = 1.0f / (4.0f * kPi);
+        r.dir = dir;
+        r.dist = kInf;
+        if (length_sq(sn) > 0.0f && dot(sn, dir) <= 0.0f) {   // below a surface's horizon
+            r.occluded = 1;
+            return r;
+        }
+        r.has_ray = 1;
+        r.ray_o = offset_origin(p, sn);
+        r.ray_tmax = kInf;
+        r.color = l.color / (pdf * (float)l.shadow_samples);
+        return r;
+    }
     if (l.type == LIGHT_AREA) {
         int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
         float ru = ((float)su + rng.next()) * l.inv_sqrt;
@@ -1544,6 +1559,7 @@ RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
         return d2 / (l.rep_area * cl);
     }
     if (l.type == LIGHT_GEOM_SPHERE || l.type == LIGHT_SPHERE) return sphere_cone_pdf(l.center, l.radius, p, wi);
+    if (l.type == LIGHT_ENV) return 1.0f / (4.0f * kPi);   // FlatSky.Pdf
     if (l.type == LIGHT_GEOM_MESH) {   // ray cast against the emitter mesh alone
         Hit h;
         int err = 0;

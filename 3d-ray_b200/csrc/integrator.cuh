@@ -75,6 +75,16 @@ RT_D V3 weight_emission(const SceneView& s, const RenderConst& rc, V3 raw, int m
     return raw;
 }
 
+// SampleSky (Renderer.cs:1820-1861) for a flat sky: its radiance, MIS-weighted
+// against the EnvironmentLight's uniform-sphere pdf unless the bounce before
+// was delta (or no EnvironmentLight samples the sky).
+RT_D V3 weight_sky(const SceneView& s, const RenderConst& rc, float prev_pdf, int prev_delta) {
+    if (prev_delta || s.env_light < 0) return s.sky;
+    float pl = 1.0f / (4.0f * kPi);   // EnvironmentLight.PdfSolidAngle -> FlatSky.Pdf
+    if (prev_pdf + pl <= 1e-20f) return v3(0.0f);
+    return s.sky * mis_weight(prev_pdf, pl, rc.mis_power);
+}
+
 // Path state carried from vertex to vertex. The megakernel keeps it in
 // registers; the wavefront stores it in SoA arrays between kernels.
 struct PathState {
@@ -255,8 +265,8 @@ struct NoAdjoint {
     RT_D void aov_ray(const Hit&, V3) {}
     // A medium scattering event at distance t along direction d.
     RT_D void aov_medium(float, V3) {}
-    // The ray left the scene (black flat sky).
-    RT_D void aov_miss() {}
+    // The ray left the scene (the flat sky's radiance).
+    RT_D void aov_miss(V3) {}
     // The surface ShadeSurface is about to shade.
     RT_D void aov_surface(V3, const Material&) {}
     // The bounce decision: a delta lobe with attenuation f, or a non-delta one.
@@ -312,8 +322,10 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         ps.w = ps.w * mb;
         beta_s = ps.beta * mb;
     }
-    if (!hit) {   // black flat sky: SampleSky returns 0
-        sink.aov_miss();
+    if (!hit) {   // SampleSky, then TraceRay's Beer-Lambert over an infinite segment
+        if (s.sky_on) ps.add(ps.w * weight_sky(s, rc, ps.prev_pdf, ps.prev_delta) * bl_factor(ps.cur_abs, INFINITY),
+                             ps.clamp_mode);
+        sink.aov_miss(s.sky);
         return false;
     }
     sink.segment(ps, h.t, SEG_ABSORPTION);
@@ -493,8 +505,8 @@ struct CaptureShadows : InlineShadows<STACK> {
         }
         p.commit_as(v3(1.0f), v3(0.0f));
     }
-    RT_D void aov_miss() {   // :1849-1850, a black flat sky
-        if (probe->pending) probe->commit_as(v3(0.0f), v3(0.0f));
+    RT_D void aov_miss(V3 sky) {   // :1849-1850
+        if (probe->pending) probe->commit_as(clamp01(sky), v3(0.0f));
     }
     RT_D void aov_surface(V3 n, const Material& m) {   // :1051-1054
         if (!probe->pending) return;

@@ -42,7 +42,7 @@ static_assert(sizeof(RtStats) == 144, "ABI layout");
 static_assert(sizeof(RtBsdfQuery) == 96, "ABI layout");
 static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
 static_assert(sizeof(RtRequest) == 72, "ABI layout");
-static_assert(sizeof(RtWorldDesc) == 168, "ABI layout");
+static_assert(sizeof(RtWorldDesc) == 184, "ABI layout");
 static_assert(sizeof(RtCapture) == 64, "ABI layout");
 static_assert(sizeof(RtSceneInfo) == 56, "ABI layout");
 
@@ -1122,6 +1122,9 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     v.sigma_s = h.sigma_s;
     v.sigma_t = h.sigma_t;
     v.hg_g = h.hg_g;
+    v.sky = h.sky;
+    v.sky_on = h.sky_on;
+    v.env_light = h.env_light;
     ray_sort_box(h, v);
     sc->opaque = 1;
     sc->dielectrics = 0;

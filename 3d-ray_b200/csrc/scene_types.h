@@ -91,6 +91,7 @@ enum : int {
     LIGHT_AREA = 3,
     LIGHT_DIRECTIONAL = 4,
     LIGHT_SPHERE = 5,        // SphereLight
+    LIGHT_ENV = 6,           // EnvironmentLight over a flat sky
 };
 
 struct Light {
@@ -175,6 +176,9 @@ struct SceneView {
     int has_medium;
     V3 sigma_a, sigma_s, sigma_t;
     float hg_g;
+    V3 sky;                     // flat sky radiance (black: no sky term)
+    int sky_on;                 // sky is not black
+    int env_light;              // index of the EnvironmentLight, or -1
     // Box of the wavefront's bounce-ray sort: origins map to cells of
     // (o - sort_lo) * sort_scale in [0, 1) (clamped); sort_scale 0 on a flat axis.
     V3 sort_lo, sort_scale;

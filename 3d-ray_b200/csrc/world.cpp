@@ -210,6 +210,11 @@ float light_power(const Light& l, const Box& bounds) {
         return kPi * l.rep_area * luminance(l.emission);
     if (l.type == LIGHT_AREA) return kPi * l.area * luminance(l.color) * l.intensity;   // AreaLight.cs:111
     if (l.type == LIGHT_SPHERE) return 4.0f * kPi * luminance(l.color) * l.intensity;   // SphereLight.cs:79-80
+    if (l.type == LIGHT_ENV) {   // EnvironmentLight.ApproximatePower (:37-52): pi L times the mean cross-section
+        V3 e = bounds.mx - bounds.mn;
+        float cs = 0.5f * (e.x * e.y + e.y * e.z + e.x * e.z);
+        return kPi * luminance(l.color) * cs;
+    }
     V3 ext = bounds.mx - bounds.mn;                                                     // DirectionalLight.cs:82-88
     float radius = 0.5f * length(ext);
     float cs = kPi * radius * radius;
@@ -870,6 +875,25 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             l.radius = sp.r;
             l.rep_area = 4.0f * kPi * sp.r * sp.r;   // Sphere.SurfaceArea (Sphere.cs:78)
         }
+        sc.lights.push_back(l);
+    }
+    // --- the flat sky and its EnvironmentLight (SceneLoader.cs:524-528; FlatSky.cs)
+    sc.sky = v3(w->sky_color[0], w->sky_color[1], w->sky_color[2]);
+    sc.sky_on = sc.sky.x != 0.0f || sc.sky.y != 0.0f || sc.sky.z != 0.0f;
+    sc.env_light = -1;
+    if (luminance(sc.sky) > 1e-6f) {   // FlatSky.HasImportanceSampling
+        Light l{};
+        l.type = LIGHT_ENV;
+        l.quad = -1;
+        l.mesh_root = -1;
+        l.mesh_entity = -1;
+        l.emissive_material = -1;
+        l.color = sc.sky;
+        l.shadow_samples = std::max(1, w->sky_light_samples);
+        l.sqrt_samples = 1;
+        l.inv_sqrt = 1.0f;
+        l.is_delta = 0;
+        sc.env_light = (int)sc.lights.size();
         sc.lights.push_back(l);
     }
     // --- emitter -> light map (Renderer.cs:409-425)

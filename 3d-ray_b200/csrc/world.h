@@ -46,6 +46,9 @@ struct HostScene {
     int has_medium = 0;
     V3 sigma_a{}, sigma_s{}, sigma_t{};
     float hg_g = 0.0f;
+    V3 sky{};
+    int sky_on = 0;
+    int env_light = -1;
 };
 
 // Returns RT_OK or an RT_ERR_* code with a message in err.

@@ -73,6 +73,8 @@ class World:
     tri_uvs: np.ndarray | None = None
     lights: list = dataclasses.field(default_factory=list)
     geometry_light_samples: int = 1
+    sky: tuple = (0.0, 0.0, 0.0)      # flat sky radiance (FlatSky); black: no EnvironmentLight
+    sky_light_samples: int = 1        # the EnvironmentLight's ShadowSamples
     camera: dict = dataclasses.field(default_factory=dict)
     medium: dict | None = None
     name: str = ""
@@ -318,6 +320,25 @@ def cornell_spheres(shadow_samples: int = 1) -> World:
     return w
 
 
+def sky_scene(sky=(0.35, 0.45, 0.65)) -> World:
+    """An open scene under a flat sky (FlatSky + EnvironmentLight): a ground
+    quad, a glossy and a diffuse sphere and a glass sphere with interior
+    absorption, with the camera seeing the sky above the horizon."""
+    w = World(name="sky")
+    ground = w.add_material("ground", disney((0.6, 0.6, 0.55), roughness=0.9))
+    red = w.add_material("red", disney((0.7, 0.15, 0.1), roughness=0.6))
+    gloss = w.add_material("gloss", disney((0.9, 0.9, 0.9), roughness=0.15, metallic=1.0))
+    glass = w.add_material("glass", disney((1.0, 1.0, 1.0), roughness=0.0, spec_trans=1.0, ior=1.5,
+                                           transmission_color=(0.6, 0.8, 0.9), transmission_depth=1.0))
+    w.add_quad((-50, 0, -50), (100, 0, 0), (0, 0, 100), ground, name="ground")
+    w.add_sphere((-2.2, 1.0, 0.0), 1.0, red, name="red")
+    w.add_sphere((0.0, 1.0, 1.5), 1.0, gloss, name="gloss")
+    w.add_sphere((2.2, 1.0, 0.0), 1.0, glass, name="glass")
+    w.sky = tuple(float(x) for x in sky)
+    w.camera = camera((0.0, 2.5, -7.0), (0.0, 1.0, 0.0), (0, 1, 0), 45.0)
+    return w
+
+
 def cornell_volume(shadow_samples: int = 1, density: float = 1.0) -> World:
     """C5: homogeneous medium (sigma_t 0.02 per unit times `density`, albedo
     0.8, HG g 0.6) filling the box, and a dielectric sphere (IOR 1.5,
@@ -483,7 +504,7 @@ def write_yaml(world: World, out_dir: str, name: str | None = None) -> str:
             lights.append(dict(type="directional", direction=list(l["direction"]), color=list(l["color"]),
                                intensity=l["intensity"]))
     c = world.camera
-    doc = dict(world=dict(sky=dict(type="flat", color=[0.0, 0.0, 0.0])),
+    doc = dict(world=dict(sky=dict(type="flat", color=[float(x) for x in world.sky])),
                camera=dict(position=list(c["look_from"]), look_at=list(c["look_at"]), vup=list(c["vup"]),
                            fov=c["vfov"], aperture=c["aperture"], focal_dist=c["focus_dist"]),
                materials=mats, entities=ents, lights=lights)

@@ -161,6 +161,12 @@ typedef struct RtWorldDesc {
     /* null, or 6 floats per triangle: uv0, uv1, uv2 of a smooth triangle, for
      * its UV-gradient tangent frame (null: (0,0), (1,0), (0,1)). */
     const float*          tri_uvs;
+    /* Flat sky colour (Rendering/Sky/FlatSky.cs): the radiance of every ray
+     * that leaves the scene. Unless it is black (luminance <= 1e-6) the
+     * library appends an EnvironmentLight after the geometry lights, as
+     * SceneLoader does (:524-528). */
+    float                 sky_color[3];
+    int32_t               sky_light_samples;  /* its ShadowSamples (the -S override, else 1); <= 0: 1 */
 } RtWorldDesc;
 
 /* ---- render parameters: the Renderer constructor (Renderer.cs:300-319) --- */

@@ -1556,7 +1556,7 @@ struct Light {
     float rep_area = 0.0f;
     V3 center{};   // sphere lights
     float radius = 0.0f;
-};
+};   // type 7: EnvironmentLight over the flat sky (colour in `color`)
 
 struct Scene {
     std::vector<Material> mats;
@@ -1581,6 +1581,8 @@ struct Scene {
     bool has_medium = false;
     V3 sigma_a{}, sigma_s{}, sigma_t{};
     float hg_g = 0.0f;
+    V3 sky{};            // flat sky radiance
+    int env_light = -1;  // its EnvironmentLight
     std::vector<const Hittable*> entity_ptr;   // entity index -> leaf hittable
 
     bool world_hit(const Ray& r, float tmin, float tmax, HitRecord& rec) const { return world.hit(r, tmin, tmax, rec); }
@@ -1588,6 +1590,11 @@ struct Scene {
 
 static float light_approx_power(const Light& l, const AABB& bounds, const Scene& sc) {
     if (l.type == 6) return 4.0f * kPi * luminance(l.color) * l.intensity;   // SphereLight.ApproximatePower (:79-80)
+    if (l.type == 7) {   // EnvironmentLight.ApproximatePower (:37-52)
+        V3 e = bounds.mx - bounds.mn;
+        float cs = 0.5f * (e.x * e.y + e.y * e.z + e.x * e.z);
+        return kPi * luminance(l.color) * cs;
+    }
     if (l.type <= 2 || l.type == 5) {   // GeometryLight.ApproximatePower (:116-120)
         const Material& m = sc.mats[l.emissive_material];
         V3 em = v3(m.d.base_color[0], m.d.base_color[1], m.d.base_color[2]) * std::fmax(m.d.intensity, 0.0f);
@@ -1645,6 +1652,15 @@ static float sphere_cone_pdf(V3 center, float radius, V3 p, V3 wi) {
 // SphereLight.IlluminateAndTestStratified (:72-141),
 // AreaLight.IlluminateAndTestStratified (:129-178), DirectionalLight (:102-160).
 static LightSample illuminate(const Scene& sc, const Light& l, V3 hit_p, V3 surf_n, int s) {
+    if (l.type == 7) {   // EnvironmentLight.IlluminateAndTest (:54-90), FlatSky.ImportanceSample
+        V3 dir = random_unit_vector();
+        float pdf = 1.0f / (4.0f * kPi);
+        if (length_sq(surf_n) > 0.0f && dot(surf_n, dir) <= 0.0f) return {true, v3(0.0f), dir, kInf};
+        V3 so = offset_origin(hit_p, surf_n);
+        V3 tr = shadow_transmittance(sc, Ray(so, dir), kEps, kInf);
+        if (near_zero(tr)) return {true, v3(0.0f), dir, kInf};
+        return {false, l.color * tr / (pdf * (float)l.shadow_samples), dir, kInf};
+    }
     if (l.type == 5) {
         int su = s % l.sqrt_samples, sv = s / l.sqrt_samples;   // Sphere.SampleSolidAngleStratified
         float inv = 1.0f / (float)l.sqrt_samples;
@@ -1842,6 +1858,7 @@ static LightSample illuminate(const Scene& sc, const Light& l, V3 hit_p, V3 surf
 // ILight.PdfSolidAngle implementations.
 static float light_pdf(const Light& l, V3 p, V3 wi) {
     if (l.type == 5 || l.type == 6) return sphere_cone_pdf(l.center, l.radius, p, wi);
+    if (l.type == 7) return 1.0f / (4.0f * kPi);   // FlatSky.Pdf
     if (l.type == 0 || l.type == 1) {   // GeometryLight.PdfSolidAngle area fallback (:254-279)
         Ray r(p, wi);
         HitRecord rec;
@@ -2278,7 +2295,18 @@ struct Tracer {
         return emitted + direct;
     }
 
-    // TraceRay (:1581-1783); sky is black (SampleSky returns 0, no env light)
+    // SampleSky (:1820-1861) for a flat sky: the AOV miss commit, then the
+    // radiance, MIS-weighted against the EnvironmentLight unless the bounce
+    // before was delta.
+    V3 sample_sky(float prev_pdf, bool prev_delta) const {
+        if (t_probe && t_probe->pending) t_probe->commit_as(clamp01(sc.sky), v3(0.0f));   // :1849-1850
+        if (prev_delta || sc.env_light < 0) return sc.sky;
+        float pl = 1.0f / (4.0f * kPi);
+        if (prev_pdf + pl <= 1e-20f) return v3(0.0f);
+        return sc.sky * mis(prev_pdf, pl);
+    }
+
+    // TraceRay (:1581-1783)
     V3 trace(const Ray& ray, int depth, float prev_pdf, bool prev_delta, IorStack& iors, V3 cur_abs, V3 beta) const {
         if (depth <= 0) return v3(0.0f);
         float bmax = std::fmax(beta.x, std::fmax(beta.y, beta.z));
@@ -2299,8 +2327,8 @@ struct Tracer {
             t_probe->camera = false;
         }
         if (!sc.has_medium) {
-            if (!hit && t_probe && t_probe->pending) t_probe->commit_as(v3(0.0f), v3(0.0f));   // black sky (:1849)
-            V3 res = !hit ? v3(0.0f) : shade_surface(ray, rec, depth, prev_pdf, prev_delta, cur_abs, beta, iors);
+            V3 res = !hit ? sample_sky(prev_pdf, prev_delta)
+                          : shade_surface(ray, rec, depth, prev_pdf, prev_delta, cur_abs, beta, iors);
             return beer_lambert(res, cur_abs, hit ? rec.t : INFINITY);
         }
         float tmax = hit ? rec.t : 1e30f;
@@ -2339,8 +2367,7 @@ struct Tracer {
             }
             return beer_lambert(mb * (lnee + lind), cur_abs, tmed);
         }
-        if (!hit && t_probe && t_probe->pending) t_probe->commit_as(v3(0.0f), v3(0.0f));   // black sky (:1849)
-        V3 so = !hit ? v3(0.0f)
+        V3 so = !hit ? mb * sample_sky(prev_pdf, prev_delta)
                      : mb * shade_surface(ray, rec, depth, prev_pdf, prev_delta, cur_abs, beta * mb, iors);
         return beer_lambert(so, cur_abs, hit ? rec.t : INFINITY);
     }
@@ -2663,6 +2690,17 @@ int or_scene_create(const RtWorldDesc* w, void** out) {
             l.radius = sp->r;
             l.rep_area = 4.0f * kPi * sp->r * sp->r;   // Sphere.SurfaceArea
         }
+        sc->lights.push_back(l);
+    }
+    // The flat sky and its EnvironmentLight (SceneLoader.cs:524-528)
+    sc->sky = v3(w->sky_color[0], w->sky_color[1], w->sky_color[2]);
+    if (luminance(sc->sky) > 1e-6f) {
+        Light l;
+        l.type = 7;
+        l.color = sc->sky;
+        l.shadow_samples = std::max(1, (int)w->sky_light_samples);
+        l.is_delta = false;
+        sc->env_light = (int)sc->lights.size();
         sc->lights.push_back(l);
     }
     // Emitter -> light map (Renderer.cs:409-425): geometry lights first, then proxies.

@@ -130,3 +130,71 @@ def test_inside_an_emissive_sphere_matches_oracle(oracle):
         s.close()
     o = _oracle_render(oracle, world, 32, 32, 256)
     np.testing.assert_allclose(g.mean(axis=(1, 2)), o.mean(axis=(1, 2)), rtol=0.03)
+
+
+# --- the flat sky and its EnvironmentLight ----------------------------------------
+def _sky_only(sky=(0.35, 0.45, 0.65)):
+    """Nothing in view: one small quad behind the camera."""
+    w = rt.scenes.World(name="sky-only")
+    m = w.add_material("m", rt.scenes.disney((0.5, 0.5, 0.5)))
+    w.add_quad((-1, -1, 10), (2, 0, 0), (0, 2, 0), m)
+    w.sky = sky
+    w.camera = rt.scenes.camera((0, 0, 0), (0, 0, -1), (0, 1, 0), 40.0)
+    return w
+
+
+def test_host_build_appends_the_environment_light():
+    assert _info(rt.scenes.sky_scene())[1].num_lights == 1
+    assert _info(rt.scenes.sky_scene(sky=(0.0, 0.0, 0.0)))[1].num_lights == 0
+    assert _info(rt.scenes.sky_scene(sky=(1e-7, 0.0, 0.0)))[1].num_lights == 0   # luminance <= 1e-6: no NEE
+
+
+def test_oracle_camera_rays_see_the_sky_at_full_weight(oracle):
+    img = _oracle_render(oracle, _sky_only(), 8, 8, 4)
+    np.testing.assert_allclose(img.mean(axis=(1, 2)), [0.35, 0.45, 0.65], rtol=1e-6)
+
+
+def test_oracle_sky_mis_is_consistent(oracle):
+    """The sky reaches a surface two ways, the EnvironmentLight's NEE and BSDF
+    rays that miss; balance and power heuristics weight them differently but
+    must estimate the same image."""
+    w = rt.scenes.sky_scene()
+    imgs = []
+    for mis in (0, 1):   # RT_MIS_BALANCE, RT_MIS_POWER
+        osc = oracle.OracleScene(abi.PackedWorld(w))
+        try:
+            img, _ = osc.render(abi.render_params(32, 24, 256, 6, mis_heuristic=mis))
+            imgs.append(np.asarray(img, np.float64).reshape(3, 24, 32))
+        finally:
+            osc.close()
+    np.testing.assert_allclose(imgs[0].mean(axis=(1, 2)), imgs[1].mean(axis=(1, 2)), rtol=0.02)
+
+
+@pytest.mark.gpu
+def test_camera_rays_see_the_sky_on_gpu():
+    from test_gpu_parity import Scene
+    s = Scene(_sky_only())
+    try:
+        for k in (abi.KERNEL_MEGAKERNEL, abi.KERNEL_WAVEFRONT):
+            g, _ = s.render(abi.render_params(8, 8, 4, 8, kernel=k))
+            np.testing.assert_allclose(g.mean(axis=(1, 2)), [0.35, 0.45, 0.65], rtol=1e-6)
+    finally:
+        s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [abi.KERNEL_MEGAKERNEL, abi.KERNEL_WAVEFRONT])
+def test_render_sky_matches_oracle(oracle, kernel):
+    """The sky term with its MIS weight, the EnvironmentLight's NEE (horizon
+    test, unbounded shadow rays, glass transmittance) against the oracle."""
+    from test_gpu_parity import Scene
+    world = rt.scenes.sky_scene()
+    s = Scene(world)
+    try:
+        g, st = s.render(abi.render_params(48, 32, 1024, 8, kernel=kernel, wavefront_size=1 << 16))
+    finally:
+        s.close()
+    assert np.all(np.isfinite(g))
+    o = _oracle_render(oracle, world, 48, 32, 256)
+    np.testing.assert_allclose(g.mean(axis=(1, 2)), o.mean(axis=(1, 2)), rtol=0.02)
+    assert rel_mse(o, g) < 0.05
