@@ -28,7 +28,28 @@ struct RenderConst {
     float rr_min_survival;
     int opaque;        // no material transmits shadow rays: any-hit shadows
     int dielectrics;   // a solid dielectric exists: keep the IOR stack
+    int light_pick;    // RT_LIGHTS_*: 0 every light, 1 / 2 one light by power / uniformly
 };
+
+// LightDistribution.Sample (LightDistribution.cs:104-122): the light whose CDF
+// entry is the first not below xi, and its pick probability.
+RT_D int pick_light(const SceneView& s, int mode, float xi, float& pdf) {
+    int n = s.num_lights;
+    const float* cdf = s.pick_cdf + (size_t)(mode - 1) * n;
+    const float* pp = s.pick_pdf + (size_t)(mode - 1) * n;
+    if (n == 1) {
+        pdf = pp[0];
+        return 0;
+    }
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        if (cdf[mid] < xi) lo = mid + 1;
+        else hi = mid;
+    }
+    pdf = pp[lo];
+    return lo;
+}
 
 struct IorStackD {   // Volumetrics/IorStack.cs (capacity 8)
     float slot[8];
@@ -155,8 +176,8 @@ RT_D V3 path_resolve(const PathState& ps, const RenderConst& rc) {
     return clamp_lum(L, rc.max_rad);
 }
 
-// NEE at a surface vertex: ComputeDirectLighting, strategy All
-// (Renderer.cs:1894-2036). The BSDF integrand and the MIS weight are evaluated
+// NEE at a surface vertex: ComputeDirectLighting (Renderer.cs:1894-2036),
+// every light (strategy All) or one picked light (Power, Uniform). The BSDF integrand and the MIS weight are evaluated
 // before the shadow ray and the ray is dropped when they are zero (the
 // reference casts it first; only the cost differs: every draw happens in the
 // light sampler). Each unoccluded sample adds w * colour * brdf * Tr_medium,
@@ -166,7 +187,15 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
                       const Material& m, V3 view, Sink& sink) {
     float view_term = shadow_terminator(rec.n, rec.n, view);
     int to_la = ps.clamp_mode;
-    for (int li = 0; li < s.num_lights; li++) {
+    int l0 = 0, l1 = s.num_lights;
+    float p_pick = 1.0f, inv_pick = 1.0f;
+    if (rc.light_pick) {   // single-light picking (Renderer.cs:1907-1974): lightAccum / pPick
+        if (s.num_lights == 0) return;
+        l0 = pick_light(s, rc.light_pick, ps.rng.next(), p_pick);
+        l1 = l0 + 1;
+        inv_pick = p_pick > 0.0f ? 1.0f / p_pick : 0.0f;
+    }
+    for (int li = l0; li < l1; li++) {
         const Light& l = s.lights[li];
         for (int si = 0; si < l.shadow_samples; si++) {
             LightSample ls = light_sample(s, l, rec.p, rec.n, si, ps.rng);
@@ -184,10 +213,11 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
             if (!l.is_delta) {
                 float pb = bsdf_pdf(m, rec, view, ls.dir);
                 if (pb > 0.0f) {
-                    float pl = light_pdf(s, l, rec.p, ls.dir);
+                    float pl = p_pick * light_pdf(s, l, rec.p, ls.dir);   // pNee = pPick * pLightSample
                     wgt = (pl + pb > 0.0f) ? mis_weight(pl, pb, rc.mis_power) : 1.0f;
                 }
             }
+            wgt *= inv_pick;
             V3 c = ps.w * (wgt * ls.color * brdf * tr_m);
             sink.shadow(ps, ls.ray_o, ls.dir, ls.ray_tmax, c, to_la);
             sink.nee_surface(ps, li, m, rec, ls.dir, view, term, ps.w * (wgt * ls.color), ls.dist, tr_m, to_la);
@@ -195,12 +225,20 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
     }
 }
 
-// NEE at a medium scattering point: ComputeDirectLightingMedium, strategy All
-// (Renderer.cs:2162-2203).
+// NEE at a medium scattering point: ComputeDirectLightingMedium
+// (Renderer.cs:2099-2206), every light or one picked light.
 template <class Sink>
 RT_D void nee_medium(const SceneView& s, const RenderConst& rc, PathState& ps, V3 p, V3 wo, Sink& sink) {
     int to_la = ps.clamp_mode;
-    for (int li = 0; li < s.num_lights; li++) {
+    int l0 = 0, l1 = s.num_lights;
+    float p_pick = 1.0f, inv_pick = 1.0f;
+    if (rc.light_pick) {   // single-light picking in the volumetric path (Renderer.cs:2110-2160)
+        if (s.num_lights == 0) return;
+        l0 = pick_light(s, rc.light_pick, ps.rng.next(), p_pick);
+        l1 = l0 + 1;
+        inv_pick = p_pick > 0.0f ? 1.0f / p_pick : 0.0f;
+    }
+    for (int li = l0; li < l1; li++) {
         const Light& l = s.lights[li];
         for (int si = 0; si < l.shadow_samples; si++) {
             LightSample ls = light_sample(s, l, p, v3(0.0f), si, ps.rng);
@@ -209,9 +247,10 @@ RT_D void nee_medium(const SceneView& s, const RenderConst& rc, PathState& ps, V
             V3 tr_m = medium_tr(s, ls.dist >= kInf ? 1e30f : ls.dist);
             float wgt = 1.0f;
             if (!l.is_delta && ph > 0.0f) {
-                float pl = light_pdf(s, l, p, ls.dir);
+                float pl = p_pick * light_pdf(s, l, p, ls.dir);
                 if (pl + ph > 0.0f) wgt = mis_weight(pl, ph, rc.mis_power);
             }
+            wgt *= inv_pick;
             V3 c = ps.w * (wgt * ls.color * ph * tr_m);
             sink.shadow(ps, ls.ray_o, ls.dir, ls.ray_tmax, c, to_la);
             sink.nee_medium(ps, li, ls.dist, to_la);

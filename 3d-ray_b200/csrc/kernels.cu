@@ -504,8 +504,8 @@ int validate_params(const RtScene* sc, const RtRenderParams* p) {
     if (p->width <= 0 || p->height <= 0 || p->spp <= 0 || p->max_depth < 0)
         return fail(RT_ERR_INVALID_ARG, "width, height and spp must be positive, max_depth non-negative");
     if ((int64_t)p->width * p->height > (int64_t)1 << 28) return fail(RT_ERR_INVALID_ARG, "image too large");
-    if (p->light_strategy != RT_LIGHTS_ALL)
-        return fail(RT_ERR_UNSUPPORTED, "only the 'all' light strategy is on the GPU path");
+    if (p->light_strategy < RT_LIGHTS_ALL || p->light_strategy > RT_LIGHTS_UNIFORM)
+        return fail(RT_ERR_INVALID_ARG, "unknown light strategy");
     int ww = p->window_w > 0 ? p->window_w : p->width;
     int wh = p->window_h > 0 ? p->window_h : p->height;
     if (p->pixel_x0 < 0 || p->pixel_y0 < 0 || p->pixel_x0 + ww > p->width || p->pixel_y0 + wh > p->height)
@@ -529,6 +529,7 @@ rt::RenderConst make_rc(const RtScene* sc, const RtRenderParams* p, const RtCame
     rc.rr_min_survival = p->rr_min_bounces >= 0 ? p->rr_min_survival : sc->host.rr_min_survival;
     rc.opaque = sc->opaque;
     rc.dielectrics = sc->dielectrics;
+    rc.light_pick = p->light_strategy;
     return rc;
 }
 
@@ -1106,6 +1107,8 @@ int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
     r = r ? r : upload(sc, h.smooth, &v.smooth);
     r = r ? r : upload(sc, h.tri_smooth, &v.tri_smooth);
     r = r ? r : upload(sc, h.emitter_light, &v.emitter_light);
+    r = r ? r : upload(sc, h.pick_cdf, &v.pick_cdf);
+    r = r ? r : upload(sc, h.pick_pdf, &v.pick_pdf);
     r = r ? r : upload(sc, h.lut_e, &v.lut_e);
     r = r ? r : upload(sc, h.lut_eavg, &v.lut_eavg);
     if (r != RT_OK) {

@@ -166,6 +166,8 @@ struct SceneView {
     const SmoothTri* smooth;
     const int* tri_smooth;      // per triangle: index into smooth or -1; null when no triangle is smooth
     const int* emitter_light;   // material -> light index or -1
+    const float* pick_cdf;      // 2 * num_lights: the power then the uniform LightDistribution CDF
+    const float* pick_pdf;      // 2 * num_lights: their pdfs
     const float* lut_e;         // 32 x 32, mu-major
     const float* lut_eavg;      // 32
     int num_lights;

@@ -938,6 +938,41 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             bounds = {vmax(raw.mn, v3(-1.0e3f)), vmin(raw.mx, v3(1.0e3f))};
         }
     }
+    // LightDistribution (Lights/LightDistribution.cs:30-102) over these bounds:
+    // the power CDF (uniform when every power is zero), then the uniform one
+    {
+        size_t n = sc.lights.size();
+        sc.pick_cdf.assign(2 * n, 0.0f);
+        sc.pick_pdf.assign(2 * n, 0.0f);
+        for (int mode = 0; mode < 2 && n > 0; mode++) {
+            std::vector<float> power(n, 0.0f);
+            float sum = 0.0f;
+            if (mode == 0)
+                for (size_t i = 0; i < n; i++) {
+                    power[i] = std::fmax(0.0f, light_power(sc.lights[i], bounds));
+                    sum += power[i];
+                }
+            float* cdf = sc.pick_cdf.data() + mode * n;
+            float* pdf = sc.pick_pdf.data() + mode * n;
+            float cum = 0.0f;
+            if (sum > 0.0f) {
+                float inv = 1.0f / sum;
+                for (size_t i = 0; i < n; i++) {
+                    pdf[i] = power[i] * inv;
+                    cum += pdf[i];
+                    cdf[i] = cum;
+                }
+            } else {
+                float u = 1.0f / (float)n;
+                for (size_t i = 0; i < n; i++) {
+                    pdf[i] = u;
+                    cum += u;
+                    cdf[i] = cum;
+                }
+            }
+            cdf[n - 1] = 1.0f;
+        }
+    }
     float flux = 0.0f;
     for (const Light& l : sc.lights) flux += light_power(l, bounds);
     V3 ext = bounds.mx - bounds.mn;

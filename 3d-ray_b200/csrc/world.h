@@ -34,6 +34,7 @@ struct HostScene {
     std::vector<SmoothTri> smooth;
     std::vector<int> tri_smooth;   // per triangle (traversal order); empty when no triangle is smooth
     std::vector<int> emitter_light;
+    std::vector<float> pick_cdf, pick_pdf;   // LightDistribution: power, then uniform (2 * lights each)
     std::vector<float> lut_e, lut_eavg;
     RtCameraDesc camera{};
     int top_root = -1;             // build layout

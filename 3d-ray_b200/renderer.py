@@ -22,7 +22,7 @@ import numpy as np
 from . import abi, scenes
 
 MIS = {"balance": 0, "power": 1}
-LIGHT_STRATEGY = {"all": 0}
+LIGHT_STRATEGY = {"all": 0, "power": 1, "uniform": 2}   # RT_LIGHTS_*
 KERNELS = {"megakernel": abi.KERNEL_MEGAKERNEL, "wavefront": abi.KERNEL_WAVEFRONT}
 
 
@@ -113,7 +113,7 @@ class Renderer:
                  indirect_clamp_factor: float = DEFAULT_INDIRECT_CLAMP_FACTOR, exposure_ev: float = 0.0,
                  kernel: str = "wavefront"):
         if light_sampling_strategy not in LIGHT_STRATEGY:
-            raise ValueError(f"light strategy {light_sampling_strategy!r} is outside the GPU path")
+            raise ValueError(f"unknown light strategy {light_sampling_strategy!r}")
         self.world = world
         self.spp = int(samples_per_pixel)
         self.max_depth = int(max_depth)
@@ -122,6 +122,7 @@ class Renderer:
         self.indirect_clamp_factor = float(indirect_clamp_factor)
         self.exposure_ev = float(exposure_ev)
         self.mis = MIS[mis_heuristic]
+        self.light_strategy = LIGHT_STRATEGY[light_sampling_strategy]
         self.kernel = KERNELS[kernel]
         self.verbose = verbose
         self._lib = abi.load()
@@ -150,7 +151,8 @@ class Renderer:
         return abi.render_params(width, height, self.spp, self.max_depth,
                                  max_sample_radiance=self.max_sample_radiance,
                                  indirect_clamp_factor=self.indirect_clamp_factor, exposure_ev=self.exposure_ev,
-                                 mis_heuristic=self.mis, kernel=self.kernel, **kw)
+                                 mis_heuristic=self.mis, light_strategy=self.light_strategy, kernel=self.kernel,
+                                 **kw)
 
     def autotune(self, width: int, height: int) -> dict:
         best = abi.RtRenderParams()

@@ -173,7 +173,9 @@ typedef struct RtWorldDesc {
 
 #define RT_MIS_BALANCE 0
 #define RT_MIS_POWER   1
-#define RT_LIGHTS_ALL  0
+#define RT_LIGHTS_ALL     0   /* every light, every shadow sample */
+#define RT_LIGHTS_POWER   1   /* one light per vertex, picked by ApproximatePower (LightDistribution.cs) */
+#define RT_LIGHTS_UNIFORM 2   /* one light per vertex, picked uniformly */
 
 #define RT_KERNEL_MEGAKERNEL 0   /* one thread per sample, whole path in registers */
 #define RT_KERNEL_WAVEFRONT  1   /* raygen/extend/shade/occlude/resolve queues     */
@@ -189,7 +191,7 @@ typedef struct RtRenderParams {
     float   indirect_clamp_factor;  /* < 0: default 0.25 (Renderer.cs:214) */
     float   exposure_ev;
     int32_t mis_heuristic;          /* RT_MIS_* */
-    int32_t light_strategy;         /* RT_LIGHTS_ALL only */
+    int32_t light_strategy;         /* RT_LIGHTS_* (LightSamplingStrategy) */
     int32_t kernel;                 /* RT_KERNEL_* */
     int32_t block_size;             /* wavefront: 64, 128 or 256; 0: autotuned / default */
     int32_t wavefront_size;         /* wavefront: path slots; 0: autotuned / default */

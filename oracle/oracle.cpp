@@ -1583,6 +1583,7 @@ struct Scene {
     float hg_g = 0.0f;
     V3 sky{};            // flat sky radiance
     int env_light = -1;  // its EnvironmentLight
+    std::vector<float> pick_cdf[2], pick_pdf[2];   // LightDistribution: power, uniform
     std::vector<const Hittable*> entity_ptr;   // entity index -> leaf hittable
 
     bool world_hit(const Ray& r, float tmin, float tmax, HitRecord& rec) const { return world.hit(r, tmin, tmax, rec); }
@@ -2026,6 +2027,7 @@ struct RenderCfg {
     int mis_power;
     int rr_min_bounces;
     float rr_min_survival;
+    int light_pick = 0;   // LightSamplingStrategy: 0 All, 1 Power, 2 Uniform
 };
 
 static inline V3 sanitize(V3 c) {   // Renderer.cs:917-923
@@ -2106,9 +2108,57 @@ struct Tracer {
     }
 
     // ComputeDirectLighting, strategy All (:1894-2036)
+    // LightDistribution.Sample (LightDistribution.cs:104-122)
+    int pick_light(float xi, float& pdf) const {
+        const std::vector<float>& cdf = sc.pick_cdf[cfg.light_pick - 1];
+        const std::vector<float>& pp = sc.pick_pdf[cfg.light_pick - 1];
+        int n = (int)cdf.size();
+        if (n == 1) {
+            pdf = pp[0];
+            return 0;
+        }
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (cdf[mid] < xi) lo = mid + 1;
+            else hi = mid;
+        }
+        pdf = pp[lo];
+        return lo;
+    }
+
     V3 direct_lighting(const HitRecord& rec, V3 view, const Disney& bsdf) const {
         V3 result = v3(0.0f);
         float view_term = shadow_terminator(rec.n, rec.n, view);   // ShadingNg == Normal (no normal maps)
+        if (cfg.light_pick) {   // single-light picking (:1907-1974)
+            if (sc.lights.empty()) return result;
+            float p_pick;
+            const Light& l = sc.lights[pick_light(random_float(), p_pick)];
+            V3 acc = v3(0.0f);
+            for (int s = 0; s < l.shadow_samples; s++) {
+                LightSample ls = illuminate(sc, l, rec.p, rec.n, s);
+                if (ls.in_shadow) continue;
+                V3 brdf = bsdf.evaluate_direct(ls.dir, view, rec.n, rec);
+                brdf *= view_term * shadow_terminator(rec.n, rec.n, ls.dir);
+                if (brdf == v3(0.0f)) continue;
+                V3 tr = v3(1.0f);
+                if (sc.has_medium) {
+                    float sd = std::isinf(ls.dist) || ls.dist >= kInf ? 1e30f : ls.dist;
+                    tr = medium_tr(sd);
+                }
+                float w_nee = 1.0f;
+                if (!l.is_delta) {
+                    float p_bsdf = bsdf.pdf(view, ls.dir, rec);
+                    if (p_bsdf > 0.0f) {
+                        float p_nee = p_pick * light_pdf(l, rec.p, ls.dir);
+                        w_nee = (p_nee + p_bsdf > 0.0f) ? mis(p_nee, p_bsdf) : 1.0f;
+                    }
+                }
+                acc += w_nee * ls.color * brdf * tr;
+            }
+            if (p_pick > 0.0f) result += acc / p_pick;
+            return result;
+        }
         for (size_t li = 0; li < sc.lights.size(); li++) {
             const Light& l = sc.lights[li];
             V3 acc = v3(0.0f);
@@ -2147,6 +2197,30 @@ struct Tracer {
     // ComputeDirectLightingMedium, strategy All (:2162-2203)
     V3 direct_lighting_medium(V3 p, V3 wo) const {
         V3 result = v3(0.0f);
+        if (cfg.light_pick) {   // single-light picking in the volumetric path (:2110-2160)
+            if (sc.lights.empty()) return result;
+            float p_pick;
+            const Light& l = sc.lights[pick_light(random_float(), p_pick)];
+            V3 acc = v3(0.0f);
+            for (int s = 0; s < l.shadow_samples; s++) {
+                LightSample ls = illuminate(sc, l, p, v3(0.0f), s);
+                if (ls.in_shadow) continue;
+                float ph = hg_eval(wo, ls.dir);
+                float sd = ls.dist >= kInf ? 1e30f : ls.dist;
+                V3 tr = medium_tr(sd);
+                float w_nee = 1.0f;
+                if (!l.is_delta) {
+                    float pp = hg_eval(wo, ls.dir);
+                    if (pp > 0.0f) {
+                        float p_nee = p_pick * light_pdf(l, p, ls.dir);
+                        if (p_nee + pp > 0.0f) w_nee = mis(p_nee, pp);
+                    }
+                }
+                acc += w_nee * ls.color * ph * tr;
+            }
+            if (p_pick > 0.0f) result += acc / p_pick;
+            return result;
+        }
         for (size_t li = 0; li < sc.lights.size(); li++) {
             const Light& l = sc.lights[li];
             V3 acc = v3(0.0f);
@@ -2730,6 +2804,39 @@ int or_scene_create(const RtWorldDesc* w, void** out) {
             bounds = {vmax(raw.mn, v3(-1.0e3f)), vmin(raw.mx, v3(1.0e3f))};
         }
     }
+    // LightDistribution (LightDistribution.cs:30-102): power, then forced uniform
+    for (int mode = 0; mode < 2; mode++) {
+        size_t n = sc->lights.size();
+        std::vector<float>& cdf = sc->pick_cdf[mode];
+        std::vector<float>& pdf = sc->pick_pdf[mode];
+        cdf.assign(n, 0.0f);
+        pdf.assign(n, 0.0f);
+        if (n == 0) continue;
+        std::vector<float> power(n, 0.0f);
+        float sum = 0.0f;
+        if (mode == 0)
+            for (size_t i = 0; i < n; i++) {
+                power[i] = std::fmax(0.0f, light_approx_power(sc->lights[i], bounds, *sc));
+                sum += power[i];
+            }
+        float cum = 0.0f;
+        if (sum > 0.0f) {
+            float inv = 1.0f / sum;
+            for (size_t i = 0; i < n; i++) {
+                pdf[i] = power[i] * inv;
+                cum += pdf[i];
+                cdf[i] = cum;
+            }
+        } else {
+            float u = 1.0f / (float)n;
+            for (size_t i = 0; i < n; i++) {
+                pdf[i] = u;
+                cum += u;
+                cdf[i] = cum;
+            }
+        }
+        cdf[n - 1] = 1.0f;
+    }
     float flux = 0.0f;
     for (const Light& l : sc->lights) flux += light_approx_power(l, bounds, *sc);
     V3 ext = bounds.mx - bounds.mn;
@@ -2932,6 +3039,7 @@ int or_render_capture(void* s, const RtRenderParams* p, float* out, int32_t thre
     tr.cfg.mis_power = p->mis_heuristic == RT_MIS_POWER;
     tr.cfg.rr_min_bounces = p->rr_min_bounces >= 0 ? p->rr_min_bounces : sc->rr_min_bounces;
     tr.cfg.rr_min_survival = p->rr_min_bounces >= 0 ? p->rr_min_survival : sc->rr_min_survival;
+    tr.cfg.light_pick = p->light_strategy;
     const int T = 16;
     int tx = (W + T - 1) / T, ty = (H + T - 1) / T;
     std::atomic<int> next(0);
@@ -2969,6 +3077,7 @@ int or_render(void* s, const RtRenderParams* p, float* out, int32_t threads, uin
     tr.cfg.mis_power = p->mis_heuristic == RT_MIS_POWER;
     tr.cfg.rr_min_bounces = p->rr_min_bounces >= 0 ? p->rr_min_bounces : sc->rr_min_bounces;
     tr.cfg.rr_min_survival = p->rr_min_bounces >= 0 ? p->rr_min_survival : sc->rr_min_survival;
+    tr.cfg.light_pick = p->light_strategy;
     int x0 = p->pixel_x0, y0 = p->pixel_y0;
     int ww = p->window_w > 0 ? p->window_w : W;
     int wh = p->window_h > 0 ? p->window_h : H;

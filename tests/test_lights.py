@@ -198,3 +198,71 @@ def test_render_sky_matches_oracle(oracle, kernel):
     o = _oracle_render(oracle, world, 48, 32, 256)
     np.testing.assert_allclose(g.mean(axis=(1, 2)), o.mean(axis=(1, 2)), rtol=0.02)
     assert rel_mse(o, g) < 0.05
+
+
+# --- Power / Uniform light picking (LightDistribution, Renderer.cs:1907-1974) -------
+def _two_suns():
+    """Delta lights only: NEE carries no MIS weight, so picking one light per
+    vertex (divided by its pick probability) estimates the same image as
+    sampling every light."""
+    w = rt.scenes.sky_scene(sky=(0.0, 0.0, 0.0))
+    w.lights.append(dict(type=rt.scenes.LIGHT_DIRECTIONAL, direction=(-1.0, -2.0, -0.5), color=(1.0, 0.95, 0.9),
+                         intensity=2.0, shadow_samples=1, angular_radius_deg=0.0))
+    w.lights.append(dict(type=rt.scenes.LIGHT_DIRECTIONAL, direction=(1.5, -1.0, 0.5), color=(0.6, 0.7, 1.0),
+                         intensity=0.7, shadow_samples=1, angular_radius_deg=0.0))
+    return w
+
+
+def _oracle_mean(oracle, world, strategy, w=32, h=24, spp=256):
+    osc = oracle.OracleScene(abi.PackedWorld(world))
+    try:
+        img, _ = osc.render(abi.render_params(w, h, spp, 6, light_strategy=strategy))
+        return np.asarray(img, np.float64).reshape(3, h, w)
+    finally:
+        osc.close()
+
+
+def test_oracle_light_picking_is_unbiased_for_delta_lights(oracle):
+    w = _two_suns()
+    every = _oracle_mean(oracle, w, 0)
+    for strategy in (1, 2):   # RT_LIGHTS_POWER, RT_LIGHTS_UNIFORM
+        np.testing.assert_allclose(_oracle_mean(oracle, w, strategy).mean(axis=(1, 2)), every.mean(axis=(1, 2)),
+                                   rtol=0.03)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("strategy,kernel", [(1, abi.KERNEL_MEGAKERNEL), (1, abi.KERNEL_WAVEFRONT),
+                                             (2, abi.KERNEL_WAVEFRONT)])
+def test_light_picking_matches_oracle(oracle, strategy, kernel):
+    """Three non-delta emitters: the pick, its probability in the NEE MIS pdf
+    and the division by it, as the oracle does them (including the reference's
+    emission MIS, which keeps the unpicked light pdf)."""
+    from test_gpu_parity import Scene
+    world = rt.scenes.cornell_spheres()
+    s = Scene(world)
+    try:
+        g, _ = s.render(abi.render_params(48, 48, 1024, 8, kernel=kernel, light_strategy=strategy,
+                                          wavefront_size=1 << 16))
+    finally:
+        s.close()
+    osc = oracle.OracleScene(abi.PackedWorld(world))
+    try:
+        o, _ = osc.render(abi.render_params(48, 48, 256, 8, light_strategy=strategy))
+    finally:
+        osc.close()
+    o = np.asarray(o, np.float64).reshape(3, 48, 48)
+    np.testing.assert_allclose(g.mean(axis=(1, 2)), o.mean(axis=(1, 2)), rtol=0.03)
+    assert rel_mse(o, g) < 0.08
+
+
+@pytest.mark.gpu
+def test_unknown_light_strategy_is_rejected():
+    from test_gpu_parity import Scene
+    s = Scene(rt.scenes.cornell())
+    try:
+        out = np.zeros((3, 8, 8), np.float32)
+        rc = s.lib.rt_render(s.h, C.byref(abi.render_params(8, 8, 1, 4, light_strategy=3)), abi.ptr(out),
+                             C.byref(abi.RtStats()))
+    finally:
+        s.close()
+    assert rc == -1   # RT_ERR_INVALID_ARG
