@@ -1287,81 +1287,15 @@ RT_D float sphere_cone_pdf(V3 center, float radius, V3 p, V3 wi) {
     return sa > kEps ? 1.0f / sa : 0.0f;
 }
 
-// Draws the light sample (all RNG draws happen here, before any shadow test):
-// GeometryLight.ComputeAreaSample (GeometryLight.cs:149-190),
-// AreaLight.IlluminateAndTestStratified (AreaLight.cs:129-178),
-// DirectionalLight.IlluminateAndTestStratified (DirectionalLight.cs:102-160).
-RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, int si, Sampler& rng) {
+// The sphere and sky samplers of light_sample, out of line: most scenes have
+// none of these lights, and the shade kernel is bound by instruction fetch.
+__device__ __noinline__ LightSample light_sample_sphere_env(const SceneView& s, const Light& l, V3 p, V3 sn, int si,
+                                                         Sampler& rng) {
     LightSample r;
     r.occluded = 0;
     r.has_ray = 0;
     r.color = v3(0.0f);
     r.dist = 0.0f;
-    if (l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH) {
-        V3 sp, ln;
-        float area;
-        if (l.type == LIGHT_GEOM_QUAD) {   // Quad.SampleStratified (Quad.cs:99-109)
-            const QuadData& q = s.quads[l.quad];
-            int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
-            float inv = 1.0f / (float)l.sqrt_samples;
-            float uu = ((float)su + rng.next()) * inv;
-            float vv = ((float)sv + rng.next()) * inv;
-            sp = q.q + uu * q.u + vv * q.v;
-            ln = q.normal;
-            area = q.area;
-        } else {   // Mesh.SampleStratified (Mesh.cs:151-178) + Triangle.Sample
-            int total = max(1, l.sqrt_samples * l.sqrt_samples);
-            float stratum = 1.0f / (float)total;
-            float jit = ((float)si + rng.next()) * stratum;
-            float target = clampf(jit, 0.0f, 0.9999999f) * l.rep_area;
-            int lo = 0, hi = l.mesh_count;   // lower_bound over the cumulative areas
-            while (lo < hi) {
-                int mid = (lo + hi) >> 1;
-                if (s.light_tris[l.mesh_first + mid].cum_area < target) lo = mid + 1;
-                else hi = mid;
-            }
-            int idx = min(max(lo, 0), l.mesh_count - 1);
-            const LightTri& t = s.light_tris[l.mesh_first + idx];
-            float x1 = rng.next();
-            float x2 = rng.next();
-            float r1 = sqrtf(x1);
-            float u = 1.0f - r1;
-            float v = x2 * r1;
-            if (t.smooth >= 0) {   // SmoothTriangle.SampleAt (:219-230)
-                const SmoothTri& st = s.smooth[t.smooth];
-                float w0 = 1.0f - u - v;
-                sp = w0 * t.v0 + u * st.v1 + v * st.v2;
-                ln = normalize(w0 * st.n0 + u * st.n1 + v * st.n2);
-            } else {
-                sp = t.v0 + u * t.e1 + v * t.e2;
-                ln = t.normal;
-            }
-            area = l.rep_area;
-        }
-        V3 tl = sp - p;
-        float d2 = length_sq(tl);
-        if (d2 < kEps * kEps) {
-            r.occluded = 1;
-            r.dir = v3(0.0f, 1.0f, 0.0f);
-            return r;
-        }
-        float dist = sqrtf(d2);
-        V3 dir = tl / dist;
-        r.dir = dir;
-        r.dist = dist;
-        float cl = fmaxf(0.0f, dot(-dir, ln));
-        if (cl <= 0.0f) {
-            r.occluded = 1;
-            return r;
-        }
-        V3 so = offset_origin(p, sn);
-        r.has_ray = 1;
-        r.ray_o = so;
-        r.ray_tmax = length(sp - so) - kEps;
-        float atten = area * cl / (d2 * (float)l.shadow_samples);
-        r.color = l.emission * atten;
-        return r;
-    }
     if (l.type == LIGHT_GEOM_SPHERE) {   // GeometryLight.ComputeSolidAngleSample (:202-238)
         int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
         float xi1 = ((float)su + rng.next()) * l.inv_sqrt;   // Sphere.SampleSolidAngleStratified
@@ -1486,6 +1420,86 @@ RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, i
         r.color = l.color / (pdf * (float)l.shadow_samples);
         return r;
     }
+    return r;   // not reached: the caller passes only these three types
+}
+
+// Draws the light sample (all RNG draws happen here, before any shadow test):
+// GeometryLight.ComputeAreaSample (GeometryLight.cs:149-190),
+// AreaLight.IlluminateAndTestStratified (AreaLight.cs:129-178),
+// DirectionalLight.IlluminateAndTestStratified (DirectionalLight.cs:102-160).
+RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, int si, Sampler& rng) {
+    LightSample r;
+    r.occluded = 0;
+    r.has_ray = 0;
+    r.color = v3(0.0f);
+    r.dist = 0.0f;
+    if (l.type == LIGHT_GEOM_QUAD || l.type == LIGHT_GEOM_MESH) {
+        V3 sp, ln;
+        float area;
+        if (l.type == LIGHT_GEOM_QUAD) {   // Quad.SampleStratified (Quad.cs:99-109)
+            const QuadData& q = s.quads[l.quad];
+            int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
+            float inv = 1.0f / (float)l.sqrt_samples;
+            float uu = ((float)su + rng.next()) * inv;
+            float vv = ((float)sv + rng.next()) * inv;
+            sp = q.q + uu * q.u + vv * q.v;
+            ln = q.normal;
+            area = q.area;
+        } else {   // Mesh.SampleStratified (Mesh.cs:151-178) + Triangle.Sample
+            int total = max(1, l.sqrt_samples * l.sqrt_samples);
+            float stratum = 1.0f / (float)total;
+            float jit = ((float)si + rng.next()) * stratum;
+            float target = clampf(jit, 0.0f, 0.9999999f) * l.rep_area;
+            int lo = 0, hi = l.mesh_count;   // lower_bound over the cumulative areas
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (s.light_tris[l.mesh_first + mid].cum_area < target) lo = mid + 1;
+                else hi = mid;
+            }
+            int idx = min(max(lo, 0), l.mesh_count - 1);
+            const LightTri& t = s.light_tris[l.mesh_first + idx];
+            float x1 = rng.next();
+            float x2 = rng.next();
+            float r1 = sqrtf(x1);
+            float u = 1.0f - r1;
+            float v = x2 * r1;
+            if (t.smooth >= 0) {   // SmoothTriangle.SampleAt (:219-230)
+                const SmoothTri& st = s.smooth[t.smooth];
+                float w0 = 1.0f - u - v;
+                sp = w0 * t.v0 + u * st.v1 + v * st.v2;
+                ln = normalize(w0 * st.n0 + u * st.n1 + v * st.n2);
+            } else {
+                sp = t.v0 + u * t.e1 + v * t.e2;
+                ln = t.normal;
+            }
+            area = l.rep_area;
+        }
+        V3 tl = sp - p;
+        float d2 = length_sq(tl);
+        if (d2 < kEps * kEps) {
+            r.occluded = 1;
+            r.dir = v3(0.0f, 1.0f, 0.0f);
+            return r;
+        }
+        float dist = sqrtf(d2);
+        V3 dir = tl / dist;
+        r.dir = dir;
+        r.dist = dist;
+        float cl = fmaxf(0.0f, dot(-dir, ln));
+        if (cl <= 0.0f) {
+            r.occluded = 1;
+            return r;
+        }
+        V3 so = offset_origin(p, sn);
+        r.has_ray = 1;
+        r.ray_o = so;
+        r.ray_tmax = length(sp - so) - kEps;
+        float atten = area * cl / (d2 * (float)l.shadow_samples);
+        r.color = l.emission * atten;
+        return r;
+    }
+    if (l.type == LIGHT_GEOM_SPHERE || l.type == LIGHT_SPHERE || l.type == LIGHT_ENV)
+        return light_sample_sphere_env(s, l, p, sn, si, rng);
     if (l.type == LIGHT_AREA) {
         int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
         float ru = ((float)su + rng.next()) * l.inv_sqrt;
@@ -1545,6 +1559,28 @@ RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, i
     return r;
 }
 
+// GeometryLight.PdfSolidAngle for an emissive mesh: a ray cast against the
+// emitter mesh alone (a whole BVH walk), out of line like the cold samplers.
+__device__ __noinline__ float mesh_light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
+    Hit h;
+    int err = 0;
+    traverse<false, 64>(s, p, wi, kEps, kInf, h, nullptr, &err, true, l.mesh_root);
+    if (err || h.kind == HIT_NONE) return 0.0f;
+    const float4* tp = s.tris + 3 * h.slot;
+    V3 n = v3(__ldg(tp).w, __ldg(tp + 1).w, __ldg(tp + 2).w);
+    int si = s.tri_smooth ? s.tri_smooth[h.slot] : -1;
+    if (si >= 0) {   // the hit record's normal is the interpolated one
+        const SmoothTri& st = s.smooth[si];
+        float w0 = 1.0f - h.u - h.v;
+        n = normalize(w0 * st.n0 + h.u * st.n1 + h.v * st.n2);
+    }
+    float cl = fabsf(dot(-wi, n));
+    if (cl < 1e-6f) return 0.0f;
+    float d2 = h.t * h.t;
+    if (l.rep_area < 1e-12f) return 0.0f;
+    return d2 / (l.rep_area * cl);
+}
+
 // ILight.PdfSolidAngle (GeometryLight.cs:254-279, AreaLight.cs:189-226,
 // DirectionalLight.cs:169-181).
 RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
@@ -1560,25 +1596,7 @@ RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
     }
     if (l.type == LIGHT_GEOM_SPHERE || l.type == LIGHT_SPHERE) return sphere_cone_pdf(l.center, l.radius, p, wi);
     if (l.type == LIGHT_ENV) return 1.0f / (4.0f * kPi);   // FlatSky.Pdf
-    if (l.type == LIGHT_GEOM_MESH) {   // ray cast against the emitter mesh alone
-        Hit h;
-        int err = 0;
-        traverse<false, 64>(s, p, wi, kEps, kInf, h, nullptr, &err, true, l.mesh_root);
-        if (err || h.kind == HIT_NONE) return 0.0f;
-        const float4* tp = s.tris + 3 * h.slot;
-        V3 n = v3(__ldg(tp).w, __ldg(tp + 1).w, __ldg(tp + 2).w);
-        int si = s.tri_smooth ? s.tri_smooth[h.slot] : -1;
-        if (si >= 0) {   // the hit record's normal is the interpolated one
-            const SmoothTri& st = s.smooth[si];
-            float w0 = 1.0f - h.u - h.v;
-            n = normalize(w0 * st.n0 + h.u * st.n1 + h.v * st.n2);
-        }
-        float cl = fabsf(dot(-wi, n));
-        if (cl < 1e-6f) return 0.0f;
-        float d2 = h.t * h.t;
-        if (l.rep_area < 1e-12f) return 0.0f;
-        return d2 / (l.rep_area * cl);
-    }
+    if (l.type == LIGHT_GEOM_MESH) return mesh_light_pdf(s, l, p, wi);
     if (l.type == LIGHT_AREA) {
         float denom = dot(l.normal, wi);
         if (fabsf(denom) < 1e-7f) return 0.0f;
