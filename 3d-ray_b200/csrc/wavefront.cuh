@@ -38,7 +38,7 @@ struct WfRequest {
     int spp, spp0;
     long long begin;      // first global work id of this request
     long long count;      // ww * wh * spp
-    float* accum;         // 3 * ww * wh: sums of clamped samples (planar)
+    float* accum;         // 3 * ww * wh: sums of clamped samples (planar, pixels in strip_pixel order)
 };
 
 // SoA path state (144 B per slot + 16 B hit).
@@ -153,6 +153,25 @@ RT_D int wf_flags(const PathState& ps, int alive) {
            (ps.clamp_mode ? PF_CLAMP : 0);
 }
 
+// The window's pixels in 8-pixel-wide column strips, rows inside a strip:
+// regen hands out work ids in this order, so the 32 camera rays of a warp
+// cover an 8x4 block rather than a 32x1 run, and the accumulation buffer is
+// laid out the same way, so that the film atomics of consecutive slots stay
+// contiguous. The last strip is narrower when ww % 8 != 0.
+constexpr int kStripW = 8;   // 4 and 16 measured the same
+RT_D void strip_pixel(int p, int ww, int wh, int& lx, int& ly) {
+    int strip = p / (kStripW * wh);
+    int in = p - strip * kStripW * wh;
+    int sw = min(kStripW, ww - kStripW * strip);
+    lx = kStripW * strip + in % sw;
+    ly = in / sw;
+}
+RT_D int strip_index(int lx, int ly, int ww, int wh) {
+    int strip = lx / kStripW;
+    int sw = min(kStripW, ww - kStripW * strip);
+    return strip * kStripW * wh + ly * sw + (lx - kStripW * strip);
+}
+
 RT_D uint32_t pixel_seed(int px, int py) { return ((uint32_t)px * 73856093u) ^ ((uint32_t)py * 19349663u); }
 
 // Rebuilds the register path state of slot i (lp/la read after occlude).
@@ -226,7 +245,7 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
         wf_load(a, i, R, ps, fl, pix);
         V3 L = path_resolve(ps, R.rc);
         int lx = pix & 0xFFFF, ly = pix >> 16;
-        size_t plane = (size_t)R.ww * R.wh, k = (size_t)ly * R.ww + lx;
+        size_t plane = (size_t)R.ww * R.wh, k = (size_t)strip_index(lx, ly, R.ww, R.wh);
         atomicAdd(R.accum + k, L.x);
         atomicAdd(R.accum + plane + k, L.y);
         atomicAdd(R.accum + 2 * plane + k, L.z);
@@ -264,7 +283,8 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
             long long npix = (long long)R.ww * R.wh;
             int s = (int)(local / npix);
             int p = (int)(local % npix);
-            int lx = p % R.ww, ly = p / R.ww;
+            int lx, ly;
+            strip_pixel(p, R.ww, R.wh, lx, ly);
             PathState ps;
             path_init(ps, R.rc, R.x0 + lx, R.y0 + ly, (uint32_t)(R.spp0 + s));
             int al = path_alive(ps);
@@ -760,7 +780,8 @@ __global__ void k_wf_finalize(const WfRequest* reqs, int nreq, float* const* fil
     const WfRequest& R = reqs[r];
     long long plane = (long long)R.ww * R.wh;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
-        int lx = (int)(i % R.ww), ly = (int)(i / R.ww);
+        int lx, ly;
+        strip_pixel((int)i, R.ww, R.wh, lx, ly);   // the accumulation buffer is in strip order
         size_t fp = (size_t)film_w[r] * film_h[r];
         size_t fi = (size_t)(R.y0 + ly) * film_w[r] + (R.x0 + lx);
         for (int c = 0; c < 3; c++) films[r][c * fp + fi] = R.accum[c * plane + i] / (float)R.spp;
