@@ -106,7 +106,15 @@ class RtSceneInfo(C.Structure):
     _fields_ = [("num_nodes", C.c_int64), ("num_tris", C.c_int64), ("num_entities", C.c_int32),
                 ("num_lights", C.c_int32), ("top_is_bvh", C.c_int32), ("max_stack_depth", C.c_int32),
                 ("rr_min_bounces", C.c_int32), ("rr_min_survival", C.c_float), ("mean_irradiance", C.c_float),
-                ("pad", C.c_int32), ("device_bytes", C.c_int64)]
+                ("bvh_on_device", C.c_int32), ("device_bytes", C.c_int64), ("bvh_build_ms", C.c_double)]
+
+
+BVH_AUTO, BVH_HOST, BVH_DEVICE = 0, 1, 2   # RT_BVH_*
+BVH_AUTO_MIN_TRIS = 65536
+
+
+class RtSceneOptions(C.Structure):
+    _fields_ = [("bvh_build", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class RtCapture(C.Structure):
@@ -267,6 +275,7 @@ def load(path: str | None = None):
         "rt_last_error": (C.c_char_p, []),
         "rt_device_count": (C.c_int, []),
         "rt_scene_create": (C.c_int, [C.POINTER(RtWorldDesc), C.POINTER(P)]),
+        "rt_scene_create_ex": (C.c_int, [C.POINTER(RtWorldDesc), C.POINTER(RtSceneOptions), C.POINTER(P)]),
         "rt_scene_destroy": (C.c_int, [P]),
         "rt_scene_info": (C.c_int, [P, C.POINTER(RtSceneInfo)]),
         "rt_scene_export_bvh": (C.c_int, [P, P, C.c_int64, P, C.c_int64, P, C.c_int64]),

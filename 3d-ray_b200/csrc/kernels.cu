@@ -44,7 +44,8 @@ static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
 static_assert(sizeof(RtRequest) == 72, "ABI layout");
 static_assert(sizeof(RtWorldDesc) == 184, "ABI layout");
 static_assert(sizeof(RtCapture) == 64, "ABI layout");
-static_assert(sizeof(RtSceneInfo) == 56, "ABI layout");
+static_assert(sizeof(RtSceneInfo) == 64, "ABI layout");
+static_assert(sizeof(RtSceneOptions) == 32, "ABI layout");
 
 constexpr int kStack = 64;       // traversal stack entries per thread
 constexpr int kBlock = 128;      // 16 x 8 pixel tiles
@@ -1055,14 +1056,25 @@ int rt_device_count(void) {
     return n;
 }
 
-int rt_scene_create(const RtWorldDesc* world, RtScene** out) {
+int rt_scene_create(const RtWorldDesc* world, RtScene** out) { return rt_scene_create_ex(world, nullptr, out); }
+
+int rt_scene_create_ex(const RtWorldDesc* world, const RtSceneOptions* options, RtScene** out) {
     if (!world || !out) return fail(RT_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
+    RtSceneOptions opt{};
+    if (options) opt = *options;
+    if (opt.bvh_build < RT_BVH_AUTO || opt.bvh_build > RT_BVH_DEVICE)
+        return fail(RT_ERR_INVALID_ARG, "bvh_build must be RT_BVH_AUTO, RT_BVH_HOST or RT_BVH_DEVICE");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(RT_ERR_NO_DEVICE, "no CUDA device");
+    rt::BuildOptions bo;
+    if (opt.bvh_build != RT_BVH_HOST) {
+        bo.device_builder = rt::device_build_meshes;
+        bo.device_min_tris = opt.bvh_build == RT_BVH_AUTO ? RT_BVH_AUTO_MIN_TRIS : 0;
+    }
     auto* sc = new RtScene();
     std::string err;
-    int rc = rt::build_world(world, sc->host, err);
+    int rc = rt::build_world(world, sc->host, err, bo);
     if (rc == RT_OK) {
         sc->w = *world;
         sc->w_materials.assign(world->materials, world->materials + world->num_materials);
@@ -1174,7 +1186,9 @@ int rt_scene_info(const RtScene* sc, RtSceneInfo* info) {
     info->rr_min_bounces = h.rr_min_bounces;
     info->rr_min_survival = h.rr_min_survival;
     info->mean_irradiance = h.mean_irradiance;
+    info->bvh_on_device = h.bvh_on_device;
     info->device_bytes = (int64_t)sc->bytes;
+    info->bvh_build_ms = h.bvh_build_ms;
     return RT_OK;
 }
 
@@ -1215,6 +1229,7 @@ int rt_world_inspect(const RtWorldDesc* world, RtSceneInfo* info, int32_t* nodes
         info->rr_min_bounces = h.rr_min_bounces;
         info->rr_min_survival = h.rr_min_survival;
         info->mean_irradiance = h.mean_irradiance;
+        info->bvh_build_ms = h.bvh_build_ms;
     }
     if (nodes) std::memcpy(nodes, h.nodes.data(), (size_t)std::min<int64_t>(max_nodes, (int64_t)h.nodes.size()) * sizeof(rt::NodeF));
     if (top_items)

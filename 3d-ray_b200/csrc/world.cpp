@@ -3,8 +3,11 @@
 // C# host computes for the same scene.
 #include "world.h"
 
+#include "sah.h"
+
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -16,28 +19,15 @@ namespace rt {
 
 namespace {
 
-struct Box {
-    V3 mn, mx;
-};
-inline Box surround(const Box& a, const Box& b) { return {vmin(a.mn, b.mn), vmax(a.mx, b.mx)}; }
-inline Box empty_box() { return {v3(kInf), v3(-kInf)}; }   // AABB.Empty (Core/AABB.cs:77)
-inline float surface_area(const Box& b) {                   // AABB.SurfaceArea (Core/AABB.cs:70-75)
-    V3 d = b.mx - b.mn;
-    if (d.x < 0.0f || d.y < 0.0f || d.z < 0.0f) return 0.0f;
-    return 2.0f * (d.x * d.y + d.x * d.z + d.y * d.z);
-}
-
 // One binned-SAH tree over `boxes`, built exactly like BvhNode's constructor
 // (fat leaves <= 4, 16 bins per axis, traversal cost 0.5, in-place partition,
 // median fallbacks). Nodes are emitted in pre-order into `out` with indices
 // local to `out`; `idx` ends in leaf order.
 struct SahBuilder {
-    static const int kMaxLeaf = 4;    // BvhNode.cs:53
-    static const int kBins = 16;      // BvhNode.cs:60
+    static const int kMaxLeaf = kSahMaxLeaf;
     const std::vector<Box>& boxes;
     std::vector<int>& idx;
     std::vector<NodeF>& out;
-    std::vector<Box> nbox;            // node boxes (for the parent union)
     int leaf_kind;
     int max_depth = 0;                // interior nodes on the longest root-leaf path
 
@@ -52,94 +42,7 @@ struct SahBuilder {
     }
 
     bool split(int start, int end, int& best_axis, int& mid) {   // BvhNode.cs:218-363
-        int span = end - start;
-        V3 cmin = v3(kInf), cmax = v3(-kInf);
-        for (int i = start; i < end; i++) {
-            const Box& b = boxes[idx[i]];
-            V3 c = (b.mn + b.mx) * 0.5f;
-            cmin = vmin(cmin, c);
-            cmax = vmax(cmax, c);
-        }
-        V3 ext = cmax - cmin;
-        float max_ext = fmaxf(ext.x, fmaxf(ext.y, ext.z));
-        if (max_ext <= 0.0f) {
-            best_axis = -1;
-            mid = start;
-            return false;
-        }
-        best_axis = -1;
-        int best_bin = -1;
-        float best_cost = kInf;
-        int cnt[kBins], pre_c[kBins], suf_c[kBins];
-        Box bb[kBins], pre_b[kBins], suf_b[kBins];
-        for (int ax = 0; ax < 3; ax++) {
-            float e = axis_of(ext, ax);
-            if (e <= 0.0f) continue;
-            float c0 = axis_of(cmin, ax);
-            float scale = (float)kBins / e;
-            for (int i = 0; i < kBins; i++) {
-                cnt[i] = 0;
-                bb[i] = empty_box();
-            }
-            for (int i = start; i < end; i++) {
-                const Box& b = boxes[idx[i]];
-                float c = axis_of((b.mn + b.mx) * 0.5f, ax);
-                int k = (int)((c - c0) * scale);
-                if (k < 0) k = 0;
-                else if (k >= kBins) k = kBins - 1;
-                cnt[k]++;
-                bb[k] = surround(bb[k], b);
-            }
-            int cum = 0;
-            Box cb = empty_box();
-            for (int i = 0; i < kBins; i++) {
-                cum += cnt[i];
-                cb = surround(cb, bb[i]);
-                pre_c[i] = cum;
-                pre_b[i] = cb;
-            }
-            cum = 0;
-            cb = empty_box();
-            for (int i = kBins - 1; i >= 0; i--) {
-                cum += cnt[i];
-                cb = surround(cb, bb[i]);
-                suf_c[i] = cum;
-                suf_b[i] = cb;
-            }
-            float parent = surface_area(pre_b[kBins - 1]);
-            if (parent <= 0.0f) continue;
-            for (int i = 0; i < kBins - 1; i++) {
-                int nl = pre_c[i], nr = suf_c[i + 1];
-                if (nl == 0 || nr == 0) continue;
-                float cost = 0.5f + (nl * surface_area(pre_b[i]) + nr * surface_area(suf_b[i + 1])) / parent;
-                if (cost < best_cost) {
-                    best_cost = cost;
-                    best_axis = ax;
-                    best_bin = i;
-                }
-            }
-        }
-        if (best_axis < 0) {
-            mid = start;
-            return false;
-        }
-        float amin = axis_of(cmin, best_axis);
-        float ascale = (float)kBins / axis_of(ext, best_axis);
-        int wp = start;
-        for (int i = start; i < end; i++) {
-            const Box& b = boxes[idx[i]];
-            float c = axis_of((b.mn + b.mx) * 0.5f, best_axis);
-            int k = (int)((c - amin) * ascale);
-            if (k < 0) k = 0;
-            else if (k >= kBins) k = kBins - 1;
-            if (k <= best_bin) {
-                std::swap(idx[i], idx[wp]);
-                wp++;
-            }
-        }
-        mid = wp;
-        if (mid == start || mid == end) mid = start + span / 2;
-        return true;
+        return sah_split(start, end, idx.data(), [this](int item) { return boxes[item]; }, best_axis, mid);
     }
 
     // Returns the node index (local to `out`) and its box.
@@ -170,39 +73,30 @@ struct SahBuilder {
     }
 };
 
-inline Box tri_box(V3 a, V3 b, V3 c) {   // Triangle.BoundingBox (Geometry/Triangle.cs:144-149)
-    return {vmin(vmin(a, b), c) - v3(kEps), vmax(vmax(a, b), c) + v3(kEps)};
-}
-
-struct MeshBuild {
-    std::vector<NodeF> nodes;
-    std::vector<int> order;   // local triangle ids in leaf order
-    Box box;
-    int max_depth = 0;
-    bool is_list = false;
-};
-
-void build_mesh(const float* tv, int64_t count, MeshBuild& mb) {
+void build_mesh(const float* tv, int64_t count, MeshBvh& mb) {
     std::vector<Box> boxes((size_t)count);
     for (int64_t t = 0; t < count; t++) {
         const float* p = tv + t * 9;
         boxes[t] = tri_box(v3(p[0], p[1], p[2]), v3(p[3], p[4], p[5]), v3(p[6], p[7], p[8]));
     }
+    mb.nodes.clear();
     mb.order.resize((size_t)count);
     for (int64_t t = 0; t < count; t++) mb.order[t] = (int)t;
+    Box box;
     if (count > 4) {   // Mesh.cs:93-96: BvhNode above 4 triangles
         SahBuilder sb(boxes, mb.order, mb.nodes, LEAF_TRIS);
-        sb.build(0, (int)count, 0, mb.box);
+        sb.build(0, (int)count, 0, box);
         mb.max_depth = sb.max_depth;
     } else {           // HittableList: flat scan, no box test
-        mb.is_list = true;
-        Box b = boxes[0];
-        for (int64_t t = 1; t < count; t++) b = surround(b, boxes[t]);
-        mb.box = b;
+        box = boxes[0];
+        for (int64_t t = 1; t < count; t++) box = surround(box, boxes[t]);
         NodeF n{};
-        SahBuilder::set_node(n, b, ~0, (int)count | (LEAF_LIST << 16));
+        SahBuilder::set_node(n, box, ~0, (int)count | (LEAF_LIST << 16));
         mb.nodes.push_back(n);
+        mb.max_depth = 0;
     }
+    mb.box_mn = box.mn;
+    mb.box_mx = box.mx;
 }
 
 float light_power(const Light& l, const Box& bounds) {
@@ -469,7 +363,7 @@ bool make_smooth(const RtWorldDesc* w, int64_t i, SmoothTri& st) {
 
 }  // namespace
 
-int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
+int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err, const BuildOptions& opt) {
     if (!w || w->num_materials <= 0 || w->num_entities <= 0 || !w->materials || !w->entities) {
         err = "world needs at least one material and one entity";
         return RT_ERR_INVALID_ARG;
@@ -491,7 +385,7 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
     }
     const int ne = w->num_entities;
     // --- mesh BVHs (independent; built in parallel like BvhNode's Parallel.Invoke)
-    std::vector<MeshBuild> mb((size_t)ne);
+    std::vector<MeshBvh> mb((size_t)ne);
     std::vector<int> mesh_ids;
     for (int e = 0; e < ne; e++) {
         const RtEntityDesc& d = w->entities[e];
@@ -522,13 +416,42 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
         }
     }
     {
+        auto t0 = std::chrono::steady_clock::now();
+        // Meshes of more than 4 triangles get a BvhNode tree; the device build
+        // takes those when asked, the host the rest (and all on a device error).
+        std::vector<int> host_ids;
+        std::vector<int> dev_ids;
+        std::vector<int64_t> dev_first, dev_count;
+        int64_t dev_tris = 0;
+        for (int e : mesh_ids) {
+            const RtEntityDesc& d = w->entities[e];
+            if (opt.device_builder && d.count > 4) {
+                dev_ids.push_back(e);
+                dev_first.push_back(d.first);
+                dev_count.push_back(d.count);
+                dev_tris += d.count;
+            } else {
+                host_ids.push_back(e);
+            }
+        }
+        sc.bvh_on_device = 0;
+        if (!dev_ids.empty() && dev_tris >= opt.device_min_tris) {
+            std::vector<MeshBvh> got(dev_ids.size());
+            std::string derr;
+            if (opt.device_builder(w->tri_verts, dev_first.data(), dev_count.data(), (int)dev_ids.size(), got.data(),
+                                   derr) == RT_OK) {
+                for (size_t i = 0; i < dev_ids.size(); i++) mb[dev_ids[i]] = std::move(got[i]);
+                sc.bvh_on_device = 1;
+            }
+        }
+        if (!sc.bvh_on_device) host_ids = mesh_ids;
         std::atomic<size_t> next{0};
-        unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)mesh_ids.size()));
+        unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)host_ids.size()));
         auto work = [&]() {
             for (;;) {
                 size_t k = next.fetch_add(1);
-                if (k >= mesh_ids.size()) break;
-                int e = mesh_ids[k];
+                if (k >= host_ids.size()) break;
+                int e = host_ids[k];
                 const RtEntityDesc& d = w->entities[e];
                 build_mesh(w->tri_verts + d.first * 9, d.count, mb[e]);
             }
@@ -537,6 +460,7 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
         for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
         work();
         for (auto& t : pool) t.join();
+        sc.bvh_build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     // --- entities, quads, spheres and their boxes (world objects in YAML order)
     std::vector<Box> ent_box((size_t)ne);
@@ -568,7 +492,7 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
             en.index = (int)sc.spheres.size();
             sc.spheres.push_back(s);
         } else {
-            ent_box[e] = mb[e].box;
+            ent_box[e] = {mb[e].box_mn, mb[e].box_mx};
             max_blas_depth = std::max(max_blas_depth, mb[e].max_depth);
         }
         sc.entities.push_back(en);
@@ -595,7 +519,7 @@ int build_world(const RtWorldDesc* w, HostScene& sc, std::string& err) {
     }
     // --- append mesh BVHs, relocating node and triangle indices
     for (int e : mesh_ids) {
-        MeshBuild& m = mb[e];
+        MeshBvh& m = mb[e];
         int node_base = (int)sc.nodes.size();
         int tri_base = (int)sc.tri_entity.size();
         for (NodeF n : m.nodes) {

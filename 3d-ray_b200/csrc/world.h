@@ -50,10 +50,38 @@ struct HostScene {
     V3 sky{};
     int sky_on = 0;
     int env_light = -1;
+    int bvh_on_device = 0;         // the mesh BVHs came from the device build
+    double bvh_build_ms = 0.0;     // wall time of the mesh-BVH phase
+};
+
+// One mesh's BVH in the build layout (pre-order, node indices local to the
+// mesh, leaf `first` an offset into `order`), as BvhNode's constructor makes
+// it for a mesh of more than 4 triangles (Geometry/Mesh.cs:93-96).
+struct MeshBvh {
+    std::vector<NodeF> nodes;
+    std::vector<int> order;        // mesh-local triangle ids in leaf order
+    V3 box_mn{}, box_mx{};
+    int max_depth = 0;             // interior nodes on the longest root-leaf path
+};
+
+// Builds the BVHs of `n` meshes whose triangles are tri_verts[first[i]*9 ...]
+// (count[i] > 4 each), exactly as the host build does. Returns RT_OK, or an
+// error code with a message; build_world then builds those meshes on the host.
+using MeshBvhBuilder = int (*)(const float* tri_verts, const int64_t* first, const int64_t* count, int n,
+                               MeshBvh* out, std::string& err);
+
+// The device build (bvh_build.cu): a MeshBvhBuilder on the current device.
+int device_build_meshes(const float* tri_verts, const int64_t* first, const int64_t* count, int n, MeshBvh* out,
+                        std::string& err);
+
+// Where build_world builds the mesh BVHs.
+struct BuildOptions {
+    MeshBvhBuilder device_builder = nullptr;   // null: host threads
+    int64_t device_min_tris = 0;               // use the device when the meshes hold at least this many
 };
 
 // Returns RT_OK or an RT_ERR_* code with a message in err.
-int build_world(const RtWorldDesc* w, HostScene& out, std::string& err);
+int build_world(const RtWorldDesc* w, HostScene& out, std::string& err, const BuildOptions& opt = BuildOptions{});
 
 // Kulla-Conty E(mu, alpha) / E_avg(alpha) tables
 // (Materials/EnergyCompensationLut.cs:48-74), built with the host libm.

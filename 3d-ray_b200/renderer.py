@@ -22,6 +22,7 @@ import numpy as np
 from . import abi, scenes
 
 MIS = {"balance": 0, "power": 1}
+BVH_BUILD = {"auto": 0, "host": 1, "device": 2}   # RT_BVH_*: where the mesh BVHs are built
 LIGHT_STRATEGY = {"all": 0, "power": 1, "uniform": 2}   # RT_LIGHTS_*
 KERNELS = {"megakernel": abi.KERNEL_MEGAKERNEL, "wavefront": abi.KERNEL_WAVEFRONT}
 
@@ -111,7 +112,7 @@ class Renderer:
                  max_sample_radiance: float | None = None, verbose: bool = False,
                  mis_heuristic: str = "balance", light_sampling_strategy: str = "all",
                  indirect_clamp_factor: float = DEFAULT_INDIRECT_CLAMP_FACTOR, exposure_ev: float = 0.0,
-                 kernel: str = "wavefront"):
+                 kernel: str = "wavefront", bvh_build: str = "auto"):
         if light_sampling_strategy not in LIGHT_STRATEGY:
             raise ValueError(f"unknown light strategy {light_sampling_strategy!r}")
         self.world = world
@@ -128,7 +129,9 @@ class Renderer:
         self._lib = abi.load()
         self._packed = abi.PackedWorld(world)
         h = C.c_void_p()
-        abi.check(self._lib.rt_scene_create(self._packed.ref(), C.byref(h)), "rt_scene_create")
+        opt = abi.RtSceneOptions()
+        opt.bvh_build = BVH_BUILD[bvh_build]
+        abi.check(self._lib.rt_scene_create_ex(self._packed.ref(), C.byref(opt), C.byref(h)), "rt_scene_create_ex")
         self._scene = h
         info = abi.RtSceneInfo()
         abi.check(self._lib.rt_scene_info(h, C.byref(info)))

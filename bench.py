@@ -333,6 +333,40 @@ def c1_side(rt, lib, abi):
     return out
 
 
+def bvh_build_side(lib, abi, pw):
+    """The bench scene's mesh BVHs: the device build against the host build on
+    every host thread (wall time of the mesh-BVH phase of scene creation,
+    triangle upload and node download included), and whether the two trees are
+    the same bit for bit."""
+    def export(h, info):
+        nodes = np.zeros((info.num_nodes, 8), np.int32)
+        order = np.zeros(info.num_tris, np.int32)
+        abi.check(lib.rt_scene_export_bvh(h, abi.ptr(nodes), nodes.shape[0], None, 0, abi.ptr(order), order.size))
+        return nodes, order
+
+    hinfo = abi.RtSceneInfo()
+    abi.check(lib.rt_world_inspect(pw.ref(), C.byref(hinfo), None, 0, None, 0, None, 0), "rt_world_inspect")
+    hn = np.zeros((hinfo.num_nodes, 8), np.int32)
+    ho = np.zeros(hinfo.num_tris, np.int32)
+    abi.check(lib.rt_world_inspect(pw.ref(), C.byref(hinfo), abi.ptr(hn), hn.shape[0], None, 0, abi.ptr(ho), ho.size))
+    runs = []
+    same = True
+    for _ in range(2):   # the first build in a process also loads its kernels
+        opt = abi.RtSceneOptions()
+        opt.bvh_build = abi.BVH_DEVICE
+        h = C.c_void_p()
+        abi.check(lib.rt_scene_create_ex(pw.ref(), C.byref(opt), C.byref(h)), "rt_scene_create_ex")
+        info = abi.RtSceneInfo()
+        abi.check(lib.rt_scene_info(h, C.byref(info)))
+        dn, do = export(h, info)
+        lib.rt_scene_destroy(h)
+        same = same and bool(info.bvh_on_device) and np.array_equal(dn, hn) and np.array_equal(do, ho)
+        runs.append(info.bvh_build_ms)
+    return {"triangles": int(hinfo.num_tris), "nodes": int(hinfo.num_nodes), "device_ms": runs[-1],
+            "device_first_ms": runs[0], "host_ms": hinfo.bvh_build_ms, "host_threads": os.cpu_count(),
+            "speedup": hinfo.bvh_build_ms / runs[-1], "identical": same}
+
+
 def batched_side(rt):
     """C3 (32 requests of uneven resolution, spp and depth over the icosphere
     field and the Cornell box) and C5 (eight 512x512 views of the box with the
@@ -711,6 +745,7 @@ def main():
             line["time_to_relmse_1e-3"] = time_to_relmse(rt, lib, abi)
             line.update(batched_side(rt))
             line["c1"] = c1_side(rt, lib, abi)
+            line["bvh_build"] = bvh_build_side(lib, abi, pw)
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rt, world)
     lib.rt_scene_destroy(scene)

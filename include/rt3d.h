@@ -245,11 +245,27 @@ const char* rt_last_error(void);
 int         rt_device_count(void);
 
 /* ---- scene lifetime ------------------------------------------------------ */
-/* Runs the host-side world assembly (SAH BVH build, flattening into SoA,
- * geometry-light extraction, Kulla-Conty LUT build) and uploads the result to
- * the current device. */
+/* Runs the world assembly (SAH BVH build, flattening into SoA, geometry-light
+ * extraction, Kulla-Conty LUT build) and uploads the result to the current
+ * device. The mesh BVHs are built as by rt_scene_create_ex with RT_BVH_AUTO. */
 int rt_scene_create(const RtWorldDesc* world, RtScene** out_scene);
 int rt_scene_destroy(RtScene* scene);
+
+/* Where the mesh BVHs (BvhNode's constructor for every mesh of more than 4
+ * triangles, Geometry/Mesh.cs:93-96) are built. Both builds give the same
+ * nodes, boxes and leaf order, bit for bit. */
+#define RT_BVH_AUTO   0   /* the device when the meshes hold >= RT_BVH_AUTO_MIN_TRIS triangles */
+#define RT_BVH_HOST   1   /* host threads */
+#define RT_BVH_DEVICE 2   /* the current device (the host when the device build fails) */
+#define RT_BVH_AUTO_MIN_TRIS 65536
+
+typedef struct RtSceneOptions {
+    int32_t bvh_build;            /* RT_BVH_* */
+    int32_t reserved[7];          /* zero */
+} RtSceneOptions;
+
+/* rt_scene_create with options (null: the defaults, all zero). */
+int rt_scene_create_ex(const RtWorldDesc* world, const RtSceneOptions* options, RtScene** out_scene);
 
 /* Scene summary for tests and logs. */
 typedef struct RtSceneInfo {
@@ -262,8 +278,9 @@ typedef struct RtSceneInfo {
     int32_t rr_min_bounces;       /* the reference's classifier result */
     float   rr_min_survival;
     float   mean_irradiance;      /* classifier input, Renderer.cs:361-372 */
-    int32_t pad;
+    int32_t bvh_on_device;        /* 1: the mesh BVHs came from the device build */
     int64_t device_bytes;
+    double  bvh_build_ms;         /* wall time of the mesh-BVH build */
 } RtSceneInfo;
 int rt_scene_info(const RtScene* scene, RtSceneInfo* info);
 

@@ -35,8 +35,8 @@ def test_abi_version(lib):
 @pytest.mark.parametrize("struct,size", [("RtMaterialDesc", 120), ("RtEntityDesc", 80), ("RtLightDesc", 104),
                                          ("RtCameraDesc", 48), ("RtMediumDesc", 36), ("RtRenderParams", 104),
                                          ("RtStats", 144), ("RtBsdfQuery", 96), ("RtBsdfResult", 80),
-                                         ("RtRequest", 72), ("RtSceneInfo", 56), ("RtWorldDesc", 184),
-                                         ("RtCapture", 64)])
+                                         ("RtRequest", 72), ("RtSceneInfo", 64), ("RtWorldDesc", 184),
+                                         ("RtCapture", 64), ("RtSceneOptions", 32)])
 def test_struct_sizes(struct, size):
     """Sizes of the C structs (checked against the header by the C compiler in
     the build: see the static_asserts in kernels.cu)."""
