@@ -32,9 +32,14 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -520,21 +525,70 @@ __global__ void k_emit_small(int count, Buffers B) {
     }
 }
 
+// RT3D_BVH_TIMING=1 prints the build's phases (host wall time) to stderr.
+struct PhaseLog {
+    bool on = getenv("RT3D_BVH_TIMING") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void mark(const char* what) {
+        if (!on) return;
+        auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "bvh_build %-10s %8.3f ms\n", what, std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
+
 inline unsigned blocks(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
-struct Pool {   // device allocations of one build, freed together
+// The build's scratch comes from a private stream-ordered pool per device.
+// The pool keeps up to kPoolKeep bytes reserved after a build (about 380 B
+// per triangle are needed), so a later build in the process skips the
+// allocation and frees never synchronise the device.
+constexpr uint64_t kPoolKeep = 1ull << 30;
+
+cudaError_t build_pool(int dev, cudaMemPool_t* out) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p;
+    cudaError_t e = cudaMemPoolCreate(&p, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = kPoolKeep;
+    e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+        cudaMemPoolDestroy(p);
+        return e;
+    }
+    pools[dev] = p;
+    *out = p;
+    return cudaSuccess;
+}
+
+struct Pool {   // device allocations of one build, stream-ordered, freed together
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
     std::vector<void*> ptrs;
     template <class T>
     cudaError_t get(T** p, size_t count) {
         void* v = nullptr;
-        cudaError_t e = cudaMalloc(&v, std::max<size_t>(count, 1) * sizeof(T));
+        cudaError_t e = cudaMallocFromPoolAsync(&v, std::max<size_t>(count, 1) * sizeof(T), pool, stream);
         if (e == cudaSuccess) ptrs.push_back(v);
         *p = (T*)v;
         return e;
     }
-    ~Pool() {
-        for (void* v : ptrs) cudaFree(v);
+    void release() {
+        for (void* v : ptrs) cudaFreeAsync(v, stream);
+        ptrs.clear();
     }
+    ~Pool() { release(); }
 };
 
 }  // namespace
@@ -563,7 +617,21 @@ int device_build_meshes(const float* tri_verts, const int64_t* first, const int6
         return RT_ERR_INVALID_ARG;
     }
     const int n = (int)total;
+    PhaseLog log;
+    int dev = 0;
+    BV_TRY(cudaGetDevice(&dev));
+    cudaStream_t st = nullptr;
+    BV_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {   // declared before the pool: destroyed after its frees are queued
+        cudaStream_t s;
+        ~StreamGuard() {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    } guard{st};
     Pool pool;
+    pool.stream = st;
+    BV_TRY(build_pool(dev, &pool.pool));
     Buffers B;
     B.n = n;
     B.meshes = meshes;
@@ -606,16 +674,7 @@ int device_build_meshes(const float* tri_verts, const int64_t* first, const int6
     BV_TRY(pool.get(&B.ctl, 1));
     BV_TRY(cub::DeviceScan::ExclusiveSum(nullptr, B.scan_bytes, B.flag, B.rank, n));
     BV_TRY(pool.get(&B.scan_tmp, B.scan_bytes));
-
-    cudaStream_t st = nullptr;
-    BV_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() {
-            cudaStreamSynchronize(s);
-            cudaStreamDestroy(s);
-        }
-    } guard{st};
+    log.mark("alloc");
 
     std::vector<int> mesh_pos(meshes);
     {
@@ -639,6 +698,7 @@ int device_build_meshes(const float* tri_verts, const int64_t* first, const int6
         err = "device BVH build: a vertex coordinate is not finite";
         return RT_ERR_UNSUPPORTED;
     }
+    log.mark("upload");
     k_init_positions<<<blocks(n, 256), 256, 0, st>>>(n, B);
     if (ctl.next_act > 0) k_root_positions<<<ctl.next_act, 256, 0, st>>>(B);
     BV_TRY(cudaGetLastError());
@@ -691,6 +751,7 @@ int device_build_meshes(const float* tri_verts, const int64_t* first, const int6
     }
     const int levels = level;
     const int n_large = lvl_off.back();
+    log.mark("levels");
 
     // --- small subtrees, subtree sizes, pre-order indices
     k_small<<<blocks(small_count, 128), 128, 0, st>>>(small_count, B);
@@ -710,6 +771,7 @@ int device_build_meshes(const float* tri_verts, const int64_t* first, const int6
     BV_TRY(cudaMemcpyAsync(root_hi.data(), B.n_hi, meshes * sizeof(float4), cudaMemcpyDeviceToHost, st));
     BV_TRY(cudaMemcpyAsync(mesh_depth.data(), B.mesh_depth, meshes * sizeof(int), cudaMemcpyDeviceToHost, st));
     BV_TRY(cudaStreamSynchronize(st));
+    log.mark("small");
     std::vector<int> mesh_base(meshes);
     int64_t total_nodes = 0;
     for (int m = 0; m < meshes; m++) {
@@ -726,6 +788,7 @@ int device_build_meshes(const float* tri_verts, const int64_t* first, const int6
     BV_TRY(cudaMemcpyAsync(all.data(), B.out, (size_t)total_nodes * sizeof(NodeF), cudaMemcpyDeviceToHost, st));
     BV_TRY(cudaMemcpyAsync(order.data(), B.order, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
     BV_TRY(cudaStreamSynchronize(st));
+    log.mark("download");
     for (int m = 0; m < meshes; m++) {
         MeshBvh& mb = out[m];
         mb.nodes.assign(all.begin() + mesh_base[m], all.begin() + mesh_base[m] + root_size[m]);
@@ -735,6 +798,10 @@ int device_build_meshes(const float* tri_verts, const int64_t* first, const int6
         mb.box_mx = v3(root_hi[m].x, root_hi[m].y, root_hi[m].z);
         mb.max_depth = mesh_depth[m];
     }
+    log.mark("unpack");
+    pool.release();
+    BV_TRY(cudaStreamSynchronize(st));
+    log.mark("free");
     return RT_OK;
 #undef BV_TRY
 }

@@ -570,6 +570,9 @@ def main():
     ap.add_argument("--res", type=int, default=256, help="--fit: square image size")
     ap.add_argument("--gradcheck", action="store_true",
                     help="adjoint gradients against central finite differences (C4, C5) and exit")
+    ap.add_argument("--bvh-build", action="store_true",
+                    help="build the bench scene's mesh BVHs on the host and twice on the device, print the timings "
+                         "and exit (the command profiled by ncu for the device build)")
     ap.add_argument("--profile-frame", action="store_true",
                     help="render the frame twice with fixed settings and exit (the command profiled by ncu)")
     args = ap.parse_args()
@@ -577,6 +580,11 @@ def main():
         return run_reference(args)
     if args.profile_frame:
         return profile_frame(args)
+    if args.bvh_build:
+        rt, world = build_world()
+        lib = rt.abi.load()
+        print(json.dumps(bvh_build_side(lib, rt.abi, rt.abi.PackedWorld(world))), flush=True)
+        return
     if args.gradcheck:
         return gradcheck(args)
     if args.fit:
