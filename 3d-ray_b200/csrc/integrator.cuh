@@ -182,7 +182,9 @@ RT_D V3 path_resolve(const PathState& ps, const RenderConst& rc) {
 // reference casts it first; only the cost differs: every draw happens in the
 // light sampler). Each unoccluded sample adds w * colour * brdf * Tr_medium,
 // times the vertex weight, through the sink.
-template <class Sink>
+// MEDIUM = false compiles the participating-medium terms out (a batch none of
+// whose scenes has a medium).
+template <bool MEDIUM = true, class Sink>
 RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, const Surface& rec,
                       const Material& m, V3 view, Sink& sink) {
     float view_term = shadow_terminator(rec.n, rec.n, view);
@@ -208,7 +210,7 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
                 continue;
             }
             V3 tr_m = v3(1.0f);
-            if (s.has_medium) tr_m = medium_tr(s, ls.dist >= kInf ? 1e30f : ls.dist);
+            if (MEDIUM && s.has_medium) tr_m = medium_tr(s, ls.dist >= kInf ? 1e30f : ls.dist);
             float wgt = 1.0f;
             if (!l.is_delta) {
                 float pb = bsdf_pdf(m, rec, view, ls.dir);
@@ -315,14 +317,15 @@ struct NoAdjoint {
 // One vertex of TraceRay given the closest hit of the current ray: the
 // volumetric branch (Renderer.cs:1704-1782), ShadeSurface (:1008-1228) and
 // ShadeSampleBounce (:1235-1383). Returns true when the path continues with
-// ps.o/ps.d as the next ray (ps.depth already decremented).
-template <class Sink>
+// ps.o/ps.d as the next ray (ps.depth already decremented). MEDIUM = false
+// compiles the volumetric branch out.
+template <bool MEDIUM = true, class Sink>
 __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderConst& rc, PathState& ps, const Hit& h,
                                              Sink& sink) {
     bool hit = h.kind != HIT_NONE;
     V3 beta_s = ps.beta;
     sink.aov_ray(h, ps.d);
-    if (s.has_medium) {
+    if (MEDIUM && s.has_medium) {
         float tmax = hit ? h.t : 1e30f;
         float tmed;
         V3 mb;
@@ -385,7 +388,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
     float rel_eta = 0.0f;
     bool dielectric = !m.thin_walled && m.spec_trans_raw > 0.0f;
     if (dielectric) rel_eta = rec.front ? (ps.iors.top() / m.ior_raw) : (m.ior_raw / ps.iors.enclosing());
-    nee_surface(s, rc, ps, rec, m, view, sink);
+    nee_surface<MEDIUM>(s, rc, ps, rec, m, view, sink);
     BsdfSample bs;
     V3 att, next_o, next_d, next_beta;
     float next_pdf;
