@@ -998,6 +998,10 @@ RT_D bool any_nonfinite(V3 a) { return !isfinite(a.x) || !isfinite(a.y) || !isfi
 // ScatterInternal (:1176-1248) with the lobe samplers (:1263-1709). ray_dir is
 // the incoming ray direction; V = normalize(-ray_dir). When a reflection lobe
 // fails, *tried (if given) receives the direction it drew.
+// TRANSMIT = false compiles the specular-transmission lobe out, for batches in
+// which no material has specTrans > 0: there p_t is exactly 0, so the lobe is
+// never picked and subtracting p_t leaves the draw unchanged.
+template <bool TRANSMIT = true>
 RT_D bool bsdf_scatter(const SceneView& s, const Material& m, const Surface& rec, V3 ray_dir, float relative_eta,
                        Sampler& rng, V3& att, V3& dir, int& lobe, V3* tried = nullptr) {
     V3 bc = m.base;
@@ -1045,7 +1049,7 @@ RT_D bool bsdf_scatter(const SceneView& s, const Material& m, const Surface& rec
             att = fres * g1l;
             att = att / fmaxf(m.p_s, 0.1f);
         }
-    } else if ((rnd -= m.p_s) < m.p_t) {   // ScatterTransmission (:1473-1608)
+    } else if ((rnd -= m.p_s), TRANSMIT && rnd < m.p_t) {   // ScatterTransmission (:1473-1608)
         lobe = LOBE_TRANSMISSION;
         bool thin = m.thin_walled != 0;
         float eta = thin ? (1.0f / m.ior) : (relative_eta > 0.0f ? relative_eta : (rec.front ? (1.0f / m.ior) : m.ior));
@@ -1169,6 +1173,7 @@ struct BsdfSample {
 };
 
 // Sample (:893-997). Returns false for a null sample.
+template <bool TRANSMIT = true>
 RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec, V3 V, float relative_eta,
                       Sampler& rng, BsdfSample& out) {
     V3 att, wo;
@@ -1176,7 +1181,7 @@ RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec,
     out.transition = 0;
     out.has_next_absorption = 0;
     out.tried = rec.n;
-    bool ok = bsdf_scatter(s, m, rec, -V, relative_eta, rng, att, wo, lobe, &out.tried);
+    bool ok = bsdf_scatter<TRANSMIT>(s, m, rec, -V, relative_eta, rng, att, wo, lobe, &out.tried);
     out.lobe = lobe;
     if (!ok) return false;
     float ndwo = dot(rec.n, wo);
@@ -1195,7 +1200,7 @@ RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec,
         out.is_delta = 0;
         return true;
     }
-    if (lobe == LOBE_TRANSMISSION) {
+    if (TRANSMIT && lobe == LOBE_TRANSMISSION) {
         if (ndwo < 0.0f && !m.thin_walled) {
             V3 sg = m.trans_sigma;
             bool has_sigma = sg.x > 0.0f || sg.y > 0.0f || sg.z > 0.0f;

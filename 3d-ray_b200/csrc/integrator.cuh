@@ -318,8 +318,9 @@ struct NoAdjoint {
 // volumetric branch (Renderer.cs:1704-1782), ShadeSurface (:1008-1228) and
 // ShadeSampleBounce (:1235-1383). Returns true when the path continues with
 // ps.o/ps.d as the next ray (ps.depth already decremented). MEDIUM = false
-// compiles the volumetric branch out.
-template <bool MEDIUM = true, class Sink>
+// compiles the volumetric branch out; TRANSMIT = false the specular
+// transmission lobe and the IOR stack (no material has specTrans > 0).
+template <bool MEDIUM = true, bool TRANSMIT = true, class Sink>
 __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderConst& rc, PathState& ps, const Hit& h,
                                              Sink& sink) {
     bool hit = h.kind != HIT_NONE;
@@ -386,14 +387,14 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
     }
     V3 view = normalize(-ps.d);
     float rel_eta = 0.0f;
-    bool dielectric = !m.thin_walled && m.spec_trans_raw > 0.0f;
+    bool dielectric = TRANSMIT && !m.thin_walled && m.spec_trans_raw > 0.0f;
     if (dielectric) rel_eta = rec.front ? (ps.iors.top() / m.ior_raw) : (m.ior_raw / ps.iors.enclosing());
     nee_surface<MEDIUM>(s, rc, ps, rec, m, view, sink);
     BsdfSample bs;
     V3 att, next_o, next_d, next_beta;
     float next_pdf;
     int next_delta;
-    if (bsdf_sample(s, m, rec, view, rel_eta, ps.rng, bs)) {   // ShadeSampleBounce
+    if (bsdf_sample<TRANSMIT>(s, m, rec, view, rel_eta, ps.rng, bs)) {   // ShadeSampleBounce
         if (bs.is_delta) {
             att = bs.f;
         } else {
@@ -416,12 +417,12 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
             ps.cur_abs = bs.next_absorption;
             sink.interior(near_zero(bs.next_absorption) ? -1 : rec.material);
         }
-        if (rc.dielectrics && bs.transition == 1) ps.iors.push(dielectric ? m.ior_raw : ps.iors.top());
-        if (rc.dielectrics && bs.transition == 2) ps.iors.pop();
+        if (TRANSMIT && rc.dielectrics && bs.transition == 1) ps.iors.push(dielectric ? m.ior_raw : ps.iors.top());
+        if (TRANSMIT && rc.dielectrics && bs.transition == 2) ps.iors.pop();
     } else {   // Sample returned null: the legacy Scatter path (:1127-1225)
         V3 sdir;
         int lobe;
-        if (!bsdf_scatter(s, m, rec, ps.d, rel_eta, ps.rng, att, sdir, lobe)) return false;
+        if (!bsdf_scatter<TRANSMIT>(s, m, rec, ps.d, rel_eta, ps.rng, att, sdir, lobe)) return false;
         sink.aov_bounce(false, att);   // Disney's IsDeltaScatter is false
         next_beta = beta_s * att;
         V3 att_pre = att;

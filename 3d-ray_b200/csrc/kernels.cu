@@ -833,8 +833,11 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     for (const HostReq& q : reqs) l4 = l4 && q.scene->host.max_stack4 <= kStack;
     bool pt = !l4 && cfg.fetch == 2;
     int groups = cfg.groups > 0 ? cfg.groups : default_groups(scenes);
-    bool medium = false;   // shade compiled with the volumetric branch only when a scene needs it
+    // shade is compiled with the volumetric branch and the transmission lobe
+    // only when a scene of the batch needs them
+    bool medium = false;
     for (const RtScene* sc : scenes) medium = medium || sc->host.has_medium;
+    const bool transmit = !a.opaque;
     a.regroup = groups == 2;
     a.raysort = groups >= 3 && !pt;
     a.shadowsort = groups == 4 && !pt;
@@ -872,8 +875,10 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
             rt::k_wf_scatter<<<g256, 256, 0, stream>>>(a);
         }
         if (ev) cudaEventRecord(ev[3], stream);
-        if (medium) rt::k_wf_shade<true><<<gs, blk, 0, stream>>>(a);
-        else rt::k_wf_shade<false><<<gs, blk, 0, stream>>>(a);
+        if (medium && transmit) rt::k_wf_shade<true, true><<<gs, blk, 0, stream>>>(a);
+        else if (medium) rt::k_wf_shade<true, false><<<gs, blk, 0, stream>>>(a);
+        else if (transmit) rt::k_wf_shade<false, true><<<gs, blk, 0, stream>>>(a);
+        else rt::k_wf_shade<false, false><<<gs, blk, 0, stream>>>(a);
         if (a.raysort) rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.rhist, a.roff, &d_ctl->nbounce);
         if (a.shadowsort) {
             rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.shist, a.soff, &d_ctl->nshadow);

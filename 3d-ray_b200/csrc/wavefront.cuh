@@ -568,7 +568,7 @@ struct QueueShadows : NoAdjoint {
 #ifndef RT_SHADE_MIN_BLOCKS
 #define RT_SHADE_MIN_BLOCKS 2
 #endif
-template <bool MEDIUM>
+template <bool MEDIUM, bool TRANSMIT>
 __global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int i;
@@ -598,7 +598,7 @@ __global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a)
     h.kind = packed == 0 ? HIT_NONE : ((unsigned)packed >> 30);
     h.slot = packed & 0x3FFFFFFF;
     QueueShadows sink{{}, &a, i, R.scene};
-    bool alive = shade_vertex<MEDIUM>(s, R.rc, ps, h, sink);
+    bool alive = shade_vertex<MEDIUM, TRANSMIT>(s, R.rc, ps, h, sink);
     wf_store(a, i, ps, wf_flags(ps, alive), req, pix);
     wf_store_media(a, i, R, ps);
     if (a.raysort && alive) {   // the continued ray's sort key and its rank in the key's count
