@@ -1186,52 +1186,51 @@ RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec,
     if (!ok) return false;
     float ndwo = dot(rec.n, wo);
     out.wo = wo;
-    if (lobe == LOBE_DIFFTRANS) {
-        V3 fb = bsdf_eval(s, m, rec, V, wo);
-        float pb = bsdf_pdf(m, rec, V, wo);
-        if (pb <= 0.0f) {
+    // Diffuse transmission and the non-delta reflection lobes both end in
+    // Evaluate + Pdf; one call site serves both (the code is long).
+    bool dt = lobe == LOBE_DIFFTRANS;
+    if (!dt) {
+        if (TRANSMIT && lobe == LOBE_TRANSMISSION) {
+            if (ndwo < 0.0f && !m.thin_walled) {
+                V3 sg = m.trans_sigma;
+                bool has_sigma = sg.x > 0.0f || sg.y > 0.0f || sg.z > 0.0f;
+                if (rec.front && has_sigma) {
+                    out.has_next_absorption = 1;
+                    out.next_absorption = sg;
+                } else if (!rec.front) {
+                    out.has_next_absorption = 1;
+                    out.next_absorption = v3(0.0f);
+                }
+                out.transition = rec.front ? 1 : 2;
+            }
             out.f = att;
             out.pdf = 1.0f;
             out.is_delta = 1;
             return true;
         }
-        out.f = fb;
-        out.pdf = pb;
-        out.is_delta = 0;
-        return true;
-    }
-    if (TRANSMIT && lobe == LOBE_TRANSMISSION) {
-        if (ndwo < 0.0f && !m.thin_walled) {
-            V3 sg = m.trans_sigma;
-            bool has_sigma = sg.x > 0.0f || sg.y > 0.0f || sg.z > 0.0f;
-            if (rec.front && has_sigma) {
-                out.has_next_absorption = 1;
-                out.next_absorption = sg;
-            } else if (!rec.front) {
-                out.has_next_absorption = 1;
-                out.next_absorption = v3(0.0f);
-            }
-            out.transition = rec.front ? 1 : 2;
+        if (ndwo <= 0.0f) {
+            out.tried = wo;
+            return false;
         }
+        bool nd_spec = lobe == LOBE_SPECULAR && m.alpha <= kDeltaAlpha;
+        bool nd_coat = lobe == LOBE_CLEARCOAT && m.cc_alpha <= kDeltaAlpha;
+        if (nd_spec || nd_coat) {
+            out.f = att;
+            out.pdf = 1.0f;
+            out.is_delta = 1;
+            return true;
+        }
+    }
+    V3 fb = bsdf_eval(s, m, rec, V, wo);
+    float pb = bsdf_pdf(m, rec, V, wo);
+    if (dt && pb <= 0.0f) {   // a diffuse-transmission direction of zero density: a delta with its weight
         out.f = att;
         out.pdf = 1.0f;
         out.is_delta = 1;
         return true;
     }
-    if (ndwo <= 0.0f) {
-        out.tried = wo;
-        return false;
-    }
-    bool nd_spec = lobe == LOBE_SPECULAR && m.alpha <= kDeltaAlpha;
-    bool nd_coat = lobe == LOBE_CLEARCOAT && m.cc_alpha <= kDeltaAlpha;
-    if (nd_spec || nd_coat) {
-        out.f = att;
-        out.pdf = 1.0f;
-        out.is_delta = 1;
-        return true;
-    }
-    out.f = bsdf_eval(s, m, rec, V, wo);
-    out.pdf = bsdf_pdf(m, rec, V, wo);
+    out.f = fb;
+    out.pdf = pb;
     out.is_delta = 0;
     return true;
 }
