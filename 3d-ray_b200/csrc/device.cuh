@@ -1172,18 +1172,11 @@ struct BsdfSample {
     V3 tried;                  // a null sample: the direction its lobe drew
 };
 
-// Sample (:893-997). Returns false for a null sample.
+// The rest of Sample (:893-997) once ScatterInternal has drawn (att, wo) with
+// `lobe`. Returns false for a null sample.
 template <bool TRANSMIT = true>
-RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec, V3 V, float relative_eta,
-                      Sampler& rng, BsdfSample& out) {
-    V3 att, wo;
-    int lobe = -1;
-    out.transition = 0;
-    out.has_next_absorption = 0;
-    out.tried = rec.n;
-    bool ok = bsdf_scatter<TRANSMIT>(s, m, rec, -V, relative_eta, rng, att, wo, lobe, &out.tried);
-    out.lobe = lobe;
-    if (!ok) return false;
+RT_D bool bsdf_sample_finish(const SceneView& s, const Material& m, const Surface& rec, V3 V, V3 att, V3 wo, int lobe,
+                             BsdfSample& out) {
     float ndwo = dot(rec.n, wo);
     out.wo = wo;
     // Diffuse transmission and the non-delta reflection lobes both end in
@@ -1233,6 +1226,53 @@ RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec,
     out.pdf = pb;
     out.is_delta = 0;
     return true;
+}
+
+// Sample (:893-997). Returns false for a null sample.
+template <bool TRANSMIT = true>
+RT_D bool bsdf_sample(const SceneView& s, const Material& m, const Surface& rec, V3 V, float relative_eta,
+                      Sampler& rng, BsdfSample& out) {
+    V3 att, wo;
+    int lobe = -1;
+    out.transition = 0;
+    out.has_next_absorption = 0;
+    out.tried = rec.n;
+    bool ok = bsdf_scatter<TRANSMIT>(s, m, rec, -V, relative_eta, rng, att, wo, lobe, &out.tried);
+    out.lobe = lobe;
+    if (!ok) return false;
+    return bsdf_sample_finish<TRANSMIT>(s, m, rec, V, att, wo, lobe, out);
+}
+
+// ShadeSampleBounce's draw: Sample, and when it returns null the legacy
+// Scatter draw the renderer falls back to (Renderer.cs:1127-1225), with fresh
+// random numbers and the ray direction itself. Both draws go through one
+// bsdf_scatter call site, so its long lobe samplers are compiled once.
+// Returns 1 with `out` filled (a sample), 2 with (latt, ldir, llobe) (the
+// legacy draw; out.lobe and out.tried describe the null sample), 0 when both
+// fail.
+template <bool TRANSMIT = true>
+RT_D int bsdf_sample_or_scatter(const SceneView& s, const Material& m, const Surface& rec, V3 V, V3 ray_dir,
+                                float relative_eta, Sampler& rng, BsdfSample& out, V3& latt, V3& ldir, int& llobe) {
+    out.transition = 0;
+    out.has_next_absorption = 0;
+    out.tried = rec.n;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {
+        V3 att, wo;
+        int lobe = -1;
+        bool ok = bsdf_scatter<TRANSMIT>(s, m, rec, pass == 0 ? -V : ray_dir, relative_eta, rng, att, wo, lobe,
+                                         pass == 0 ? &out.tried : nullptr);
+        if (pass == 1) {
+            if (!ok) return 0;
+            latt = att;
+            ldir = wo;
+            llobe = lobe;
+            return 2;
+        }
+        out.lobe = lobe;
+        if (ok && bsdf_sample_finish<TRANSMIT>(s, m, rec, V, att, wo, lobe, out)) return 1;
+    }
+    return 0;
 }
 
 // ShadowTransmittance (:560-584) and ShadowAbsorption (:609-614).

@@ -394,7 +394,10 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
     V3 att, next_o, next_d, next_beta;
     float next_pdf;
     int next_delta;
-    if (bsdf_sample<TRANSMIT>(s, m, rec, view, rel_eta, ps.rng, bs)) {   // ShadeSampleBounce
+    V3 latt, ldir;
+    int llobe = -1;
+    int drawn = bsdf_sample_or_scatter<TRANSMIT>(s, m, rec, view, ps.d, rel_eta, ps.rng, bs, latt, ldir, llobe);
+    if (drawn == 1) {   // ShadeSampleBounce
         if (bs.is_delta) {
             att = bs.f;
         } else {
@@ -420,9 +423,10 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         if (TRANSMIT && rc.dielectrics && bs.transition == 1) ps.iors.push(dielectric ? m.ior_raw : ps.iors.top());
         if (TRANSMIT && rc.dielectrics && bs.transition == 2) ps.iors.pop();
     } else {   // Sample returned null: the legacy Scatter path (:1127-1225)
-        V3 sdir;
-        int lobe;
-        if (!bsdf_scatter<TRANSMIT>(s, m, rec, ps.d, rel_eta, ps.rng, att, sdir, lobe)) return false;
+        if (drawn == 0) return false;
+        V3 sdir = ldir;
+        int lobe = llobe;
+        att = latt;
         sink.aov_bounce(false, att);   // Disney's IsDeltaScatter is false
         next_beta = beta_s * att;
         V3 att_pre = att;
