@@ -98,8 +98,10 @@ struct WfArgs {
     const int* key_base;   // per scene: first key
     int regroup;      // extend/occlude regroup their block's rays by kind (block_group)
     int raysort;      // extend walks bounce rays sorted by ray_key, then camera rays in pixel order
-    int rkey_bits;    // ray_key: origin cell bits per axis (0 .. 4)
-    int rdir_bits;    // ray_key: direction bits (0, 3: octant, or an even count up to 8)
+    int rkey_bits;    // ray_key of bounce rays: origin cell bits per axis (0 .. 4)
+    int rdir_bits;    // ray_key of bounce rays: direction bits (0, 3: octant, or an even count up to 8)
+    int skey_bits;    // the same two for shadow records
+    int sdir_bits;
     int* rhist;       // kRayKeys: bounce rays per key (filled by shade)
     int* roff;        // kRayKeys: the keys' first positions in order (the scanned histogram)
     int shadowsort;   // occlude walks the shadow records sorted by ray_key
@@ -551,7 +553,7 @@ struct QueueShadows : NoAdjoint {
         a->S.d[j] = make_float4(d.x, d.y, d.z, ibits((slot << 1) | to_la));
         a->S.c[j] = make_float4(c.x, c.y, c.z, ibits(scene));
         if (a->shadowsort) {   // the record's sort key and its rank in the key's count
-            int key = ray_key(a->views[scene], o, d, a->rkey_bits, a->rdir_bits);
+            int key = ray_key(a->views[scene], o, d, a->skey_bits, a->sdir_bits);
             unsigned grp = __match_any_sync(__activemask(), key);
             int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
             int base = 0;
