@@ -355,8 +355,7 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                                          TravCounters* cnt, int* err, bool has_root = false, int root = 0) {
     const int kNone = INT_MIN;   // "pop the next entry" (no leaf code can take this value)
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
-    int st_code[STACK];
-    float st_te[STACK];
+    int2 st[STACK];   // (code, entry distance bits): one 8-byte access per push and pop
     int sp = 0;
     float closest = tmax;
     best.kind = HIT_NONE;
@@ -369,9 +368,7 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
         if (cnt) cnt->nodes++;                // the world root's BvhNode.Hit
     } else {
         for (int i = s.num_top_items - 1; i >= 0; --i) {
-            st_code[sp] = leaf_code(s.top_items[i], LEAF_ENT1, 1);
-            st_te[sp] = -kInf;
-            sp++;
+            st[sp++] = make_int2(leaf_code(s.top_items[i], LEAF_ENT1, 1), __float_as_int(-kInf));
         }
     }
     for (;;) {
@@ -395,9 +392,7 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                     *err = RT_ERR_STACK;
                     return false;
                 }
-                st_code[sp] = fc;
-                st_te[sp] = tf;
-                sp++;
+                st[sp++] = make_int2(fc, __float_as_int(tf));
             }
             code = hn ? nc : (hf ? fc : kNone);
         }
@@ -437,11 +432,8 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                     *err = RT_ERR_STACK;
                     return false;
                 }
-                for (int i = count - 1; i >= 0; --i) {
-                    st_code[sp] = leaf_code(s.top_items[first + i], LEAF_ENT1, 1);
-                    st_te[sp] = -kInf;
-                    sp++;
-                }
+                for (int i = count - 1; i >= 0; --i)
+                    st[sp++] = make_int2(leaf_code(s.top_items[first + i], LEAF_ENT1, 1), __float_as_int(-kInf));
             } else {   // triangle leaf (or a mesh's flat list)
                 for (int i = 0; i < count; i++) {
                     float t, u, vv;
@@ -456,9 +448,9 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
         }
         // Pop the next entry the current closest t does not prune.
         while (sp > 0) {
-            --sp;
-            if (!(st_te[sp] > closest)) {
-                code = st_code[sp];
+            int2 e = st[--sp];
+            if (!(__int_as_float(e.y) > closest)) {
+                code = e.x;
                 break;
             }
         }
