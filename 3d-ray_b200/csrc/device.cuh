@@ -355,8 +355,16 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                                          TravCounters* cnt, int* err, bool has_root = false, int root = 0) {
     const int kNone = INT_MIN;   // "pop the next entry" (no leaf code can take this value)
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
-    int2 st[STACK];   // (code, entry distance bits): one 8-byte access per push and pop
+    // (code, entry distance bits): one 8-byte access per push and pop. An
+    // any-hit walk returns at its first hit, so its closest t stays tmax and no
+    // entry is ever pruned at pop time: it keeps the codes alone.
+    int2 st[ANY ? 1 : STACK];
+    int stc[ANY ? STACK : 1];
     int sp = 0;
+    auto push = [&](int c, float te) {
+        if (ANY) stc[sp++] = c;
+        else st[sp++] = make_int2(c, __float_as_int(te));
+    };
     float closest = tmax;
     best.kind = HIT_NONE;
     int code = kNone;
@@ -368,7 +376,7 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
         if (cnt) cnt->nodes++;                // the world root's BvhNode.Hit
     } else {
         for (int i = s.num_top_items - 1; i >= 0; --i) {
-            st[sp++] = make_int2(leaf_code(s.top_items[i], LEAF_ENT1, 1), __float_as_int(-kInf));
+            push(leaf_code(s.top_items[i], LEAF_ENT1, 1), -kInf);
         }
     }
     for (;;) {
@@ -392,7 +400,7 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                     *err = RT_ERR_STACK;
                     return false;
                 }
-                st[sp++] = make_int2(fc, __float_as_int(tf));
+                push(fc, tf);
             }
             code = hn ? nc : (hf ? fc : kNone);
         }
@@ -432,8 +440,7 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                     *err = RT_ERR_STACK;
                     return false;
                 }
-                for (int i = count - 1; i >= 0; --i)
-                    st[sp++] = make_int2(leaf_code(s.top_items[first + i], LEAF_ENT1, 1), __float_as_int(-kInf));
+                for (int i = count - 1; i >= 0; --i) push(leaf_code(s.top_items[first + i], LEAF_ENT1, 1), -kInf);
             } else {   // triangle leaf (or a mesh's flat list)
                 for (int i = 0; i < count; i++) {
                     float t, u, vv;
@@ -447,11 +454,15 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
             }
         }
         // Pop the next entry the current closest t does not prune.
-        while (sp > 0) {
-            int2 e = st[--sp];
-            if (!(__int_as_float(e.y) > closest)) {
-                code = e.x;
-                break;
+        if (ANY) {
+            if (sp > 0) code = stc[--sp];
+        } else {
+            while (sp > 0) {
+                int2 e = st[--sp];
+                if (!(__int_as_float(e.y) > closest)) {
+                    code = e.x;
+                    break;
+                }
             }
         }
         if (code == kNone) return true;
