@@ -892,9 +892,11 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
             rt::k_wf_sscatter<<<gsh256, 256, 0, stream>>>(a);
         }
         if (ev) cudaEventRecord(ev[4], stream);
-        if (l4) rt::k_wf_occlude<kStack, true><<<gsh, tblk, 0, stream>>>(a);
+        if (l4 && a.opaque) rt::k_wf_occlude<kStack, true, true><<<gsh, tblk, 0, stream>>>(a);
+        else if (l4) rt::k_wf_occlude<kStack, true, false><<<gsh, tblk, 0, stream>>>(a);
         else if (pt && a.opaque) rt::k_wf_occlude_pt<kStack><<<gpt_o, tblk, 0, stream>>>(a);
-        else rt::k_wf_occlude<kStack, false><<<gsh, tblk, 0, stream>>>(a);
+        else if (a.opaque) rt::k_wf_occlude<kStack, false, true><<<gsh, tblk, 0, stream>>>(a);
+        else rt::k_wf_occlude<kStack, false, false><<<gsh, tblk, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[5], stream);
     };
     const int batch = 4;
