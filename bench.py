@@ -721,7 +721,7 @@ def main():
                 l2_bytes = float(line.split(":")[1])
     roof["traffic"] = traffic
     # L2 roofline beside the HBM one: the scene is largely L2-resident, so the
-    # traversal kernels are judged against L2 bandwidth too. The peak is a
+    # traversal kernels are compared against L2 bandwidth too. The peak is a
     # project micro-benchmark (L2-only float4 streams over a 32 MiB buffer).
     l2_peak = C.c_double(0.0)
     if lib.rt_probe_l2_bandwidth(dev, 32 << 20, 64, C.byref(l2_peak)) == abi.RT_OK:
