@@ -15,7 +15,10 @@ import numpy as np
 from . import scenes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "librt3d.so")
+# RT3D_LIB selects another build of the same ABI, e.g. lib/librt3d_checked.so
+# (every kernel index range-checked) for a run of the test suite.
+LIB_PATH = os.environ.get("RT3D_LIB") or os.path.join(HERE, "lib", "librt3d.so")
+CHECKED_LIB_PATH = os.path.join(HERE, "lib", "librt3d_checked.so")
 
 RT_OK = 0
 ERRORS = {-1: "RT_ERR_INVALID_ARG", -2: "RT_ERR_OOM", -3: "RT_ERR_CUDA", -4: "RT_ERR_TIMEOUT",
@@ -89,7 +92,7 @@ class RtRenderParams(C.Structure):
                 ("sort_materials", C.c_int32), ("pixel_x0", C.c_int32), ("pixel_y0", C.c_int32),
                 ("window_w", C.c_int32), ("window_h", C.c_int32), ("count_work", C.c_int32), ("profile_kernels", C.c_int32),
                 ("node_layout", C.c_int32), ("ray_fetch", C.c_int32), ("trace_block_size", C.c_int32),
-                ("ray_groups", C.c_int32)]
+                ("ray_groups", C.c_int32), ("iteration_limit", C.c_int32), ("shadow_queue_limit", C.c_int32)]
 
 
 class RtStats(C.Structure):
@@ -136,7 +139,17 @@ class RtBsdfQuery(C.Structure):
 class RtBsdfResult(C.Structure):
     _fields_ = [("f", F3), ("pdf", C.c_float), ("fd", F3), ("pad0", C.c_float), ("wo", F3),
                 ("s_pdf", C.c_float), ("s_f", F3), ("lobe", C.c_int32), ("is_delta", C.c_int32),
-                ("has_sample", C.c_int32), ("dims_used", C.c_uint32), ("pad1", C.c_int32)]
+                ("has_sample", C.c_int32), ("dims_used", C.c_uint32), ("transition", C.c_int32)]
+
+
+class RtMediumQuery(C.Structure):
+    _fields_ = [("pixel_seed", C.c_uint32), ("sample_index", C.c_uint32), ("dim", C.c_uint32), ("tmax", C.c_float),
+                ("wo", F3), ("wi", F3)]
+
+
+class RtMediumResult(C.Structure):
+    _fields_ = [("scattered", C.c_int32), ("dims_used", C.c_uint32), ("t", C.c_float), ("phase_eval", C.c_float),
+                ("beta", F3), ("tr", F3), ("phase_wi", F3), ("phase_pdf", C.c_float)]
 
 
 # numpy views of the two batch records (same layout as the C structs)
@@ -147,9 +160,16 @@ BSDF_QUERY_DTYPE = np.dtype([("material", "<i4"), ("front_face", "<i4"), ("pixel
 BSDF_RESULT_DTYPE = np.dtype([("f", "<f4", 3), ("pdf", "<f4"), ("fd", "<f4", 3), ("pad0", "<f4"),
                               ("wo", "<f4", 3), ("s_pdf", "<f4"), ("s_f", "<f4", 3), ("lobe", "<i4"),
                               ("is_delta", "<i4"), ("has_sample", "<i4"), ("dims_used", "<u4"),
-                              ("pad1", "<i4")])
+                              ("transition", "<i4")])
+MEDIUM_QUERY_DTYPE = np.dtype([("pixel_seed", "<u4"), ("sample_index", "<u4"), ("dim", "<u4"), ("tmax", "<f4"),
+                               ("wo", "<f4", 3), ("wi", "<f4", 3)])
+MEDIUM_RESULT_DTYPE = np.dtype([("scattered", "<i4"), ("dims_used", "<u4"), ("t", "<f4"), ("phase_eval", "<f4"),
+                                ("beta", "<f4", 3), ("tr", "<f4", 3), ("phase_wi", "<f4", 3),
+                                ("phase_pdf", "<f4")])
 assert BSDF_QUERY_DTYPE.itemsize == C.sizeof(RtBsdfQuery)
 assert BSDF_RESULT_DTYPE.itemsize == C.sizeof(RtBsdfResult)
+assert MEDIUM_QUERY_DTYPE.itemsize == C.sizeof(RtMediumQuery)
+assert MEDIUM_RESULT_DTYPE.itemsize == C.sizeof(RtMediumResult)
 
 
 def _f3(x):
@@ -272,6 +292,7 @@ def load(path: str | None = None):
     P = C.c_void_p
     sig = {
         "rt_abi_version": (C.c_int, []),
+        "rt_checked_build": (C.c_int, []),
         "rt_last_error": (C.c_char_p, []),
         "rt_device_count": (C.c_int, []),
         "rt_scene_create": (C.c_int, [C.POINTER(RtWorldDesc), C.POINTER(P)]),
@@ -294,6 +315,7 @@ def load(path: str | None = None):
         "rt_trace_closest": (C.c_int, [P, P, C.c_int64, C.c_float, C.c_float, P, C.c_int32]),
         "rt_trace_any": (C.c_int, [P, P, C.c_int64, P, C.c_int32]),
         "rt_bsdf_batch": (C.c_int, [P, P, C.c_int64, P]),
+        "rt_medium_batch": (C.c_int, [P, P, C.c_int64, P]),
         "rt_sobol_batch": (C.c_int, [P, P, P, C.c_int64, P]),
         "rt_energy_lut": (C.c_int, [P, P]),
         "rt_probe_l2_bandwidth": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, C.POINTER(C.c_double)]),

@@ -19,6 +19,26 @@
 namespace rt {
 
 // ---------------------------------------------------------------------------
+// Checked build (-DRT_CHECKED): every index that comes from scene data or from
+// the wavefront's queues is tested against its array's length before the
+// access. An index out of range raises a device flag, which the host turns
+// into RT_ERR_BOUNDS when the call ends, and is replaced by 0 (the checked
+// build gives every array at least one element), so the access stays in
+// bounds and nothing traps. The product build compiles the tests away.
+// ---------------------------------------------------------------------------
+#ifdef RT_CHECKED
+static __device__ int g_bounds_flag;
+RT_D long long checked_index(long long i, long long n) {
+    if (i >= 0 && i < n) return i;
+    atomicExch(&g_bounds_flag, 1);
+    return 0;
+}
+#define RT_IX(i, n) checked_index((long long)(i), (long long)(n))
+#else
+#define RT_IX(i, n) (i)
+#endif
+
+// ---------------------------------------------------------------------------
 // Owen-scrambled Sobol (Core/Sampling/OwenSobol.cs:48-210)
 // ---------------------------------------------------------------------------
 __constant__ uint32_t c_dim1_dirs[32] = {
@@ -161,15 +181,16 @@ RT_D bool sphere_test(const SphereData& s, V3 o, V3 d, float tmin, float tmax, f
 
 // Tests one quad/sphere entity. Returns true on an accepted hit.
 RT_D bool entity_test(const SceneView& s, int e, V3 o, V3 d, float tmin, float tmax, Hit& h) {
-    Entity en = s.entities[e];
+    Entity en = s.entities[RT_IX(e, s.n_entities)];
     float t, a = 0.0f, b = 0.0f;
     if (en.kind == ENT_QUAD) {
-        if (!quad_test(s.quads[en.index], o, d, tmin, tmax, (en.flags & ENT_BACKFACE_CULLED) != 0, t, a, b))
+        if (!quad_test(s.quads[RT_IX(en.index, s.n_quads)], o, d, tmin, tmax, (en.flags & ENT_BACKFACE_CULLED) != 0,
+                       t, a, b))
             return false;
         h = Hit{t, a, b, HIT_QUAD, e};
         return true;
     }
-    if (!sphere_test(s.spheres[en.index], o, d, tmin, tmax, t)) return false;
+    if (!sphere_test(s.spheres[RT_IX(en.index, s.n_spheres)], o, d, tmin, tmax, t)) return false;
     h = Hit{t, 0.0f, 0.0f, HIT_SPHERE, e};
     return true;
 }
@@ -245,7 +266,7 @@ struct Walker {
             if (cnt) cnt->nodes++;                // the world root's BvhNode.Hit
         } else {
             for (int i = s.num_top_items - 1; i >= 0; --i) {
-                st_code[sp] = leaf_code(s.top_items[i], LEAF_ENT1, 1);
+                st_code[sp] = leaf_code(s.top_items[RT_IX(i, s.num_top_items)], LEAF_ENT1, 1);
                 st_te[sp] = -kInf;
                 sp++;
             }
@@ -257,7 +278,7 @@ struct Walker {
     RT_D bool step(const SceneView& s, TravCounters* cnt, int* err) {
         // Descend interior records: test both children, go near, stack far.
         while (code >= 0) {
-            const float4* np = s.cnodes + (size_t)code * 4;
+            const float4* np = s.cnodes + (size_t)RT_IX(code, s.n_cnodes) * 4;
             float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), e = __ldg(np + 3);
             if (cnt) cnt->nodes += 2;
             float tel, ter;
@@ -290,11 +311,12 @@ struct Walker {
             int count = (v & 7) + 1;
             code = kNone;
             if (kind == LEAF_ENT1) {
-                Entity en = s.entities[first];
+                Entity en = s.entities[RT_IX(first, s.n_entities)];
                 if (en.kind == ENT_MESH) {   // Mesh.Hit -> its BVH root (box test) or flat list
                     if (en.index >= 0) {
                         if (cnt) cnt->nodes++;
-                        float4 lo = __ldg(s.ent_box + 2 * first), hi = __ldg(s.ent_box + 2 * first + 1);
+                        float4 lo = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities)),
+                               hi = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
                         float te;
                         if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
                             code = en.index;
@@ -320,7 +342,7 @@ struct Walker {
                     return true;
                 }
                 for (int i = count - 1; i >= 0; --i) {
-                    st_code[sp] = leaf_code(s.top_items[first + i], LEAF_ENT1, 1);
+                    st_code[sp] = leaf_code(s.top_items[RT_IX(first + i, s.num_top_items)], LEAF_ENT1, 1);
                     st_te[sp] = -kInf;
                     sp++;
                 }
@@ -328,7 +350,7 @@ struct Walker {
                 for (int i = 0; i < count; i++) {
                     float t, u, vv;
                     if (cnt) cnt->tris++;
-                    if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, vv)) {
+                    if (tri_test(s.tris, RT_IX(first + i, s.n_tris), o, d, tmin, closest, t, u, vv)) {
                         best = Hit{t, u, vv, HIT_TRI, first + i};
                         closest = t;
                         if (ANY) return true;
@@ -376,13 +398,13 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
         if (cnt) cnt->nodes++;                // the world root's BvhNode.Hit
     } else {
         for (int i = s.num_top_items - 1; i >= 0; --i) {
-            push(leaf_code(s.top_items[i], LEAF_ENT1, 1), -kInf);
+            push(leaf_code(s.top_items[RT_IX(i, s.num_top_items)], LEAF_ENT1, 1), -kInf);
         }
     }
     for (;;) {
         // Descend interior records: test both children, go near, stack far.
         while (code >= 0) {
-            const float4* np = s.cnodes + (size_t)code * 4;
+            const float4* np = s.cnodes + (size_t)RT_IX(code, s.n_cnodes) * 4;
             float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), e = __ldg(np + 3);
             if (cnt) cnt->nodes += 2;
             float tel, ter;
@@ -412,11 +434,12 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
             int count = (v & 7) + 1;
             code = kNone;
             if (kind == LEAF_ENT1) {
-                Entity en = s.entities[first];
+                Entity en = s.entities[RT_IX(first, s.n_entities)];
                 if (en.kind == ENT_MESH) {   // Mesh.Hit -> its BVH root (box test) or flat list
                     if (en.index >= 0) {
                         if (cnt) cnt->nodes++;
-                        float4 lo = __ldg(s.ent_box + 2 * first), hi = __ldg(s.ent_box + 2 * first + 1);
+                        float4 lo = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities)),
+                               hi = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
                         float te;
                         if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
                             code = en.index;
@@ -440,12 +463,13 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                     *err = RT_ERR_STACK;
                     return false;
                 }
-                for (int i = count - 1; i >= 0; --i) push(leaf_code(s.top_items[first + i], LEAF_ENT1, 1), -kInf);
+                for (int i = count - 1; i >= 0; --i)
+                    push(leaf_code(s.top_items[RT_IX(first + i, s.num_top_items)], LEAF_ENT1, 1), -kInf);
             } else {   // triangle leaf (or a mesh's flat list)
                 for (int i = 0; i < count; i++) {
                     float t, u, vv;
                     if (cnt) cnt->tris++;
-                    if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, vv)) {
+                    if (tri_test(s.tris, RT_IX(first + i, s.n_tris), o, d, tmin, closest, t, u, vv)) {
                         best = Hit{t, u, vv, HIT_TRI, first + i};
                         closest = t;
                         if (ANY) return true;
@@ -496,14 +520,14 @@ __device__ __forceinline__ bool traverse4(const SceneView& s, V3 o, V3 d, float 
         code = s.top_root4;
     } else {
         for (int i = s.num_top_items - 1; i >= 0; --i) {
-            st_code[sp] = leaf_code(s.top_items[i], LEAF_ENT1, 1);
+            st_code[sp] = leaf_code(s.top_items[RT_IX(i, s.num_top_items)], LEAF_ENT1, 1);
             st_te[sp] = -kInf;
             sp++;
         }
     }
     for (;;) {
         while (code >= 0) {
-            const float4* q = s.cnodes4 + (size_t)code * 8;
+            const float4* q = s.cnodes4 + (size_t)RT_IX(code, s.n_cnodes4) * 8;
             float4 lx = __ldg(q), ly = __ldg(q + 1), lz = __ldg(q + 2);
             float4 hx = __ldg(q + 3), hy = __ldg(q + 4), hz = __ldg(q + 5);
             float4 cc = __ldg(q + 6), mt = __ldg(q + 7);
@@ -549,11 +573,12 @@ __device__ __forceinline__ bool traverse4(const SceneView& s, V3 o, V3 d, float 
             int count = (v & 7) + 1;
             code = kNone;
             if (kind == LEAF_ENT1) {
-                Entity en = s.entities[first];
+                Entity en = s.entities[RT_IX(first, s.n_entities)];
                 if (en.kind == ENT_MESH) {
-                    int r4 = __ldg(s.mesh_root4 + first);
+                    int r4 = __ldg(s.mesh_root4 + RT_IX(first, s.n_entities));
                     if (en.index >= 0) {
-                        float4 lo = __ldg(s.ent_box + 2 * first), hi = __ldg(s.ent_box + 2 * first + 1);
+                        float4 lo = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities)),
+                               hi = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
                         float te;
                         if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
                             code = r4;
@@ -577,14 +602,14 @@ __device__ __forceinline__ bool traverse4(const SceneView& s, V3 o, V3 d, float 
                     return false;
                 }
                 for (int i = count - 1; i >= 0; --i) {
-                    st_code[sp] = leaf_code(s.top_items[first + i], LEAF_ENT1, 1);
+                    st_code[sp] = leaf_code(s.top_items[RT_IX(first + i, s.num_top_items)], LEAF_ENT1, 1);
                     st_te[sp] = -kInf;
                     sp++;
                 }
             } else {
                 for (int i = 0; i < count; i++) {
                     float t, u, vv;
-                    if (tri_test(s.tris, first + i, o, d, tmin, closest, t, u, vv)) {
+                    if (tri_test(s.tris, RT_IX(first + i, s.n_tris), o, d, tmin, closest, t, u, vv)) {
                         best = Hit{t, u, vv, HIT_TRI, first + i};
                         closest = t;
                         if (ANY) return true;
@@ -626,15 +651,16 @@ RT_D Surface make_surface(const SceneView& s, const Hit& h, V3 o, V3 d) {
     r.t = h.t;
     r.p = o + h.t * d;   // Ray.At
     if (h.kind == HIT_TRI) {
-        const float4* tp = s.tris + 3 * h.slot;
+        int ti = RT_IX(h.slot, s.n_tris);
+        const float4* tp = s.tris + 3 * ti;
         float4 a0 = __ldg(tp), a1 = __ldg(tp + 1), a2 = __ldg(tp + 2);
         V3 e1 = ld3(a1), e2 = ld3(a2);
         V3 n = v3(a0.w, a1.w, a2.w);
         r.front = dot(d, n) < 0.0f;   // HitRecord.SetFaceNormal
         r.n = r.front ? n : -n;
-        int si = s.tri_smooth ? s.tri_smooth[h.slot] : -1;
+        int si = s.tri_smooth ? s.tri_smooth[ti] : -1;
         if (si >= 0) {   // SmoothTriangle.Hit (Geometry/SmoothTriangle.cs:166-197)
-            const SmoothTri& st = s.smooth[si];
+            const SmoothTri& st = s.smooth[RT_IX(si, s.n_smooth)];
             float w0 = 1.0f - h.u - h.v;
             V3 sn = normalize(w0 * st.n0 + h.u * st.n1 + h.v * st.n2);
             r.n = r.front ? sn : -sn;   // the face normal decides the side
@@ -644,11 +670,11 @@ RT_D Surface make_surface(const SceneView& s, const Hit& h, V3 o, V3 d) {
             r.tangent = length_sq(e1) > 0.0f ? normalize(e1) : v3(1.0f, 0.0f, 0.0f);
             r.bitangent = length_sq(e2) > 0.0f ? normalize(e2) : v3(0.0f, 0.0f, 1.0f);
         }
-        r.entity = s.tri_entity[h.slot];
-        r.prim = s.tri_local[h.slot];
+        r.entity = s.tri_entity[ti];
+        r.prim = s.tri_local[ti];
     } else if (h.kind == HIT_QUAD) {
-        Entity en = s.entities[h.slot];
-        const QuadData& q = s.quads[en.index];
+        Entity en = s.entities[RT_IX(h.slot, s.n_entities)];
+        const QuadData& q = s.quads[RT_IX(en.index, s.n_quads)];
         r.front = dot(d, q.normal) < 0.0f;
         r.n = r.front ? q.normal : -q.normal;
         r.tangent = q.tangent;
@@ -656,8 +682,8 @@ RT_D Surface make_surface(const SceneView& s, const Hit& h, V3 o, V3 d) {
         r.entity = h.slot;
         r.prim = 0;
     } else {
-        Entity en = s.entities[h.slot];
-        const SphereData& sp = s.spheres[en.index];
+        Entity en = s.entities[RT_IX(h.slot, s.n_entities)];
+        const SphereData& sp = s.spheres[RT_IX(en.index, s.n_spheres)];
         V3 outward = (r.p - sp.c) / sp.r;
         r.front = dot(d, outward) < 0.0f;
         r.n = r.front ? outward : -outward;
@@ -668,7 +694,7 @@ RT_D Surface make_surface(const SceneView& s, const Hit& h, V3 o, V3 d) {
         r.entity = h.slot;
         r.prim = 0;
     }
-    r.material = s.entities[r.entity].material;
+    r.material = RT_IX(s.entities[RT_IX(r.entity, s.n_entities)].material, s.n_materials);
     return r;
 }
 
@@ -1484,7 +1510,7 @@ RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, i
         V3 sp, ln;
         float area;
         if (l.type == LIGHT_GEOM_QUAD) {   // Quad.SampleStratified (Quad.cs:99-109)
-            const QuadData& q = s.quads[l.quad];
+            const QuadData& q = s.quads[RT_IX(l.quad, s.n_quads)];
             int su = si % l.sqrt_samples, sv = si / l.sqrt_samples;
             float inv = 1.0f / (float)l.sqrt_samples;
             float uu = ((float)su + rng.next()) * inv;
@@ -1500,18 +1526,18 @@ RT_D LightSample light_sample(const SceneView& s, const Light& l, V3 p, V3 sn, i
             int lo = 0, hi = l.mesh_count;   // lower_bound over the cumulative areas
             while (lo < hi) {
                 int mid = (lo + hi) >> 1;
-                if (s.light_tris[l.mesh_first + mid].cum_area < target) lo = mid + 1;
+                if (s.light_tris[RT_IX(l.mesh_first + mid, s.n_light_tris)].cum_area < target) lo = mid + 1;
                 else hi = mid;
             }
             int idx = min(max(lo, 0), l.mesh_count - 1);
-            const LightTri& t = s.light_tris[l.mesh_first + idx];
+            const LightTri& t = s.light_tris[RT_IX(l.mesh_first + idx, s.n_light_tris)];
             float x1 = rng.next();
             float x2 = rng.next();
             float r1 = sqrtf(x1);
             float u = 1.0f - r1;
             float v = x2 * r1;
             if (t.smooth >= 0) {   // SmoothTriangle.SampleAt (:219-230)
-                const SmoothTri& st = s.smooth[t.smooth];
+                const SmoothTri& st = s.smooth[RT_IX(t.smooth, s.n_smooth)];
                 float w0 = 1.0f - u - v;
                 sp = w0 * t.v0 + u * st.v1 + v * st.v2;
                 ln = normalize(w0 * st.n0 + u * st.n1 + v * st.n2);
@@ -1613,11 +1639,12 @@ __device__ __noinline__ float mesh_light_pdf(const SceneView& s, const Light& l,
     int err = 0;
     traverse<false, 64>(s, p, wi, kEps, kInf, h, nullptr, &err, true, l.mesh_root);
     if (err || h.kind == HIT_NONE) return 0.0f;
-    const float4* tp = s.tris + 3 * h.slot;
+    int ti = RT_IX(h.slot, s.n_tris);
+    const float4* tp = s.tris + 3 * ti;
     V3 n = v3(__ldg(tp).w, __ldg(tp + 1).w, __ldg(tp + 2).w);
-    int si = s.tri_smooth ? s.tri_smooth[h.slot] : -1;
+    int si = s.tri_smooth ? s.tri_smooth[ti] : -1;
     if (si >= 0) {   // the hit record's normal is the interpolated one
-        const SmoothTri& st = s.smooth[si];
+        const SmoothTri& st = s.smooth[RT_IX(si, s.n_smooth)];
         float w0 = 1.0f - h.u - h.v;
         n = normalize(w0 * st.n0 + h.u * st.n1 + h.v * st.n2);
     }
@@ -1632,7 +1659,7 @@ __device__ __noinline__ float mesh_light_pdf(const SceneView& s, const Light& l,
 // DirectionalLight.cs:169-181).
 RT_D float light_pdf(const SceneView& s, const Light& l, V3 p, V3 wi) {
     if (l.type == LIGHT_GEOM_QUAD) {
-        const QuadData& q = s.quads[l.quad];
+        const QuadData& q = s.quads[RT_IX(l.quad, s.n_quads)];
         float t, a, b;
         if (!quad_test(q, p, wi, kEps, kInf, false, t, a, b)) return 0.0f;
         float cl = fabsf(dot(-wi, q.normal));   // |.| makes the face flip irrelevant

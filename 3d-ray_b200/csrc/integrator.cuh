@@ -90,9 +90,9 @@ RT_D float shadow_terminator(V3 ng, V3 ns, V3 w) {   // Core/MathUtils.cs:44-61
 __device__ __noinline__ V3 weight_emission(const SceneView& s, const RenderConst& rc, V3 raw, int mat, V3 o, V3 d, float prev_pdf,
                         int prev_delta) {
     if (prev_delta) return raw;
-    int li = s.emitter_light[mat];
+    int li = s.emitter_light[RT_IX(mat, s.n_materials)];
     if (li >= 0) {
-        float pl = light_pdf(s, s.lights[li], o, d);
+        float pl = light_pdf(s, s.lights[RT_IX(li, s.num_lights)], o, d);
         if (prev_pdf + pl <= 1e-20f) return v3(0.0f);
         return raw * mis_weight(prev_pdf, pl, rc.mis_power);
     }
@@ -201,7 +201,7 @@ RT_D void nee_surface(const SceneView& s, const RenderConst& rc, PathState& ps, 
         inv_pick = p_pick > 0.0f ? 1.0f / p_pick : 0.0f;
     }
     for (int li = l0; li < l1; li++) {
-        const Light& l = s.lights[li];
+        const Light& l = s.lights[RT_IX(li, s.num_lights)];
         for (int si = 0; si < l.shadow_samples; si++) {
             LightSample ls = light_sample(s, l, rec.p, rec.n, si, ps.rng);
             if (ls.occluded || !ls.has_ray) continue;
@@ -244,7 +244,7 @@ RT_D void nee_medium(const SceneView& s, const RenderConst& rc, PathState& ps, V
         inv_pick = p_pick > 0.0f ? 1.0f / p_pick : 0.0f;
     }
     for (int li = l0; li < l1; li++) {
-        const Light& l = s.lights[li];
+        const Light& l = s.lights[RT_IX(li, s.num_lights)];
         for (int si = 0; si < l.shadow_samples; si++) {
             LightSample ls = light_sample(s, l, p, v3(0.0f), si, ps.rng);
             if (ls.occluded || !ls.has_ray) continue;

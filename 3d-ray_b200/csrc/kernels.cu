@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -37,7 +38,7 @@ static_assert(sizeof(RtEntityDesc) == 80, "ABI layout");
 static_assert(sizeof(RtLightDesc) == 104, "ABI layout");
 static_assert(sizeof(RtCameraDesc) == 48, "ABI layout");
 static_assert(sizeof(RtMediumDesc) == 36, "ABI layout");
-static_assert(sizeof(RtRenderParams) == 104, "ABI layout");
+static_assert(sizeof(RtRenderParams) == 112, "ABI layout");
 static_assert(sizeof(RtStats) == 144, "ABI layout");
 static_assert(sizeof(RtBsdfQuery) == 96, "ABI layout");
 static_assert(sizeof(RtBsdfResult) == 80, "ABI layout");
@@ -46,6 +47,8 @@ static_assert(sizeof(RtWorldDesc) == 184, "ABI layout");
 static_assert(sizeof(RtCapture) == 64, "ABI layout");
 static_assert(sizeof(RtSceneInfo) == 64, "ABI layout");
 static_assert(sizeof(RtSceneOptions) == 32, "ABI layout");
+static_assert(sizeof(RtMediumQuery) == 40, "ABI layout");
+static_assert(sizeof(RtMediumResult) == 56, "ABI layout");
 
 constexpr int kStack = 64;       // traversal stack entries per thread
 constexpr int kBlock = 128;      // 16 x 8 pixel tiles
@@ -120,12 +123,19 @@ void ray_sort_box(const rt::HostScene& h, rt::SceneView& v) {
     v.sort_scale = rt::v3(scale[0], scale[1], scale[2]);
 }
 
+// `null_when_empty`: the kernels read a null pointer as "absent" (tri_smooth).
+// The checked build gives every other array at least one zeroed element, so
+// the index it substitutes for an out-of-range one can always be read.
 template <typename T>
-int upload(RtScene* sc, const std::vector<T>& v, const T** out) {
+int upload(RtScene* sc, const std::vector<T>& v, const T** out, bool null_when_empty = false) {
+#ifdef RT_CHECKED
+    if (v.empty() && !null_when_empty) return upload(sc, std::vector<T>(1, T{}), out);
+#endif
     if (v.empty()) {
         *out = nullptr;
         return RT_OK;
     }
+    (void)null_when_empty;
     void* p = nullptr;
     size_t n = v.size() * sizeof(T);
     if (cudaMalloc(&p, n) != cudaSuccess) return fail(RT_ERR_OOM, "cudaMalloc of " + std::to_string(n) + " bytes failed");
@@ -162,10 +172,17 @@ __global__ void __launch_bounds__(kBlock) k_render_mega(rt::SceneView s, rt::Ren
     if (lx >= ww || ly >= wh) return;
     int sb = chunk * per_chunk;
     int se = min(sb + per_chunk, spp);
-    V3 sum = rt::v3(0.0f);
+    // The chunk's sum in double: a float sum of tens of thousands of samples
+    // drifts by ~1e-3 of its value through the rounding of every addition.
+    double sx = 0.0, sy = 0.0, sz = 0.0;
     rt::Counters cnt{{0u, 0u, 0u}, {0u, 0u, 0u}, 0u, 0u};
-    for (int si = sb; si < se; si++)
-        sum = sum + rt::trace_sample<STACK, COUNT>(s, rc, x0 + lx, y0 + ly, (uint32_t)(spp0 + si), &cnt, err);
+    for (int si = sb; si < se; si++) {
+        V3 l = rt::trace_sample<STACK, COUNT>(s, rc, x0 + lx, y0 + ly, (uint32_t)(spp0 + si), &cnt, err);
+        sx += l.x;
+        sy += l.y;
+        sz += l.z;
+    }
+    V3 sum = rt::v3((float)sx, (float)sy, (float)sz);
     if (COUNT) {
         atomicAdd(work + 0, (unsigned long long)cnt.closest.nodes);
         atomicAdd(work + 1, (unsigned long long)cnt.closest.tris);
@@ -467,7 +484,36 @@ __global__ void k_bsdf(rt::SceneView s, const RtBsdfQuery* q, int64_t n, RtBsdfR
         r.s_f[0] = bs.f.x; r.s_f[1] = bs.f.y; r.s_f[2] = bs.f.z;
         r.s_pdf = bs.pdf;
         r.is_delta = bs.is_delta;
+        r.transition = bs.transition;
     }
+    out[i] = r;
+}
+
+// Medium batch: HomogeneousMedium.Sample over [0, tmax], then
+// HenyeyGreensteinPhase.Sample(wo), on one Sobol stream per query, with
+// Transmittance(tmax) and Evaluate(wo, wi) beside them.
+__global__ void k_medium(rt::SceneView s, const RtMediumQuery* q, int64_t n, RtMediumResult* out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    RtMediumQuery qq = q[i];
+    RtMediumResult r;
+    memset(&r, 0, sizeof(r));
+    V3 wo = rt::v3(qq.wo[0], qq.wo[1], qq.wo[2]);
+    V3 wi = rt::v3(qq.wi[0], qq.wi[1], qq.wi[2]);
+    rt::Sampler rng{qq.pixel_seed, qq.sample_index, qq.dim};
+    float t = 0.0f;
+    V3 beta;
+    r.scattered = rt::medium_sample(s, qq.tmax, rng, t, beta) ? 1 : 0;
+    r.t = t;
+    r.beta[0] = beta.x; r.beta[1] = beta.y; r.beta[2] = beta.z;
+    float pdf = 0.0f;
+    V3 d = rt::hg_sample(s.hg_g, wo, rng, pdf);
+    r.phase_wi[0] = d.x; r.phase_wi[1] = d.y; r.phase_wi[2] = d.z;
+    r.phase_pdf = pdf;
+    r.dims_used = rng.dim - qq.dim;
+    V3 tr = rt::medium_tr(s, qq.tmax);
+    r.tr[0] = tr.x; r.tr[1] = tr.y; r.tr[2] = tr.z;
+    r.phase_eval = rt::hg_eval(s.hg_g, wo, wi);
     out[i] = r;
 }
 
@@ -491,13 +537,28 @@ __global__ void k_sobol(const uint32_t* idx, const uint32_t* dim, const uint32_t
     out[i] = rt::sobol_sample(idx[i], dim[i], seed[i]);
 }
 
+// The checked build's out-of-range flag (one per device, shared by every
+// scene): read and cleared once the stream's work is done.
+int checked_flag(cudaStream_t stream) {
+#ifdef RT_CHECKED
+    int flag = 0, zero = 0;
+    CUDA_TRY(cudaMemcpyFromSymbolAsync(&flag, rt::g_bounds_flag, sizeof(int), 0, cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaMemcpyToSymbolAsync(rt::g_bounds_flag, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    if (flag) return fail(RT_ERR_BOUNDS, "checked build: a kernel met an index out of its array's range");
+#else
+    (void)stream;
+#endif
+    return RT_OK;
+}
+
 int check_err(RtScene* sc) {
     int e = 0;
     CUDA_TRY(cudaMemcpyAsync(&e, sc->d_err, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
     CUDA_TRY(cudaStreamSynchronize(sc->stream));
     if (e == RT_ERR_STACK) return fail(RT_ERR_STACK, "traversal stack bound exceeded");
     if (e != 0) return fail(RT_ERR_BOUNDS, "device error " + std::to_string(e));
-    return RT_OK;
+    return checked_flag(sc->stream);
 }
 
 int validate_params(const RtScene* sc, const RtRenderParams* p) {
@@ -620,6 +681,11 @@ struct WfWorkspace {
     size_t bytes = 0;
     unsigned long long* pinned = nullptr;   // two read-back slots of {next, live | overflow}
     cudaEvent_t polled[2] = {nullptr, nullptr};   // each slot's read-back has landed
+    // The last instantiated iteration graph and the kernel arguments and launch
+    // shapes it was captured with: a repeated render of the same configuration
+    // replays it instead of capturing and instantiating a new one.
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> exec_key;
 };
 std::mutex g_wf_mu;
 WfWorkspace g_wf_ws[16];
@@ -647,7 +713,15 @@ struct WfConfig {
     int fetch = 1;     // 1 one ray per thread, 2 persistent warps with dynamic fetch (two-wide only)
     int tblock = 0;    // block of extend/occlude (0: block)
     int groups = 0;    // 1 slot order, 2 block-local regrouping, 3 sorted bounce rays, 4 and shadow rays; 0 default_groups
+    int iter_limit = 0;     // test only: > 0 caps the iterations below the host's bound
+    int shadow_limit = 0;   // test only: > 0 caps the shadow queue's records
 };
+
+// The test-only limits of a render request (0: none).
+void apply_test_limits(WfConfig& cfg, const RtRenderParams* p) {
+    cfg.iter_limit = std::max(0, p->iteration_limit);
+    cfg.shadow_limit = std::max(0, p->shadow_queue_limit);
+}
 
 // Untuned ray order: bounce and shadow rays sorted, except with a
 // participating medium. There nearly every slot is a bounce ray scattered in
@@ -721,6 +795,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     nslots = (nslots + 255) / 256 * 256;
     int64_t cap = (int64_t)nslots * max_shadow;
     if (cap >= ((int64_t)1 << 31) || nslots >= (1 << 29)) return fail(RT_ERR_INVALID_ARG, "wavefront too large");
+    if (cfg.shadow_limit > 0) cap = std::min<int64_t>(cap, cfg.shadow_limit);
     // Workspace layout.
     size_t need = 0;
     auto add = [&](size_t b) { need = ((need + 255) & ~(size_t)255) + b; };
@@ -740,12 +815,15 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     add(sizeof(int));
     for (int k = 0; k < 3; k++) add((size_t)cap * sizeof(int));
     for (int k = 0; k < 4; k++) add((size_t)rt::kRayKeys * sizeof(int));
-    for (auto& q : wreq) add((size_t)3 * q.ww * q.wh * sizeof(float));
+    for (auto& q : wreq) add((size_t)3 * q.ww * q.wh * sizeof(double));
     add(reqs.size() * sizeof(float*));
     add(reqs.size() * sizeof(int) * 2);
     need += 1024;
     WfWorkspace& ws = g_wf_ws[dev];
     if (ws.bytes < need) {
+        if (ws.exec) cudaGraphExecDestroy(ws.exec);   // captured with pointers into the old workspace
+        ws.exec = nullptr;
+        ws.exec_key.clear();
         if (ws.mem) cudaFree(ws.mem);
         ws.mem = nullptr;
         ws.bytes = 0;
@@ -758,7 +836,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
             return fail(RT_ERR_CUDA, "event creation failed");
     Carve cv{static_cast<char*>(ws.mem)};
-    rt::WfArgs a{};
+    rt::WfArgs a;
+    std::memset(&a, 0, sizeof(a));   // padding too: the bytes key the cached graph
     auto* d_views = cv.take<rt::SceneView>(views.size());
     auto* d_reqs = cv.take<rt::WfRequest>(wreq.size());
     auto* d_kb = cv.take<int>(key_base.size());
@@ -794,7 +873,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     std::vector<float*> films(reqs.size());
     std::vector<int> fdims(2 * reqs.size());
     for (size_t r = 0; r < reqs.size(); r++) {
-        wreq[r].accum = cv.take<float>((size_t)3 * wreq[r].ww * wreq[r].wh);
+        wreq[r].accum = cv.take<double>((size_t)3 * wreq[r].ww * wreq[r].wh);
         films[r] = reqs[r].d_film;
         fdims[r] = reqs[r].W;
         fdims[reqs.size() + r] = reqs[r].H;
@@ -802,6 +881,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     auto* d_films = cv.take<float*>(reqs.size());
     auto* d_fdims = cv.take<int>(2 * reqs.size());
     a.views = d_views;
+    a.nviews = (int)views.size();
     a.reqs = d_reqs;
     a.nreq = (int)wreq.size();
     a.nslots = nslots;
@@ -823,7 +903,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     CUDA_TRY(cudaMemsetAsync(a.S.count, 0, sizeof(int), stream));
     for (int* h : {a.rhist, a.roff, a.shist, a.soff})
         CUDA_TRY(cudaMemsetAsync(h, 0, (size_t)rt::kRayKeys * sizeof(int), stream));
-    for (auto& q : wreq) CUDA_TRY(cudaMemsetAsync(q.accum, 0, (size_t)3 * q.ww * q.wh * sizeof(float), stream));
+    for (auto& q : wreq) CUDA_TRY(cudaMemsetAsync(q.accum, 0, (size_t)3 * q.ww * q.wh * sizeof(double), stream));
     CUDA_TRY(cudaMemsetAsync(s0->d_err, 0, sizeof(int), stream));
     CUDA_TRY(cudaStreamSynchronize(stream));   // host vectors above go out of scope
     // One iteration: reset, regen, extend, [scan, scatter], shade, occlude.
@@ -900,7 +980,6 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         if (ev) cudaEventRecord(ev[5], stream);
     };
     const int batch = 4;
-    cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<cudaEvent_t> pev;
     if (cfg.profile) {
@@ -908,20 +987,37 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         for (auto& e : pev)
             if (cudaEventCreate(&e) != cudaSuccess) return fail(RT_ERR_CUDA, "event creation failed");
     } else {
-        CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        launch_iter(nullptr);
-        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
-        if (ce != cudaSuccess) return fail(RT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&exec, graph, 0);
-        if (ce != cudaSuccess) {
-            cudaGraphDestroy(graph);
-            return fail(RT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        // The graph is a function of the kernels' arguments and launch shapes
+        // alone (everything else it reads lives in the workspace), so those
+        // bytes key the cached one.
+        const unsigned shape[] = {(unsigned)blk, (unsigned)tblk, (unsigned)l4, (unsigned)pt, (unsigned)medium,
+                                  (unsigned)transmit, gpt_e, gpt_o, gs, gst, gsh, g256, gsh256};
+        std::vector<unsigned char> key(sizeof(a) + sizeof(shape));
+        std::memcpy(key.data(), &a, sizeof(a));
+        std::memcpy(key.data() + sizeof(a), shape, sizeof(shape));
+        if (ws.exec && ws.exec_key == key) {
+            exec = ws.exec;
+        } else {
+            if (ws.exec) cudaGraphExecDestroy(ws.exec);
+            ws.exec = nullptr;
+            ws.exec_key.clear();
+            cudaGraph_t graph = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            launch_iter(nullptr);
+            cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+            if (ce != cudaSuccess) return fail(RT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);   // the executable graph does not need it
+            if (ce != cudaSuccess) return fail(RT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+            ws.exec = exec;
+            ws.exec_key = std::move(key);
         }
     }
     int per_iter = 5 + (sort ? 2 : 0) + (a.raysort ? 1 : 0) + (a.shadowsort ? 2 : 0);
     int max_depth = 1;
     for (auto& q : wreq) max_depth = std::max(max_depth, q.rc.max_depth);
     int64_t limit = (total / nslots + 2) * (int64_t)(max_depth + 2) + 64;
+    if (cfg.iter_limit > 0) limit = std::min<int64_t>(limit, cfg.iter_limit);
     int64_t iters = 0;
     double t_regen = 0, t_extend = 0, t_sort = 0, t_shade = 0, t_occlude = 0;
     int rc = RT_OK;
@@ -991,8 +1087,15 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         CUDA_TRY(cudaStreamSynchronize(stream));
         rc = check_err(s0);
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    // On an error exit up to two batches of replays may still be queued; they
+    // write the shared workspace and the films, so let them finish before the
+    // graph goes away and the next call reuses the workspace.
+    if (rc != RT_OK) cudaStreamSynchronize(stream);
+    if (rc == RT_ERR_CUDA && ws.exec) {   // a failed launch: do not replay that graph again
+        cudaGraphExecDestroy(ws.exec);
+        ws.exec = nullptr;
+        ws.exec_key.clear();
+    }
     for (auto e : pev) cudaEventDestroy(e);
     if (rc != RT_OK) return rc;
     if (st) {
@@ -1047,6 +1150,7 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
     if (p->trace_block_size > 0) cfg.tblock = p->trace_block_size;
     if (p->ray_groups >= 1 && p->ray_groups <= 4) cfg.groups = p->ray_groups;
     cfg.profile = p->profile_kernels != 0;
+    apply_test_limits(cfg, p);
     if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
         return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
     if (cfg.tblock != 0 && cfg.tblock != 64 && cfg.tblock != 128 && cfg.tblock != 256)
@@ -1064,6 +1168,14 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
 extern "C" {
 
 int rt_abi_version(void) { return RT3D_ABI_VERSION; }
+
+int rt_checked_build(void) {
+#ifdef RT_CHECKED
+    return 1;
+#else
+    return 0;
+#endif
+}
 
 const char* rt_last_error(void) { return g_err.c_str(); }
 
@@ -1134,7 +1246,7 @@ int rt_scene_create_ex(const RtWorldDesc* world, const RtSceneOptions* options, 
     r = r ? r : upload(sc, h.lights, &v.lights);
     r = r ? r : upload(sc, h.light_tris, &v.light_tris);
     r = r ? r : upload(sc, h.smooth, &v.smooth);
-    r = r ? r : upload(sc, h.tri_smooth, &v.tri_smooth);
+    r = r ? r : upload(sc, h.tri_smooth, &v.tri_smooth, true);
     r = r ? r : upload(sc, h.emitter_light, &v.emitter_light);
     r = r ? r : upload(sc, h.pick_cdf, &v.pick_cdf);
     r = r ? r : upload(sc, h.pick_pdf, &v.pick_pdf);
@@ -1149,6 +1261,15 @@ int rt_scene_create_ex(const RtWorldDesc* world, const RtSceneOptions* options, 
     v.top_root = h.top_root_code;
     v.top_root4 = h.top_root4;
     v.num_top_items = (int)h.top_items.size();
+    v.n_cnodes = (int)(h.cnodes.size() / 4);
+    v.n_cnodes4 = (int)(h.cnodes4.size() / 8);
+    v.n_tris = (int)(h.tris.size() / 3);
+    v.n_entities = (int)h.entities.size();
+    v.n_quads = (int)h.quads.size();
+    v.n_spheres = (int)h.spheres.size();
+    v.n_materials = (int)h.materials.size();
+    v.n_light_tris = (int)h.light_tris.size();
+    v.n_smooth = (int)h.smooth.size();
     v.has_medium = h.has_medium;
     v.sigma_a = h.sigma_a;
     v.sigma_s = h.sigma_s;
@@ -1366,6 +1487,9 @@ extern "C" {
 int rt_render_device_noalloc(RtScene* sc, const RtRenderParams* p, float* d_film, RtStats* st) {
     if (!sc || !p || !d_film) return fail(RT_ERR_INVALID_ARG, "null argument");
     if (p->count_work) return fail(RT_ERR_INVALID_ARG, "count_work is not available without allocation");
+    if (p->kernel != RT_KERNEL_MEGAKERNEL)
+        return fail(RT_ERR_INVALID_ARG, "the allocation-free render runs the megakernel only (kernel must be "
+                                        "RT_KERNEL_MEGAKERNEL)");
     std::lock_guard<std::mutex> lk(sc->mu);
     auto t0 = std::chrono::steady_clock::now();
     int rc_ = validate_params(sc, p);
@@ -1411,6 +1535,8 @@ int rt_render_device_noalloc(RtScene* sc, const RtRenderParams* p, float* d_film
     CUDA_TRY(cudaStreamSynchronize(sc->stream));
     if (e == RT_ERR_STACK) return fail(RT_ERR_STACK, "traversal stack bound exceeded");
     if (e != 0) return fail(RT_ERR_BOUNDS, "device error " + std::to_string(e));
+    rc_ = checked_flag(sc->stream);
+    if (rc_ != RT_OK) return rc_;
     if (st) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
@@ -1460,6 +1586,21 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
     if (!scenes || !reqs || !outs || !common || n <= 0 || num_scenes <= 0)
         return fail(RT_ERR_INVALID_ARG, "null argument or empty batch");
     auto t0 = std::chrono::steady_clock::now();
+    // Every distinct scene of the batch stays locked for the whole call, as a
+    // single-scene call locks its scene: the batch uses their streams, error
+    // words, events and parameters. Locks are taken in address order, so two
+    // batches over overlapping scenes cannot deadlock.
+    std::vector<RtScene*> locked;
+    for (int i = 0; i < n; i++) {
+        if (reqs[i].scene < 0 || reqs[i].scene >= num_scenes || !scenes[reqs[i].scene])
+            return fail(RT_ERR_INVALID_ARG, "request " + std::to_string(i) + ": bad scene");
+        locked.push_back(scenes[reqs[i].scene]);
+    }
+    std::sort(locked.begin(), locked.end(), std::less<RtScene*>());
+    locked.erase(std::unique(locked.begin(), locked.end()), locked.end());
+    std::vector<std::unique_lock<std::mutex>> guards;
+    guards.reserve(locked.size());
+    for (RtScene* sc : locked) guards.emplace_back(sc->mu);
     std::vector<HostReq> hq((size_t)n);
     std::vector<float*> d_films((size_t)n, nullptr);
     int rc = RT_OK;
@@ -1516,6 +1657,7 @@ int rt_render_batch(RtScene* const* scenes, int32_t num_scenes, const RtRequest*
         if (common->trace_block_size > 0) cfg.tblock = common->trace_block_size;
         if (common->ray_groups >= 1 && common->ray_groups <= 4) cfg.groups = common->ray_groups;
         cfg.profile = common->profile_kernels != 0;
+        apply_test_limits(cfg, common);
         rc = wf_render(hq, cfg, st);
     }
     for (int i = 0; i < n; i++) {
@@ -1974,6 +2116,26 @@ int rt_bsdf_batch(RtScene* sc, const RtBsdfQuery* q, int64_t n, RtBsdfResult* ou
     auto* d_o = reinterpret_cast<RtBsdfResult*>(static_cast<char*>(sc->scratch) + qb);
     CUDA_TRY(cudaMemcpyAsync(d_q, q, qb, cudaMemcpyHostToDevice, sc->stream));
     k_bsdf<<<(unsigned)((n + 127) / 128), 128, 0, sc->stream>>>(sc->view, d_q, n, d_o);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, d_o, ob, cudaMemcpyDeviceToHost, sc->stream));
+    CUDA_TRY(cudaStreamSynchronize(sc->stream));
+    return RT_OK;
+}
+
+int rt_medium_batch(RtScene* sc, const RtMediumQuery* q, int64_t n, RtMediumResult* out) {
+    if (!sc || !q || !out || n < 0) return fail(RT_ERR_INVALID_ARG, "null argument");
+    if (!sc->host.has_medium) return fail(RT_ERR_INVALID_ARG, "the scene has no participating medium");
+    if (n == 0) return RT_OK;
+    std::lock_guard<std::mutex> lk(sc->mu);
+    CUDA_TRY(cudaSetDevice(sc->device));
+    size_t qb = (size_t)n * sizeof(RtMediumQuery), ob = (size_t)n * sizeof(RtMediumResult);
+    size_t qb_al = (qb + 255) & ~(size_t)255;
+    int rc = ensure_scratch(sc, qb_al + ob);
+    if (rc != RT_OK) return rc;
+    auto* d_q = static_cast<RtMediumQuery*>(sc->scratch);
+    auto* d_o = reinterpret_cast<RtMediumResult*>(static_cast<char*>(sc->scratch) + qb_al);
+    CUDA_TRY(cudaMemcpyAsync(d_q, q, qb, cudaMemcpyHostToDevice, sc->stream));
+    k_medium<<<(unsigned)((n + 127) / 128), 128, 0, sc->stream>>>(sc->view, d_q, n, d_o);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, d_o, ob, cudaMemcpyDeviceToHost, sc->stream));
     CUDA_TRY(cudaStreamSynchronize(sc->stream));

@@ -184,6 +184,9 @@ struct SceneView {
     // Box of the wavefront's bounce-ray sort: origins map to cells of
     // (o - sort_lo) * sort_scale in [0, 1) (clamped); sort_scale 0 on a flat axis.
     V3 sort_lo, sort_scale;
+    // Lengths of the arrays above, in elements; the checked build tests every
+    // index into them.
+    int n_cnodes, n_cnodes4, n_tris, n_entities, n_quads, n_spheres, n_materials, n_light_tris, n_smooth;
 };
 
 }  // namespace rt

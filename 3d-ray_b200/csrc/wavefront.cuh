@@ -38,7 +38,9 @@ struct WfRequest {
     int spp, spp0;
     long long begin;      // first global work id of this request
     long long count;      // ww * wh * spp
-    float* accum;         // 3 * ww * wh: sums of clamped samples (planar, pixels in strip_pixel order)
+    double* accum;        // 3 * ww * wh: sums of clamped samples (planar, pixels in strip_pixel order).
+                          // Double: a float sum of 65 536 samples of one pixel drifts by ~1e-3 of its
+                          // value through the rounding of every addition.
 };
 
 // SoA path state (144 B per slot + 16 B hit).
@@ -89,6 +91,7 @@ constexpr int kRayKeys = 1 << 15;
 
 struct WfArgs {
     const SceneView* views;
+    int nviews;
     const WfRequest* reqs;
     int nreq;
     int nslots;
@@ -240,17 +243,17 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
     bool alive = in && (flags & PF_ALIVE);
     bool need = in && !alive;
     if (need && (flags & PF_DONE)) {   // resolve the finished sample into its film
-        int req = fbits(a.P.pre[i].w);
+        int req = RT_IX(fbits(a.P.pre[i].w), a.nreq);
         const WfRequest& R = a.reqs[req];
         PathState ps;
         int fl, pix;
         wf_load(a, i, R, ps, fl, pix);
         V3 L = path_resolve(ps, R.rc);
         int lx = pix & 0xFFFF, ly = pix >> 16;
-        size_t plane = (size_t)R.ww * R.wh, k = (size_t)strip_index(lx, ly, R.ww, R.wh);
-        atomicAdd(R.accum + k, L.x);
-        atomicAdd(R.accum + plane + k, L.y);
-        atomicAdd(R.accum + 2 * plane + k, L.z);
+        size_t plane = (size_t)R.ww * R.wh, k = (size_t)RT_IX(strip_index(lx, ly, R.ww, R.wh), plane);
+        atomicAdd(R.accum + k, (double)L.x);
+        atomicAdd(R.accum + plane + k, (double)L.y);
+        atomicAdd(R.accum + 2 * plane + k, (double)L.z);
     }
     unsigned m = __ballot_sync(full, need);
     if (lane == 0) s_warp[wid] = __popc(m);
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
     if (alive && a.raysort) {
         // a bounce ray shade continued: its key's first position plus the rank
         // shade's count gave it
-        int pos = a.roff[a.P.keys[i]] + a.P.rrank[i];
+        int pos = a.roff[RT_IX(a.P.keys[i], kRayKeys)] + a.P.rrank[i];
         if (pos < a.ctl->nbounce) a.P.order[pos] = i;
         else atomicExch(a.err, RT_ERR_BOUNDS);
     }
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
         if (id >= a.ctl->total) {
             a.P.d[i].w = ibits(0);
         } else {
-            int req = find_request(a.reqs, a.nreq, id);
+            int req = RT_IX(find_request(a.reqs, a.nreq, id), a.nreq);
             const WfRequest& R = a.reqs[req];
             long long local = (long long)(id - (unsigned long long)R.begin);
             long long npix = (long long)R.ww * R.wh;
@@ -397,8 +400,8 @@ RT_D void extend_store(const WfArgs& a, int i, int req, const SceneView& s, cons
     if (a.sort) {   // material key for the counting sort
         int key = a.nkeys;   // misses and emitters sort last
         if (h.kind != HIT_NONE) {
-            int ent = h.kind == HIT_TRI ? s.tri_entity[h.slot] : h.slot;
-            key = a.key_base[a.reqs[req].scene] + s.entities[ent].material;
+            int ent = h.kind == HIT_TRI ? s.tri_entity[RT_IX(h.slot, s.n_tris)] : h.slot;
+            key = RT_IX(a.key_base[a.reqs[req].scene] + s.entities[RT_IX(ent, s.n_entities)].material, a.nkeys);
         }
         a.P.keys[i] = key;
         // one atomic per distinct key in the warp (__match_any_sync groups lanes)
@@ -427,6 +430,7 @@ __global__ void __launch_bounds__(256, 5) k_wf_extend(WfArgs a) {
         if ((long long)i >= n || i >= a.nslots) return;
         i = a.P.order[i];
         if (i < 0) return;
+        i = RT_IX(i, a.nslots);
     } else if (a.regroup) {
         __shared__ int s_idx[256], s_cnt[9][8], s_tot;
         int cls = -1;
@@ -444,8 +448,8 @@ __global__ void __launch_bounds__(256, 5) k_wf_extend(WfArgs a) {
     float4 d = a.P.d[i];
     if (!(fbits(d.w) & PF_ALIVE)) return;
     float4 o = a.P.o[i];
-    int req = fbits(a.P.pre[i].w);
-    const SceneView& s = a.views[a.reqs[req].scene];
+    int req = RT_IX(fbits(a.P.pre[i].w), a.nreq);
+    const SceneView& s = a.views[RT_IX(a.reqs[req].scene, a.nviews)];
     Hit h;
     trace<false, STACK, L4>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf, h, nullptr, a.err);
     extend_store(a, i, req, s, h);
@@ -484,9 +488,9 @@ __global__ void __launch_bounds__(256) k_wf_extend_pt(WfArgs a) {
                     float4 d = a.P.d[i];
                     if (fbits(d.w) & PF_ALIVE) {
                         float4 o = a.P.o[i];
-                        req = fbits(a.P.pre[i].w);
+                        req = RT_IX(fbits(a.P.pre[i].w), a.nreq);
                         slot = (int)i;
-                        w.start(a.views[a.reqs[req].scene], v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf,
+                        w.start(a.views[RT_IX(a.reqs[req].scene, a.nviews)], v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, kInf,
                                 nullptr, false, 0);
                     }
                 }
@@ -494,7 +498,7 @@ __global__ void __launch_bounds__(256) k_wf_extend_pt(WfArgs a) {
             continue;
         }
         if (slot >= 0) {
-            const SceneView& s = a.views[a.reqs[req].scene];
+            const SceneView& s = a.views[RT_IX(a.reqs[req].scene, a.nviews)];
             if (w.step(s, nullptr, a.err)) {
                 extend_store(a, slot, req, s, w.best);
                 slot = -1;
@@ -525,7 +529,7 @@ __global__ void k_wf_scatter(WfArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nslots) return;
     if (!(fbits(a.P.d[i].w) & PF_ALIVE)) return;
-    int key = a.P.keys[i];
+    int key = RT_IX(a.P.keys[i], a.nkeys + 1);
     unsigned grp = __match_any_sync(__activemask(), key);
     int lane = threadIdx.x & 31;
     int leader = __ffs(grp) - 1;
@@ -533,7 +537,7 @@ __global__ void k_wf_scatter(WfArgs a) {
     int base = 0;
     if (lane == leader) base = atomicAdd(&a.ctl->hist[key], __popc(grp));
     base = __shfl_sync(grp, base, leader);
-    a.P.order[base + rank] = i;
+    a.P.order[RT_IX(base + rank, a.nslots)] = i;
 }
 
 // Shadow sink of the wavefront: queue the ray with its contribution.
@@ -580,7 +584,7 @@ __global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a)
     if (a.sort) {
         // the scatter left the live slots in material order in order[0 .. live)
         if (t >= a.ctl->hist[a.nkeys]) return;
-        i = a.P.order[t];
+        i = RT_IX(a.P.order[RT_IX(t, a.nslots)], a.nslots);
     } else {
         if (t >= a.nslots) return;
         i = t;
@@ -588,9 +592,9 @@ __global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a)
     float4 d4 = a.P.d[i];
     int flags = fbits(d4.w);
     if (!(flags & PF_ALIVE)) return;
-    int req = fbits(a.P.pre[i].w);
+    int req = RT_IX(fbits(a.P.pre[i].w), a.nreq);
     const WfRequest& R = a.reqs[req];
-    const SceneView& s = a.views[R.scene];
+    const SceneView& s = a.views[RT_IX(R.scene, a.nviews)];
     PathState ps;
     int fl, pix;
     wf_load(a, i, R, ps, fl, pix);
@@ -672,7 +676,7 @@ __global__ void k_wf_sscatter(WfArgs a) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     int n = min(*a.S.count, a.S.capacity);
     if (j >= n) return;
-    int pos = a.soff[a.S.key[j]] + a.S.rank[j];
+    int pos = a.soff[RT_IX(a.S.key[j], kRayKeys)] + a.S.rank[j];
     if (pos < n) a.S.order[pos] = j;
     else atomicExch(a.err, RT_ERR_BOUNDS);
 }
@@ -704,17 +708,17 @@ __global__ void __launch_bounds__(256) k_wf_occlude_pt(WfArgs a) {
                 } else {
                     float4 o = a.S.o[j], d = a.S.d[j], c = a.S.c[j];
                     rec = (int)j;
-                    w.start(a.views[fbits(c.w)], v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, o.w, nullptr, false, 0);
+                    w.start(a.views[RT_IX(fbits(c.w), a.nviews)], v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps, o.w, nullptr, false, 0);
                 }
             }
             continue;
         }
         if (rec >= 0) {
             float4 c = a.S.c[rec];
-            if (w.step(a.views[fbits(c.w)], nullptr, a.err)) {
+            if (w.step(a.views[RT_IX(fbits(c.w), a.nviews)], nullptr, a.err)) {
                 if (w.best.kind == HIT_NONE) {   // visible: transmittance 1
                     int packed = fbits(a.S.d[rec].w);
-                    int slot = packed >> 1;
+                    int slot = RT_IX(packed >> 1, a.nslots);
                     float4* dst = (packed & 1) ? (a.P.la + slot) : (a.P.lp + slot);
                     float* f = reinterpret_cast<float*>(dst);
                     atomicAdd(f, c.x);
@@ -738,7 +742,7 @@ __global__ void __launch_bounds__(256, OPAQUE ? 5 : 1) k_wf_occlude(WfArgs a) {
     int n = min(*a.S.count, a.S.capacity);
     if (a.shadowsort) {
         if (j >= n) return;
-        j = a.S.order[j];
+        j = RT_IX(a.S.order[j], n);
     } else if (a.regroup) {
         // shadow rays by direction octant (blocks wholly past the queue leave at once)
         if ((int)(blockIdx.x * blockDim.x) >= n) return;
@@ -755,12 +759,12 @@ __global__ void __launch_bounds__(256, OPAQUE ? 5 : 1) k_wf_occlude(WfArgs a) {
         return;
     }
     float4 o = a.S.o[j], d = a.S.d[j], c = a.S.c[j];
-    const SceneView& s = a.views[fbits(c.w)];
+    const SceneView& s = a.views[RT_IX(fbits(c.w), a.nviews)];
     V3 tr = shadow_transmittance<STACK, L4>(s, OPAQUE ? 1 : a.opaque, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kEps,
                                             o.w, nullptr, a.err);
     if (near_zero(tr)) return;
     int packed = fbits(d.w);
-    int slot = packed >> 1;
+    int slot = RT_IX(packed >> 1, a.nslots);
     V3 v = v3(c.x, c.y, c.z) * tr;
     float4* dst = (packed & 1) ? (a.P.la + slot) : (a.P.lp + slot);
     float* f = reinterpret_cast<float*>(dst);
@@ -795,7 +799,7 @@ __global__ void k_wf_finalize(const WfRequest* reqs, int nreq, float* const* fil
         strip_pixel((int)i, R.ww, R.wh, lx, ly);   // the accumulation buffer is in strip order
         size_t fp = (size_t)film_w[r] * film_h[r];
         size_t fi = (size_t)(R.y0 + ly) * film_w[r] + (R.x0 + lx);
-        for (int c = 0; c < 3; c++) films[r][c * fp + fi] = R.accum[c * plane + i] / (float)R.spp;
+        for (int c = 0; c < 3; c++) films[r][c * fp + fi] = (float)(R.accum[c * plane + i] / (double)R.spp);
     }
 }
 

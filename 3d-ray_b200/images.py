@@ -111,7 +111,7 @@ def _attribute(name: str, typ: str, payload: bytes) -> bytes:
 
 
 def _header(width: int, height: int, chans) -> bytes:
-    """ExrImage.BuildHeader (ExrImage.cs:138-186)."""
+    """ExrImage.BuildHeader (ExrImage.cs:158-212)."""
     chl = b"".join(n.encode("ascii") + b"\0" + struct.pack("<iB3xii", t, 0, 1, 1) for n, t, _ in chans) + b"\0"
     chroma = struct.pack("<8f", 0.6400, 0.3300, 0.3000, 0.6000, 0.1500, 0.0600, 0.3127, 0.3290)
     box = struct.pack("<4i", 0, 0, width - 1, height - 1)
@@ -136,7 +136,7 @@ def _half(plane: np.ndarray) -> np.ndarray:
 
 
 def write_exr(path: str, width: int, height: int, channels, level: int = 9):
-    """ExrImage.Write (ExrImage.cs:25-105). `channels` is a list of (name,
+    """ExrImage.Write (ExrImage.cs:52-137). `channels` is a list of (name,
     HALF or FLOAT, plane of width*height floats, rows top to bottom)."""
     if width <= 0 or height <= 0:
         raise ValueError(f"Invalid EXR dimensions {width}x{height}.")

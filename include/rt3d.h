@@ -33,7 +33,12 @@
  *   rt_trace_any       : ShadowRay.Transmittance (Geometry/ShadowRay.cs:59-157)
  *   rt_bsdf_batch      : DisneyBsdf.Sample/Evaluate/Pdf/EvaluateDirect
  *                        (Materials/DisneyBsdf.cs:418-997)
+ *   rt_medium_batch    : HomogeneousMedium.Sample/Transmittance and
+ *                        HenyeyGreensteinPhase.Sample/Evaluate
+ *                        (Volumetrics/HomogeneousMedium.cs:36-76,
+ *                        Volumetrics/HenyeyGreensteinPhase.cs:23-54)
  *   rt_sobol_batch     : OwenSobol.Sample (Core/Sampling/OwenSobol.cs:48-89)
+ *   rt_tonemap         : Renderer.AcesToneMap (Rendering/Renderer.cs:893-907)
  */
 #ifndef RT3D_H
 #define RT3D_H
@@ -45,7 +50,7 @@
 extern "C" {
 #endif
 
-#define RT3D_ABI_VERSION 1
+#define RT3D_ABI_VERSION 2   /* 2: RtRenderParams gained the two test-only limits */
 
 /* ---- status codes -------------------------------------------------------- */
 #define RT_OK                  0
@@ -214,6 +219,13 @@ typedef struct RtRenderParams {
                                        then the camera rays in pixel order, 4 as 3 and occlude walks
                                        the shadow rays sorted the same way; 0 the autotuned choice
                                        (else 4, or 1 when a scene has a participating medium) */
+    /* Test-only limits of the wavefront, for exercising its failure paths.
+     * Both are 0 in production: the host then sizes the queue and bounds the
+     * iterations itself, and neither limit is ever reached. */
+    int32_t iteration_limit;        /* > 0: the wavefront gives up after this many iterations and
+                                       returns RT_ERR_TIMEOUT (the host-side bound on its poll loop) */
+    int32_t shadow_queue_limit;     /* > 0: the shadow queue holds at most this many records; a fuller
+                                       queue is refused by the kernel and the call returns RT_ERR_BOUNDS */
 } RtRenderParams;
 
 /* Counters and timings of one call. */
@@ -240,6 +252,13 @@ typedef struct RtScene RtScene;
 
 /* ---- version / errors ---------------------------------------------------- */
 int         rt_abi_version(void);
+/* 1 in the checked build (librt3d_checked.so), 0 in the product build. The
+ * checked build tests every index its kernels take from scene data or from
+ * the wavefront's queues against the array's length; an index out of range is
+ * replaced by 0 (no trap) and the call returns RT_ERR_BOUNDS. It is a
+ * diagnostic build for the test suite: its flag is one word per device,
+ * shared by all scenes, so concurrent calls may report each other's error. */
+int         rt_checked_build(void);
 const char* rt_last_error(void);
 /* Number of visible CUDA devices; < 0 on error. Loads no kernels. */
 int         rt_device_count(void);
@@ -319,7 +338,8 @@ int rt_render_device(RtScene* scene, const RtRenderParams* params, float* d_hdr_
  * call makes no allocation. Limits and rules:
  *   - the render window may hold at most 2 796 181 pixels (3 floats each in
  *     8 Mi floats minus a 256-byte header); larger windows return
- *     RT_ERR_INVALID_ARG; count_work is rejected;
+ *     RT_ERR_INVALID_ARG; count_work is rejected, and so is any
+ *     params->kernel other than RT_KERNEL_MEGAKERNEL;
  *   - the first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress); make that first call before any stream capture;
  *   - every call shares the array: calls that overlap on the GPU (any scenes,
@@ -336,7 +356,8 @@ typedef struct RtRequest {
 } RtRequest;
 
 /* Renders n requests of uneven size in one persistent wavefront launch.
- * outs[i] is a host buffer of 3*W_i*H_i floats. */
+ * outs[i] is a host buffer of 3*W_i*H_i floats. Every distinct scene of the
+ * batch is locked for the duration of the call, like a single-scene call. */
 int rt_render_batch(RtScene* const* scenes, int32_t num_scenes,
                     const RtRequest* requests, int32_t n,
                     const RtRenderParams* common, float* const* outs, RtStats* stats);
@@ -462,9 +483,38 @@ typedef struct RtBsdfResult {
     int32_t is_delta;
     int32_t has_sample;
     uint32_t dims_used;
-    int32_t pad1;
+    int32_t transition;                  /* Sample's BsdfSample.Transition: 0 none, 1 enter, 2 exit */
 } RtBsdfResult;
 int rt_bsdf_batch(RtScene* scene, const RtBsdfQuery* q, int64_t n, RtBsdfResult* out);
+
+/* Medium batch: the scene's global homogeneous medium and its
+ * Henyey-Greenstein phase on one Sobol stream per query. In this order:
+ *   HomogeneousMedium.Sample over a segment of length tmax (hero channel, then
+ *   the distance draw when that channel's sigma_t > 0;
+ *   Volumetrics/HomogeneousMedium.cs:46-76), then
+ *   HenyeyGreensteinPhase.Sample(wo) with the next two draws
+ *   (Volumetrics/HenyeyGreensteinPhase.cs:32-54), plus
+ *   Transmittance(tmax) (HomogeneousMedium.cs:36-44) and Evaluate(wo, wi)
+ *   (HenyeyGreensteinPhase.cs:23-30). wo is the incoming ray direction, as
+ *   the renderer passes it (Renderer.cs:1750-1765). A scene without a medium
+ *   is RT_ERR_INVALID_ARG. */
+typedef struct RtMediumQuery {
+    uint32_t pixel_seed, sample_index, dim;
+    float tmax;
+    float wo[3];
+    float wi[3];
+} RtMediumQuery;
+typedef struct RtMediumResult {
+    int32_t scattered;                   /* Sample: a scattering event before tmax */
+    uint32_t dims_used;                  /* Sobol dimensions both samples consumed */
+    float t;                             /* Sample: the event's distance (tmax when it passed) */
+    float phase_eval;                    /* Evaluate(wo, wi) */
+    float beta[3];                       /* Sample: the segment's weight */
+    float tr[3];                         /* Transmittance(tmax) */
+    float phase_wi[3];                   /* phase Sample: direction */
+    float phase_pdf;                     /* phase Sample: pdf */
+} RtMediumResult;
+int rt_medium_batch(RtScene* scene, const RtMediumQuery* q, int64_t n, RtMediumResult* out);
 
 /* Owen-scrambled Sobol draws: out[i] = Sample(idx[i], dim[i], seed[i]). */
 int rt_sobol_batch(const uint32_t* sample_index, const uint32_t* dim, const uint32_t* pixel_seed,
@@ -472,7 +522,8 @@ int rt_sobol_batch(const uint32_t* sample_index, const uint32_t* dim, const uint
 
 /* Display transform: exposure gain 2^ev, ACES filmic fit, gamma 1/2.2
  * (Renderer.AcesToneMap, Rendering/Renderer.cs:893-907). Planar HDR in
- * (3*W*H host floats), interleaved RGB out (W*H*3 host floats in [0, 1]). */
+ * (3*W*H host floats), interleaved RGB out (W*H*3 host floats in [0, 1]).
+ * It takes no scene, so it runs on the calling thread's current device. */
 int rt_tonemap(const float* hdr_rgb_planar, int32_t width, int32_t height, float exposure_ev, float* rgb_out);
 
 /* Kulla-Conty tables the scene uses: E (32x32, mu-major) then E_avg (32). */

@@ -48,6 +48,8 @@ def lib():
             ("or_trace_closest", C.c_int, [P, P, C.c_int64, C.c_float, C.c_float, P, P, C.c_int32]),
             ("or_trace_any", C.c_int, [P, P, C.c_int64, P]),
             ("or_bsdf_batch", C.c_int, [P, P, C.c_int64, P]),
+            ("or_medium_batch", C.c_int, [P, P, C.c_int64, P]),
+            ("or_tonemap", C.c_int, [P, C.c_int32, C.c_int32, C.c_float, P]),
             ("or_render", C.c_int, [P, P, P, C.c_int32, P]),
             ("or_render_capture", C.c_int, [P, P, P, C.c_int32]),
         ]:
@@ -101,6 +103,18 @@ def medium_sample(sigma_a, sigma_s, tmax, u_ch, u_d):
     beta = np.empty(3, np.float32)
     sc = lib().or_medium_sample(_p(sa), _p(ss), tmax, u_ch, u_d, _p(t), _p(beta))
     return bool(sc), float(t[0]), beta
+
+
+def tonemap(hdr_planar: np.ndarray, exposure_ev: float = 0.0) -> np.ndarray:
+    """Renderer.ToneMapToDisplay with AcesToneMap: planar [3, H, W] HDR in,
+    interleaved [H, W, 3] display RGB out."""
+    hdr = np.ascontiguousarray(hdr_planar, np.float32)
+    _, h, w = hdr.shape
+    out = np.empty((h, w, 3), np.float32)
+    rc = lib().or_tonemap(_p(hdr), w, h, exposure_ev, _p(out))
+    if rc != 0:
+        raise RuntimeError("oracle tonemap failed")
+    return out
 
 
 def energy_lut():
@@ -170,6 +184,14 @@ class OracleScene:
     def bsdf(self, queries: np.ndarray, result_dtype) -> np.ndarray:
         out = np.zeros(queries.shape[0], result_dtype)
         lib().or_bsdf_batch(self.h, _p(queries), queries.shape[0], _p(out))
+        return out
+
+    def medium(self, queries: np.ndarray, result_dtype) -> np.ndarray:
+        """Medium and phase draws on each query's Sobol stream (RtMediumQuery
+        records in, RtMediumResult records out)."""
+        out = np.zeros(queries.shape[0], result_dtype)
+        if lib().or_medium_batch(self.h, _p(queries), queries.shape[0], _p(out)) != 0:
+            raise RuntimeError("oracle medium batch: the scene has no medium")
         return out
 
     def render_capture(self, params, threads: int | None = None) -> dict:

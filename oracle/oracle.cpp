@@ -3015,7 +3015,66 @@ int or_bsdf_batch(void* s, const RtBsdfQuery* q, int64_t n, RtBsdfResult* out) {
             r.s_f[0] = bs.f.x; r.s_f[1] = bs.f.y; r.s_f[2] = bs.f.z;
             r.s_pdf = bs.pdf;
             r.is_delta = bs.is_delta ? 1 : 0;
+            r.transition = bs.transition;
         }
+    }
+    return 0;
+}
+
+// The scene's global medium on one Sobol stream per query: HomogeneousMedium
+// .Sample (:46-76) over [0, tmax], then HenyeyGreensteinPhase.Sample (:32-54)
+// with the next two draws, as TraceRay's volumetric branch draws them
+// (Renderer.cs:1704-1765); Transmittance(tmax) (:36-44) and Evaluate (:23-30)
+// beside them.
+int or_medium_batch(void* s, const RtMediumQuery* q, int64_t n, RtMediumResult* out) {
+    Scene* sc = static_cast<Scene*>(s);
+    if (!sc->has_medium) return -1;
+    for (int64_t i = 0; i < n; i++) {
+        const RtMediumQuery& qq = q[i];
+        RtMediumResult& r = out[i];
+        std::memset(&r, 0, sizeof(r));
+        V3 wo = v3(qq.wo[0], qq.wo[1], qq.wo[2]);
+        V3 wi = v3(qq.wi[0], qq.wi[1], qq.wi[2]);
+        begin_pixel_sample(qq.pixel_seed, qq.sample_index);
+        t_sampler.dim = qq.dim;
+        float t = 0.0f;
+        V3 beta;
+        float u_ch = random_float();
+        r.scattered = medium_draw(sc->sigma_t, sc->sigma_s, qq.tmax, u_ch, [] { return random_float(); }, t, beta);
+        r.t = t;
+        r.beta[0] = beta.x; r.beta[1] = beta.y; r.beta[2] = beta.z;
+        float u1 = random_float(), u2 = random_float();
+        float pdf = 0.0f;
+        V3 d = hg_draw(sc->hg_g, wo, u1, u2, pdf);
+        r.phase_wi[0] = d.x; r.phase_wi[1] = d.y; r.phase_wi[2] = d.z;
+        r.phase_pdf = pdf;
+        r.dims_used = t_sampler.dim - qq.dim;
+        end_pixel_sample();
+        V3 tr = medium_transmittance(sc->sigma_t, qq.tmax);
+        r.tr[0] = tr.x; r.tr[1] = tr.y; r.tr[2] = tr.z;
+        r.phase_eval = hg_evaluate(sc->hg_g, wo, wi);
+    }
+    return 0;
+}
+
+// Renderer.ToneMapToDisplay (:741-751): each pixel times the exposure scale
+// 2^ev (:333), then AcesToneMap (:893-907): floor at zero, the ACES filmic fit
+// x(2.51x + 0.03) / (x(2.43x + 0.59) + 0.14) per channel, clamp to [0, 1],
+// gamma 1/2.2. Planar HDR in, interleaved RGB out.
+int or_tonemap(const float* hdr, int32_t width, int32_t height, float exposure_ev, float* rgb) {
+    if (!hdr || !rgb || width <= 0 || height <= 0) return -1;
+    const float scale = std::pow(2.0f, exposure_ev);
+    const float inv_gamma = 1.0f / 2.2f;
+    size_t npix = (size_t)width * height;
+    for (size_t i = 0; i < npix; i++) {
+        V3 c = v3(hdr[i], hdr[npix + i], hdr[2 * npix + i]) * scale;
+        c = vmax(c, v3(0.0f));
+        V3 a = c * (2.51f * c + v3(0.03f));
+        V3 b = c * (2.43f * c + v3(0.59f)) + v3(0.14f);
+        V3 m = v3(a.x / b.x, a.y / b.y, a.z / b.z);
+        rgb[3 * i + 0] = std::pow(std::fmin(std::fmax(m.x, 0.0f), 1.0f), inv_gamma);
+        rgb[3 * i + 1] = std::pow(std::fmin(std::fmax(m.y, 0.0f), 1.0f), inv_gamma);
+        rgb[3 * i + 2] = std::pow(std::fmin(std::fmax(m.z, 0.0f), 1.0f), inv_gamma);
     }
     return 0;
 }

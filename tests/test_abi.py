@@ -29,14 +29,15 @@ def test_all_declared_symbols_exported(lib):
 
 
 def test_abi_version(lib):
-    assert lib.rt_abi_version() == 1
+    assert lib.rt_abi_version() == 2
 
 
 @pytest.mark.parametrize("struct,size", [("RtMaterialDesc", 120), ("RtEntityDesc", 80), ("RtLightDesc", 104),
-                                         ("RtCameraDesc", 48), ("RtMediumDesc", 36), ("RtRenderParams", 104),
+                                         ("RtCameraDesc", 48), ("RtMediumDesc", 36), ("RtRenderParams", 112),
                                          ("RtStats", 144), ("RtBsdfQuery", 96), ("RtBsdfResult", 80),
                                          ("RtRequest", 72), ("RtSceneInfo", 64), ("RtWorldDesc", 184),
-                                         ("RtCapture", 64), ("RtSceneOptions", 32)])
+                                         ("RtCapture", 64), ("RtSceneOptions", 32), ("RtMediumQuery", 40),
+                                         ("RtMediumResult", 56)])
 def test_struct_sizes(struct, size):
     """Sizes of the C structs (checked against the header by the C compiler in
     the build: see the static_asserts in kernels.cu)."""
@@ -56,3 +57,4 @@ def test_renderer_params_mirror_reference_defaults():
     p = rt.abi.render_params(8, 8, 4, 3)
     assert p.max_sample_radiance == 10.0 and abs(p.indirect_clamp_factor - 0.25) < 1e-7
     assert p.rr_min_bounces == -1 and p.sort_materials == -1
+    assert p.iteration_limit == 0 and p.shadow_queue_limit == 0   # the test-only limits are off

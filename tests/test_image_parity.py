@@ -1,0 +1,121 @@
+"""Whole-image parity at the oracle's noise floor.
+
+The north star asks for images within relMSE 1e-3 of a 65 536-sample reference
+render. Here the GPU renders each scene at 65 536 samples per pixel (Sobol
+indices [0, 65536)), with the megakernel and with the wavefront, and the
+committed oracle renders (tests/golden/oracle_images.npz, made by
+tests/golden/make_reference_images.py) hold 4096 samples from the disjoint
+range [65536, 69632), as two halves of 2048.
+
+If the GPU estimates the same image as the oracle, the difference between
+the two is the oracle's own noise (plus the GPU's, 16 times smaller). So:
+
+- relMSE(oracle, GPU) must sit at the noise floor that the oracle's two halves
+  measure pixel by pixel (their squared difference over four is the
+  variance of their mean);
+- each channel's whole-image mean difference, divided by its standard error
+  from the same per-pixel variances, stays within 4.5 standard errors, and
+  every 8x8 tile's within 5 (192 tiles per image). A 1% bias in the estimator
+  (Russian roulette, the clamps, the MIS weights, Beer-Lambert,
+  Renderer.cs:1008-1383) moves the whole-image z by tens of standard errors
+  on these scenes (C5's literal medium, optical depth 11 across the box, is
+  the exception: there one standard error of the image mean is 0.6%, and its
+  10x thinner variant carries the estimator check).
+
+relMSE = mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2), on linear
+HDR after the per-sample clamp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rt
+
+abi = rt.abi
+GOLDEN = os.path.join(ROOT, "tests", "golden", "oracle_images.npz")
+
+FLOOR_MARGIN = 1.5    # relMSE may exceed the estimated floor by this factor (estimation noise)
+Z_MAX = 4.5           # whole-image mean per channel
+Z_MAX_TILE = 5.0      # each of the 3 x 64 tiles
+ROUNDING = 1e-4       # float32 summation of the oracle's 2048 samples per pixel and half
+
+
+def _golden():
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_reference_images as m
+    return m, np.load(GOLDEN)
+
+
+def rel_weights(ref):
+    return 1.0 / (ref.astype(np.float64) ** 2 + 1e-2)
+
+
+def parity_stats(a, b, g, gpu_spp_ratio):
+    """a, b: the oracle's halves; g: the GPU image whose samples are
+    `gpu_spp_ratio` times the oracle's 4096. Returns (relMSE, floor, tile z,
+    channel z)."""
+    a, b, g = (x.astype(np.float64) for x in (a, b, g))
+    o = 0.5 * (a + b)
+    var_o = 0.25 * (a - b) ** 2               # variance of the oracle's mean, per pixel
+    var = var_o * (1.0 + 1.0 / gpu_spp_ratio)  # of the difference oracle - GPU
+    # A pixel whose every sample returns the same value (the sky, say) has no
+    # variance, but the oracle sums each half's 2048 samples in float32, one
+    # addition after another, and that drifts by up to ~6e-5 of the value (the
+    # GPU sums in double): a floor of ROUNDING relative to the value.
+    var = var + (ROUNDING * np.abs(o)) ** 2 + 1e-20
+    w = rel_weights(g)
+    rel = float(np.mean((o - g) ** 2 * w))
+    floor = float(np.mean(var * w))
+    c, h, wd = o.shape
+    d = (o - g).reshape(c, h // 8, 8, wd // 8, 8)
+    v = var.reshape(c, h // 8, 8, wd // 8, 8)
+    tz = d.sum(axis=(2, 4)) / np.sqrt(v.sum(axis=(2, 4)))
+    cz = (o - g).sum(axis=(1, 2)) / np.sqrt(var.sum(axis=(1, 2)))
+    return rel, floor, tz, cz
+
+
+def test_oracle_halves_are_consistent_and_noisy():
+    """CPU check of the fixtures: the halves agree in the mean (their own
+    z-test), differ pixel by pixel (independent samples) and are finite."""
+    m, g = _golden()
+    assert int(g["width"]) == m.WIDTH and int(g["half_spp"]) == m.HALF_SPP
+    for name in m.scenes():
+        a, b = g[f"{name}_a"].astype(np.float64), g[f"{name}_b"].astype(np.float64)
+        assert a.shape == (3, m.HEIGHT, m.WIDTH) and np.all(np.isfinite(a)) and np.all(np.isfinite(b))
+        assert np.mean(a != b) > 0.5, name
+        var_half = 0.5 * (a - b) ** 2   # per-pixel variance of one half, twice over
+        z = (a - b).sum(axis=(1, 2)) / np.sqrt(2 * var_half.sum(axis=(1, 2)))
+        assert np.all(np.abs(z) < Z_MAX), (name, z)
+
+
+SCENE_NAMES = ["cornell", "cornell_sphere", "sky", "cornell_spheres", "volume", "volume_thin"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [abi.KERNEL_MEGAKERNEL, abi.KERNEL_WAVEFRONT])
+@pytest.mark.parametrize("name", SCENE_NAMES)
+def test_gpu_image_at_the_oracle_noise_floor(name, kernel):
+    m, gold = _golden()
+    world, depth = m.scenes()[name]
+    lib = abi.load()
+    pw = abi.PackedWorld(world)
+    h = C.c_void_p()
+    abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
+    try:
+        p = abi.render_params(m.WIDTH, m.HEIGHT, m.GPU_SPP, depth, kernel=kernel)
+        img = np.zeros((3, m.HEIGHT, m.WIDTH), np.float32)
+        st = abi.RtStats()
+        abi.check(lib.rt_render(h, C.byref(p), abi.ptr(img), C.byref(st)), "rt_render")
+    finally:
+        lib.rt_scene_destroy(h)
+    assert st.samples == m.WIDTH * m.HEIGHT * m.GPU_SPP and np.all(np.isfinite(img))
+    rel, floor, tz, cz = parity_stats(gold[f"{name}_a"], gold[f"{name}_b"], img, m.GPU_SPP / (2 * m.HALF_SPP))
+    assert rel <= FLOOR_MARGIN * floor, (name, rel, floor)
+    assert np.all(np.abs(cz) < Z_MAX), (name, cz)
+    worst = np.unravel_index(np.argmax(np.abs(tz)), tz.shape)
+    assert np.abs(tz).max() < Z_MAX_TILE, (name, worst, tz[worst])

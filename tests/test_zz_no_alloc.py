@@ -4,8 +4,8 @@ start-up, or a latency-critical render thread where the device-synchronising
 cudaMalloc/cudaFree are not allowed). Its scratch lives in one fixed array in
 the library; this test checks, through the C-ABI, that two calls in a row give
 the same film as the allocating rt_render_device, and that an oversized
-window is refused. Collected last so that a run stopping at the first failure
-has already run every other test."""
+window and a wavefront request are refused. Collected last so that a run
+stopping at the first failure has already run every other test."""
 from __future__ import annotations
 
 import ctypes as C
@@ -53,5 +53,10 @@ def test_noalloc_matches_allocating_render_twice(cornell_world):
         big = abi.render_params(4096, 4096, 1, 1, kernel=abi.KERNEL_MEGAKERNEL)
         rc = lib.rt_render_device_noalloc(h, C.byref(big), C.c_void_p(ref.data_ptr()), C.byref(st2))
         assert rc == -1 and b"allocation-free maximum" in lib.rt_last_error()
+        # the wavefront's queues need allocated memory: a wavefront request is
+        # refused, not silently rendered by the megakernel
+        wf = abi.render_params(W, H, 64, 8, kernel=abi.KERNEL_WAVEFRONT)
+        rc = lib.rt_render_device_noalloc(h, C.byref(wf), C.c_void_p(ref.data_ptr()), C.byref(st2))
+        assert rc == -1 and b"megakernel" in lib.rt_last_error()
     finally:
         lib.rt_scene_destroy(h)
