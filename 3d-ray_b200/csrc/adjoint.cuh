@@ -409,6 +409,15 @@ RT_D V3 clamp_lum_vjp(V3 cin, float mx, V3 g) {
     return r * keep;
 }
 
+// What the out-of-line hooks read of the path state, passed by value: handing
+// them the PathState itself by reference would take its address and move the
+// whole state out of registers into local memory for the entire replay loop.
+struct PathView {
+    V3 lp, la, mask;
+    int clamp_mode, first;
+};
+RT_D PathView path_view(const PathState& ps) { return PathView{ps.lp, ps.la, ps.mask, ps.clamp_mode, ps.first}; }
+
 // Per-thread adjoint state of one replayed sample, and the replay sink.
 struct AdjointSink {
     const SceneView* s;
@@ -439,11 +448,11 @@ struct AdjointSink {
         else if (acc) atomicAdd(acc + i, v);
         else atomicAdd(gacc + i, (double)v);
     }
-    RT_D V3 gain(const PathState& ps, int to_la) const {   // adjoint of a term added now
+    RT_D V3 gain(const PathView& ps, int to_la) const {   // adjoint of a term added now
         if (!to_la) return g_a;
         return g_la * ps.mask;
     }
-    RT_D void target(const PathState& ps, V3& g, V3& S) const {   // adjoint and radiance still to come
+    RT_D void target(const PathView& ps, V3& g, V3& S) const {   // adjoint and radiance still to come
         if (ps.clamp_mode) {
             g = g_la;
             S = tot_la - ps.la;
@@ -514,7 +523,7 @@ struct AdjointSink {
     // Gradients shared by the surface and medium NEE terms: the emitter's
     // radiance, the medium transmittance over the light distance and the
     // shadow ray's absorption and surface crossings.
-    RT_NI void nee_common(const PathState& ps, int li, float dist, int to_la) {
+    RT_NI void nee_common(PathView ps, int li, float dist, int to_la) {
         V3 gx = gain(ps, to_la) * sh_x;
         if (is_zero(gx)) return;
         const Light& l = s->lights[li];
@@ -568,7 +577,7 @@ struct AdjointSink {
 
     RT_D void segment(const PathState& ps, float t, int mode) {
         V3 g, S;
-        target(ps, g, S);
+        target(path_view(ps), g, S);
         V3 gs = g * S;
         if (is_zero(gs)) return;
         if (mode != SEG_MEDIUM_PASS && abs_mat >= 0) {
@@ -591,7 +600,7 @@ struct AdjointSink {
     }
 
     RT_D void emission(const PathState& ps, int mat, V3 we, int to_la) {
-        V3 g = gain(ps, to_la) * ps.w * we;
+        V3 g = gain(path_view(ps), to_la) * ps.w * we;
         const Material& m = s->materials[mat];
         int b = mat * kAdjPerMat;
         if (m.emission.x > 0.0f) add(b + 0, g.x / m.emission.x);
@@ -599,9 +608,12 @@ struct AdjointSink {
         if (m.emission.z > 0.0f) add(b + 2, g.z / m.emission.z);
     }
 
-    RT_NI void nee_surface(const PathState& ps, int li, const Material& m, const Surface& rec, V3 L, V3 V,
-                           float term, V3 coef, float dist, V3 tr_m, int to_la) {
-        if (!sh_added) return;
+    RT_D void nee_surface(const PathState& ps, int li, const Material& m, const Surface& rec, V3 L, V3 V,
+                          float term, V3 coef, float dist, V3 tr_m, int to_la) {
+        if (sh_added) nee_surface_impl(path_view(ps), li, m, rec, L, V, term, coef, dist, tr_m, to_la);
+    }
+    RT_NI void nee_surface_impl(PathView ps, int li, const Material& m, const Surface& rec, V3 L, V3 V,
+                                float term, V3 coef, float dist, V3 tr_m, int to_la) {
         nee_common(ps, li, dist, to_la);
         // the term is coef * (f_direct * term) * tr_m * tr: differentiate f_direct
         unsigned bits = mmask[rec.material] & ((1u << kAdjBsdfDirs) - 1u);
@@ -616,11 +628,16 @@ struct AdjointSink {
         }
     }
     RT_D void nee_medium(const PathState& ps, int li, float dist, int to_la) {
-        if (sh_added) nee_common(ps, li, dist, to_la);
+        if (sh_added) nee_common(path_view(ps), li, dist, to_la);
     }
 
-    RT_NI void scatter(const PathState& ps, const Material& m, const Surface& rec, V3 V, V3 dir, int lobe, int mode,
-                       float pdf, V3 att_pre, V3 att, int null_lobe, V3 null_dir) {
+    RT_D void scatter(const PathState& ps, const Material& m, const Surface& rec, V3 V, V3 dir, int lobe, int mode,
+                      float pdf, V3 att_pre, V3 att, int null_lobe, V3 null_dir) {
+        if (mmask[rec.material] & ((1u << kAdjBsdfDirs) - 1u))
+            scatter_impl(path_view(ps), m, rec, V, dir, lobe, mode, pdf, att_pre, att, null_lobe, null_dir);
+    }
+    RT_NI void scatter_impl(PathView ps, const Material& m, const Surface& rec, V3 V, V3 dir, int lobe, int mode,
+                            float pdf, V3 att_pre, V3 att, int null_lobe, V3 null_dir) {
         unsigned bits = mmask[rec.material] & ((1u << kAdjBsdfDirs) - 1u);
         if (!bits) return;
         V3 coef;

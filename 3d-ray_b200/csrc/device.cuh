@@ -125,9 +125,31 @@ struct Counters {
 
 RT_D V3 ld3(const float4& f) { return v3(f.x, f.y, f.z); }
 
+// Read-only load of scene data (BVH records, triangles, entity boxes) with an
+// L2 evict-last policy. The path state the wavefront streams each iteration
+// (~0.6 GB at 4 M slots) is far larger than the 126 MB L2; without the hint it
+// pushes the ~86 MB scene of the icosphere field out of L2 between the
+// traversal kernels. A hint: results are unchanged.
+#ifndef RT_L2_HINTS
+#define RT_L2_HINTS 1
+#endif
+RT_D float4 ldg_scene(const float4* p) {
+#if RT_L2_HINTS
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    float4 v;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p), "l"(pol));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
 // Geometry/Triangle.cs:49-89 (Moller-Trumbore, |a| < 1e-7 reject, inclusive t range)
 RT_D bool tri_test(const float4* tris, int i, V3 o, V3 d, float tmin, float tmax, float& t, float& u, float& v) {
-    float4 a0 = __ldg(tris + 3 * i), a1 = __ldg(tris + 3 * i + 1), a2 = __ldg(tris + 3 * i + 2);
+    float4 a0 = ldg_scene(tris + 3 * i), a1 = ldg_scene(tris + 3 * i + 1), a2 = ldg_scene(tris + 3 * i + 2);
     V3 v0 = ld3(a0), e1 = ld3(a1), e2 = ld3(a2);
     V3 h = cross(d, e2);
     float a = dot(e1, h);
@@ -279,7 +301,7 @@ struct Walker {
         // Descend interior records: test both children, go near, stack far.
         while (code >= 0) {
             const float4* np = s.cnodes + (size_t)RT_IX(code, s.n_cnodes) * 4;
-            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), e = __ldg(np + 3);
+            float4 a = ldg_scene(np), b = ldg_scene(np + 1), c = ldg_scene(np + 2), e = ldg_scene(np + 3);
             if (cnt) cnt->nodes += 2;
             float tel, ter;
             bool hl = box_hit_te(a.x, a.y, a.z, b.x, b.y, b.z, o, inv, tmin, closest, tel);
@@ -315,8 +337,8 @@ struct Walker {
                 if (en.kind == ENT_MESH) {   // Mesh.Hit -> its BVH root (box test) or flat list
                     if (en.index >= 0) {
                         if (cnt) cnt->nodes++;
-                        float4 lo = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities)),
-                               hi = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
+                        float4 lo = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities)),
+                               hi = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
                         float te;
                         if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
                             code = en.index;
@@ -405,14 +427,19 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
         // Descend interior records: test both children, go near, stack far.
         while (code >= 0) {
             const float4* np = s.cnodes + (size_t)RT_IX(code, s.n_cnodes) * 4;
-            float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), e = __ldg(np + 3);
+            float4 a = ldg_scene(np), b = ldg_scene(np + 1), c = ldg_scene(np + 2), e = ldg_scene(np + 3);
             if (cnt) cnt->nodes += 2;
             float tel, ter;
             bool hl = box_hit_te(a.x, a.y, a.z, b.x, b.y, b.z, o, inv, tmin, closest, tel);
             bool hr = box_hit_te(c.x, c.y, c.z, e.x, e.y, e.z, o, inv, tmin, closest, ter);
             int axis = __float_as_int(c.w);
             float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
-            bool left_near = da >= 0.0f;
+            // An opaque any-hit answer does not depend on the visit order, so
+            // that walk enters the child whose box the ray meets first (an
+            // occluder near the origin ends it sooner); every other walk, and
+            // the counting build, keeps BvhNode's order (near child by the sign
+            // of the ray along the split axis).
+            bool left_near = (ANY && !cnt) ? (tel <= ter) : (da >= 0.0f);
             int lc = __float_as_int(a.w), rc = __float_as_int(b.w);
             int nc = left_near ? lc : rc, fc = left_near ? rc : lc;
             bool hn = left_near ? hl : hr, hf = left_near ? hr : hl;
@@ -438,8 +465,8 @@ __device__ __forceinline__ bool traverse(const SceneView& s, V3 o, V3 d, float t
                 if (en.kind == ENT_MESH) {   // Mesh.Hit -> its BVH root (box test) or flat list
                     if (en.index >= 0) {
                         if (cnt) cnt->nodes++;
-                        float4 lo = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities)),
-                               hi = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
+                        float4 lo = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities)),
+                               hi = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
                         float te;
                         if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
                             code = en.index;
@@ -528,9 +555,9 @@ __device__ __forceinline__ bool traverse4(const SceneView& s, V3 o, V3 d, float 
     for (;;) {
         while (code >= 0) {
             const float4* q = s.cnodes4 + (size_t)RT_IX(code, s.n_cnodes4) * 8;
-            float4 lx = __ldg(q), ly = __ldg(q + 1), lz = __ldg(q + 2);
-            float4 hx = __ldg(q + 3), hy = __ldg(q + 4), hz = __ldg(q + 5);
-            float4 cc = __ldg(q + 6), mt = __ldg(q + 7);
+            float4 lx = ldg_scene(q), ly = ldg_scene(q + 1), lz = ldg_scene(q + 2);
+            float4 hx = ldg_scene(q + 3), hy = ldg_scene(q + 4), hz = ldg_scene(q + 5);
+            float4 cc = ldg_scene(q + 6), mt = ldg_scene(q + 7);
             int c0 = __float_as_int(cc.x), c1 = __float_as_int(cc.y), c2 = __float_as_int(cc.z),
                 c3 = __float_as_int(cc.w);
             float t0, t1, t2, t3;
@@ -577,8 +604,8 @@ __device__ __forceinline__ bool traverse4(const SceneView& s, V3 o, V3 d, float 
                 if (en.kind == ENT_MESH) {
                     int r4 = __ldg(s.mesh_root4 + RT_IX(first, s.n_entities));
                     if (en.index >= 0) {
-                        float4 lo = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities)),
-                               hi = __ldg(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
+                        float4 lo = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities)),
+                               hi = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
                         float te;
                         if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, closest, te)) {
                             code = r4;
@@ -628,10 +655,108 @@ __device__ __forceinline__ bool traverse4(const SceneView& s, V3 o, V3 d, float 
     }
 }
 
+// Opaque any-hit over the four-wide records. The answer (is anything hit in
+// [tmin, tmax]) does not depend on the visit order, so this walk keeps none:
+// every hit slot of a record is taken, the first one at once and the others
+// from a stack of codes, and the first accepted primitive ends the walk. A
+// grandchild box holds every primitive below it, so no primitive the
+// two-wide walk could hit is skipped.
+template <int STACK>
+__device__ __forceinline__ bool traverse4_any(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
+                                              int* err) {
+    const int kNone = INT_MIN;
+    V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);   // Core/Ray.cs:43
+    int stc[STACK];
+    int sp = 0;
+    best.kind = HIT_NONE;
+    int code = kNone;
+    if (s.top_is_bvh) {
+        code = s.top_root4;
+    } else {
+        for (int i = s.num_top_items - 1; i >= 0; --i) stc[sp++] = leaf_code(s.top_items[RT_IX(i, s.num_top_items)],
+                                                                                LEAF_ENT1, 1);
+    }
+    for (;;) {
+        while (code >= 0) {
+            const float4* q = s.cnodes4 + (size_t)RT_IX(code, s.n_cnodes4) * 8;
+            float4 lx = ldg_scene(q), ly = ldg_scene(q + 1), lz = ldg_scene(q + 2);
+            float4 hx = ldg_scene(q + 3), hy = ldg_scene(q + 4), hz = ldg_scene(q + 5);
+            float4 cc = ldg_scene(q + 6);
+            float te;
+            int c[4] = {__float_as_int(cc.x), __float_as_int(cc.y), __float_as_int(cc.z), __float_as_int(cc.w)};
+            bool h[4];
+            h[0] = c[0] != kNone && box_hit_te(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, o, inv, tmin, tmax, te);
+            h[1] = c[1] != kNone && box_hit_te(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, o, inv, tmin, tmax, te);
+            h[2] = c[2] != kNone && box_hit_te(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, o, inv, tmin, tmax, te);
+            h[3] = c[3] != kNone && box_hit_te(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, o, inv, tmin, tmax, te);
+            code = kNone;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (!h[j]) continue;
+                if (code == kNone) {
+                    code = c[j];
+                } else {
+                    if (sp >= STACK) {
+                        *err = RT_ERR_STACK;
+                        return false;
+                    }
+                    stc[sp++] = c[j];
+                }
+            }
+        }
+        if (code != kNone) {
+            int v = ~code;
+            int first = v >> 5;
+            int kind = (v >> 3) & 3;
+            int count = (v & 7) + 1;
+            code = kNone;
+            if (kind == LEAF_ENT1) {
+                Entity en = s.entities[RT_IX(first, s.n_entities)];
+                if (en.kind == ENT_MESH) {
+                    int r4 = __ldg(s.mesh_root4 + RT_IX(first, s.n_entities));
+                    if (en.index >= 0) {
+                        float4 lo = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities)),
+                               hi = ldg_scene(s.ent_box + 2 * RT_IX(first, s.n_entities) + 1);
+                        float te;
+                        if (box_hit_te(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, o, inv, tmin, tmax, te)) code = r4;
+                    } else {
+                        code = r4;
+                    }
+                    if (code != kNone) continue;
+                } else {
+                    Hit hh;
+                    if (entity_test(s, first, o, d, tmin, tmax, hh)) {
+                        best = hh;
+                        return true;
+                    }
+                }
+            } else if (kind == LEAF_ENTS) {
+                if (sp + count > STACK) {
+                    *err = RT_ERR_STACK;
+                    return false;
+                }
+                for (int i = count - 1; i >= 0; --i)
+                    stc[sp++] = leaf_code(s.top_items[RT_IX(first + i, s.num_top_items)], LEAF_ENT1, 1);
+            } else {
+                for (int i = 0; i < count; i++) {
+                    float t, u, vv;
+                    if (tri_test(s.tris, RT_IX(first + i, s.n_tris), o, d, tmin, tmax, t, u, vv)) {
+                        best = Hit{t, u, vv, HIT_TRI, first + i};
+                        return true;
+                    }
+                }
+            }
+        }
+        if (sp == 0) return true;
+        code = stc[--sp];
+    }
+}
+
 // The node layout as a template switch (counting builds use the two-wide one).
 template <bool ANY, int STACK, bool L4>
 __device__ __forceinline__ bool trace(const SceneView& s, V3 o, V3 d, float tmin, float tmax, Hit& best,
                                       TravCounters* cnt, int* err) {
+    if (L4 && ANY) return traverse4_any<STACK>(s, o, d, tmin, tmax, best, err);
     if (L4) return traverse4<ANY, STACK>(s, o, d, tmin, tmax, best, err);
     return traverse<ANY, STACK>(s, o, d, tmin, tmax, best, cnt, err);
 }
@@ -653,7 +778,7 @@ RT_D Surface make_surface(const SceneView& s, const Hit& h, V3 o, V3 d) {
     if (h.kind == HIT_TRI) {
         int ti = RT_IX(h.slot, s.n_tris);
         const float4* tp = s.tris + 3 * ti;
-        float4 a0 = __ldg(tp), a1 = __ldg(tp + 1), a2 = __ldg(tp + 2);
+        float4 a0 = ldg_scene(tp), a1 = ldg_scene(tp + 1), a2 = ldg_scene(tp + 2);
         V3 e1 = ld3(a1), e2 = ld3(a2);
         V3 n = v3(a0.w, a1.w, a2.w);
         r.front = dot(d, n) < 0.0f;   // HitRecord.SetFaceNormal
@@ -1641,7 +1766,7 @@ __device__ __noinline__ float mesh_light_pdf(const SceneView& s, const Light& l,
     if (err || h.kind == HIT_NONE) return 0.0f;
     int ti = RT_IX(h.slot, s.n_tris);
     const float4* tp = s.tris + 3 * ti;
-    V3 n = v3(__ldg(tp).w, __ldg(tp + 1).w, __ldg(tp + 2).w);
+    V3 n = v3(ldg_scene(tp).w, ldg_scene(tp + 1).w, ldg_scene(tp + 2).w);
     int si = s.tri_smooth ? s.tri_smooth[ti] : -1;
     if (si >= 0) {   // the hit record's normal is the interpolated one
         const SmoothTri& st = s.smooth[RT_IX(si, s.n_smooth)];

@@ -234,35 +234,48 @@ def rel_mse(x, r):
     return float(np.mean((x - r) ** 2 / (r ** 2 + 1e-2)))
 
 
-def time_to_relmse(rt, lib, abi, kernels=("wavefront", "megakernel"), target=1e-3):
-    """Cornell box 256x256, depth 8: seconds of device time until relMSE <= 1e-3
-    against a 65 536-spp reference (rendered from a disjoint Sobol range so it
-    is uncorrelated with the test images)."""
+def time_to_relmse_on(lib, abi, h, width, height, depth, window=None, target=1e-3,
+                      kernels=("wavefront", "megakernel")):
+    """Seconds of device time until a render reaches relMSE <= target against
+    a 65 536-spp wavefront reference of the same frame (or window), rendered
+    from a disjoint Sobol range so that it is uncorrelated with the test
+    images; spp doubles from 16."""
     import torch
-    world = rt.scenes.cornell()
-    pw = abi.PackedWorld(world)
-    h = C.c_void_p()
-    abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
-    Wc = Hc = 256
-    film = torch.empty((3, Hc, Wc), dtype=torch.float32, device="cuda")
+    x0, y0, ww, wh = window or (0, 0, width, height)
+    win = dict(pixel_x0=x0, pixel_y0=y0, window_w=ww, window_h=wh) if window else {}
+    film = torch.empty((3, height, width), dtype=torch.float32, device="cuda")
     st = abi.RtStats()
     ref_spp = 65536
-    p = abi.render_params(Wc, Hc, ref_spp, 8, kernel=abi.KERNEL_WAVEFRONT, spp_offset=1 << 20)
+    p = abi.render_params(width, height, ref_spp, depth, kernel=abi.KERNEL_WAVEFRONT, spp_offset=1 << 20, **win)
     abi.check(lib.rt_render_device(h, C.byref(p), C.c_void_p(film.data_ptr()), C.byref(st)), "reference")
-    ref = film.cpu().numpy().copy()
-    out = {"workload": "cornell 256x256 depth 8", "reference_spp": ref_spp, "target": target}
+    ref = film[:, y0:y0 + wh, x0:x0 + ww].cpu().numpy().copy()
+    out = {"reference_spp": ref_spp, "reference_seconds": st.kernel_ms / 1e3, "target": target}
     for kname in kernels:
         kid = abi.KERNEL_WAVEFRONT if kname == "wavefront" else abi.KERNEL_MEGAKERNEL
         spp = 16
         while spp <= 16384:
-            p = abi.render_params(Wc, Hc, spp, 8, kernel=kid)
+            p = abi.render_params(width, height, spp, depth, kernel=kid, **win)
             abi.check(lib.rt_render_device(h, C.byref(p), C.c_void_p(film.data_ptr()), C.byref(st)), kname)
-            e = rel_mse(film.cpu().numpy(), ref)
+            e = rel_mse(film[:, y0:y0 + wh, x0:x0 + ww].cpu().numpy(), ref)
             if e <= target:
                 out[kname] = {"seconds": st.kernel_ms / 1e3, "spp": spp, "rel_mse": e}
                 break
             spp *= 2
-    lib.rt_scene_destroy(h)
+    if "wavefront" in out and "megakernel" in out:
+        out["speedup_wavefront"] = out["megakernel"]["seconds"] / out["wavefront"]["seconds"]
+    return out
+
+
+def time_to_relmse(rt, lib, abi):
+    """Cornell box 256x256, depth 8 (the C1 frame at the configuration's size)."""
+    pw = abi.PackedWorld(rt.scenes.cornell())
+    h = C.c_void_p()
+    abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
+    try:
+        out = {"workload": "cornell 256x256 depth 8"}
+        out.update(time_to_relmse_on(lib, abi, h, 256, 256, 8))
+    finally:
+        lib.rt_scene_destroy(h)
     return out
 
 
@@ -455,8 +468,11 @@ def gradcheck(args):
             d = adj[:, j] - fd[:, j]
             ma, mf = float(adj[:, j].mean()), float(fd[:, j].mean())
             se = float(d.std(ddof=1) / np.sqrt(nb))
-            rows[key] = {"adjoint": ma, "fd": mf, "eps": eps, "rel_err": abs(ma - mf) / max(abs(mf), 1e-30),
-                         "diff_stderr_rel": se / max(abs(mf), 1e-30), "z": float(d.mean() / se) if se > 0 else 0.0}
+            den = max(abs(mf), 1e-30)
+            rows[key] = {"adjoint": ma, "fd": mf, "eps": eps, "rel_err": abs(ma - mf) / den,
+                         "diff_stderr_rel": se / den, "z": float(d.mean() / se) if se > 0 else 0.0,
+                         "adjoint_stderr_rel": float(adj[:, j].std(ddof=1) / np.sqrt(nb)) / den,
+                         "fd_stderr_rel": float(fd[:, j].std(ddof=1) / np.sqrt(nb)) / den}
         n = res * res * rp.spp * nb
         print(json.dumps({"gradcheck": name, "clamps": clamps, "image": f"{res}x{res}", "samples": n,
                           "batches": nb, "adjoint_ms": adj_ms, "adjoint_msamples_per_s": n / adj_ms / 1e3,
@@ -751,6 +767,12 @@ def main():
         line["plain_kernel"] = {"value": mv, "unit": UNIT, "ms_per_step": mt, "speedup_wavefront": value / mv}
         if rank == 0:
             line["time_to_relmse_1e-3"] = time_to_relmse(rt, lib, abi)
+            # the bench frame itself: a 256x256 window at its centre (a 65 536-spp
+            # reference of the whole 1080p frame would take minutes)
+            win = ((W - 256) // 2, (H - 256) // 2, 256, 256)
+            t2 = {"workload": f"icospheres {W}x{H} depth {DEPTH}, window {win}"}
+            t2.update(time_to_relmse_on(lib, abi, scene, W, H, DEPTH, window=win))
+            line["time_to_relmse_1e-3_icospheres"] = t2
             line.update(batched_side(rt))
             line["c1"] = c1_side(rt, lib, abi)
             line["bvh_build"] = bvh_build_side(lib, abi, pw)
