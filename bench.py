@@ -405,28 +405,50 @@ def gradcheck(args):
     """The path-replay adjoint against central finite differences under common
     random numbers: C4 (the Cornell box with a Disney sphere: the sphere's
     baseColor, roughness, metallic, specular and sheen, and the emitter's
-    radiance), once with the reference's luminance clamps and once without, and
-    C5 (the medium's sigma_a and sigma_s and the glass sphere's absorption). The
-    samples are split into 8 independent Sobol batches; per parameter the line
-    gives the mean adjoint and finite-difference gradients, their relative
-    difference, and the standard error of the per-batch difference. The loss is
-    a fixed random weighting of the HDR film."""
+    radiance, with the reference's luminance clamps), C5 (the medium's
+    sigma_a and sigma_s and the glass sphere's absorption) and the absorption
+    of a glass sphere of optical depth ~1 under the flat sky (C5's glass, 90
+    units of radius at sigma_a (0.1, 0.3, 0.5), passes e^-18 of the light or
+    less, so its absorption gradient is close to zero).
+
+    Each parameter gets its own linear loss L = sum(w * film), with w the sign
+    of that parameter's finite-difference image from an independent pilot
+    render: every pixel's change then adds to the gradient instead of partly
+    cancelling, so the gradient stands well above the sampling noise (a fixed
+    weighting: the pilot's samples are disjoint from the check's). The check's
+    samples are split into 8 independent Sobol batches; in each, the adjoint
+    (rt_adjoint) and the central difference of two wavefront renders of the
+    same samples at theta +- eps estimate dL/dtheta. Per parameter the line
+    gives both means, their relative difference, the standard error of the
+    per-batch difference and of each estimate, all relative to the
+    finite-difference mean."""
     rt = load_package()
     abi = rt.abi
     spp = args.spp if args.spp != SPP else 16384
     nb = 8
+    only = [x for x in args.gc_params.split(",") if x] if args.gc_params else []
     sphere = dict(base_color=(0.6, 0.3, 0.2), roughness=0.4, metallic=0.2, specular=0.6, sheen=0.3)
-    for name, clamps in (("c4", True), ("c4", False), ("c5", True)):
+    for name in ("c4", "c5", "glass"):
+        if only and not any(o.startswith(name + ":") for o in only):
+            continue
         if name == "c4":
             w = rt.scenes.cornell_sphere(sphere)
-            res = 64
-        else:
+            res, depth = 64, 8
+        elif name == "c5":
             w = rt.scenes.cornell_volume()
-            res = 48
+            res, depth = 48, 16
+        else:   # a glass sphere of optical depth ~1 under the sky (C5's glass transmits e^-18 and less)
+            w = rt.scenes.sky_scene()
+            res, depth = 48, 8
         ds = rt.DiffScene(w)
-        kw = {} if clamps else dict(max_sample_radiance=1e30, indirect_clamp_factor=1.0)
-        rp = abi.render_params(res, res, max(spp // nb, 1), 8, kernel=abi.KERNEL_MEGAKERNEL, **kw)
-        wimg = np.random.default_rng(1).uniform(0.0, 1.0, (3, res, res)).astype(np.float32)
+        kw = dict(max_sample_radiance=1e30, indirect_clamp_factor=1.0) if args.gc_no_clamps else {}
+        per = max(spp // nb, 1)
+        # the finite differences may take more samples per batch than the
+        # adjoint (the adjoint's are the first of them), and a larger eps
+        fper = max(per, args.gc_fd_spp // nb) if args.gc_fd_spp else per
+        rp = abi.render_params(res, res, per, depth, kernel=abi.KERNEL_MEGAKERNEL, **kw)
+        rw = abi.render_params(res, res, fper, depth, kernel=abi.KERNEL_WAVEFRONT, **kw)
+        pilot = abi.render_params(res, res, 2048, depth, kernel=abi.KERNEL_WAVEFRONT, spp_offset=1 << 24, **kw)
         theta = ds.get_params()
         if name == "c4":
             slots = {f"sphere.base_color[{c}]": (ds.slot("fit_sphere", "base_color", c), 1e-3) for c in range(3)}
@@ -435,7 +457,7 @@ def gradcheck(args):
             for c in range(3):
                 i = ds.slot("light", "radiance", c)
                 slots[f"light.radiance[{c}]"] = (i, 1e-3 * float(theta[i]))
-        else:
+        elif name == "c5":
             slots = {}
             for c in range(3):
                 for nm in ("sigma_a", "sigma_s"):
@@ -443,39 +465,56 @@ def gradcheck(args):
                     slots[f"medium.{nm}[{c}]"] = (i, 1e-2 * float(theta[i]))
                 i = ds.slot("glass", "absorption", c)
                 slots[f"glass.absorption[{c}]"] = (i, 1e-2 * float(theta[i]))
-        idx = [i for i, _ in slots.values()]
+        else:
+            slots = {f"glass.absorption[{c}]": (ds.slot("glass", "absorption", c),
+                                                1e-2 * float(theta[ds.slot("glass", "absorption", c)]))
+                     for c in range(3)}
 
-        def loss(th):
+        if only:
+            slots = {k: (i, e * args.gc_eps) for k, (i, e) in slots.items()
+                     if any(o == f"{name}:{k}" for o in only)}
+
+        def film_at(i, value, p):
+            th = theta.copy()
+            th[i] = value
             ds.set_params(th)
-            return float((ds.render(rp).astype(np.float64) * wimg).sum())
+            return ds.render(p).astype(np.float64)
 
-        adj = np.zeros((nb, len(idx)))
-        fd = np.zeros((nb, len(idx)))
-        adj_ms = 0.0
-        for b in range(nb):
-            rp.spp_offset = b * rp.spp
-            g = ds.adjoint(rp, wimg, idx)
-            adj_ms += ds.last_stats.kernel_ms
-            for j, (i, eps) in enumerate(slots.values()):
-                tp, tm = theta.copy(), theta.copy()
-                tp[i] += eps
-                tm[i] -= eps
-                fd[b, j] = (loss(tp) - loss(tm)) / (2.0 * eps)
-                adj[b, j] = g[i]
-            ds.set_params(theta)
         rows = {}
-        for j, (key, (i, eps)) in enumerate(slots.items()):
-            d = adj[:, j] - fd[:, j]
-            ma, mf = float(adj[:, j].mean()), float(fd[:, j].mean())
-            se = float(d.std(ddof=1) / np.sqrt(nb))
+        adj_ms, t0 = 0.0, time.time()
+        for key, (i, eps) in slots.items():
+            d = film_at(i, theta[i] + eps, pilot) - film_at(i, theta[i] - eps, pilot)
+            wimg = np.sign(d).astype(np.float32)
+            adj = np.zeros(nb)
+            fd = np.zeros(nb)
+            for b in range(nb):
+                rp.spp_offset = rw.spp_offset = b * fper
+                ds.set_params(theta)
+                adj[b] = ds.adjoint(rp, wimg, [i])[i]
+                adj_ms += ds.last_stats.kernel_ms
+                lp = float((film_at(i, theta[i] + eps, rw) * wimg).sum())
+                lm = float((film_at(i, theta[i] - eps, rw) * wimg).sum())
+                fd[b] = (lp - lm) / (2.0 * eps)
+                if args.gc_richardson:   # (4 D(eps) - D(2 eps)) / 3 cancels the eps^2 term
+                    lp2 = float((film_at(i, theta[i] + 2 * eps, rw) * wimg).sum())
+                    lm2 = float((film_at(i, theta[i] - 2 * eps, rw) * wimg).sum())
+                    fd[b] = (4.0 * fd[b] - (lp2 - lm2) / (4.0 * eps)) / 3.0
+            ds.set_params(theta)
+            diff = adj - fd
+            ma, mf = float(adj.mean()), float(fd.mean())
             den = max(abs(mf), 1e-30)
+            se = float(diff.std(ddof=1) / np.sqrt(nb))
             rows[key] = {"adjoint": ma, "fd": mf, "eps": eps, "rel_err": abs(ma - mf) / den,
-                         "diff_stderr_rel": se / den, "z": float(d.mean() / se) if se > 0 else 0.0,
-                         "adjoint_stderr_rel": float(adj[:, j].std(ddof=1) / np.sqrt(nb)) / den,
-                         "fd_stderr_rel": float(fd[:, j].std(ddof=1) / np.sqrt(nb)) / den}
-        n = res * res * rp.spp * nb
-        print(json.dumps({"gradcheck": name, "clamps": clamps, "image": f"{res}x{res}", "samples": n,
-                          "batches": nb, "adjoint_ms": adj_ms, "adjoint_msamples_per_s": n / adj_ms / 1e3,
+                         "diff_stderr_rel": se / den, "z": float(diff.mean() / se) if se > 0 else 0.0,
+                         "adjoint_stderr_rel": float(adj.std(ddof=1) / np.sqrt(nb)) / den,
+                         "fd_stderr_rel": float(fd.std(ddof=1) / np.sqrt(nb)) / den}
+        n = res * res * per * nb
+        print(json.dumps({"gradcheck": name, "clamps": not args.gc_no_clamps, "image": f"{res}x{res}",
+                          "samples_per_param": n,
+                          "richardson": bool(args.gc_richardson),
+                          "fd_samples_per_param": res * res * fper * nb,
+                          "batches": nb, "loss": "sign of the pilot finite-difference image, per parameter",
+                          "adjoint_msamples_per_s": n * len(slots) / adj_ms / 1e3, "seconds": time.time() - t0,
                           "params": rows}), flush=True)
         ds.close()
 
@@ -522,7 +561,8 @@ def fit(args):
     x_le = torch.tensor(np.log(init_e), dtype=torch.float64, requires_grad=True)
     opt = torch.optim.Adam([x_s, x_le], lr=1e-2)
     mask = s_idx + e_idx
-    hist, hist_truth = [], []
+    hist, hist_truth, traj = [], [], []
+    keys = ["base_r", "base_g", "base_b", "roughness", "metallic", "specular", "sheen"]
     t0 = time.perf_counter()
     adj_ms = 0.0
     for it in range(steps):
@@ -532,9 +572,14 @@ def fit(args):
             hist_truth.append(float(((ds.render(rp).astype(np.float64) - target) ** 2).mean()))
         sv = x_s.detach().numpy().astype(np.float32)
         ev = np.exp(x_le.detach().numpy()).astype(np.float32)
+        if it % 20 == 0:   # the trajectory: every parameter's error before step it
+            traj.append({"step": it, **{k: round(float(abs(a - b)), 4) for k, a, b in zip(keys, sv, truth_s)},
+                         **{f"radiance_{c}": round(float(abs(ev[c] / truth_e[c] - 1)), 4) for c in range(3)}})
         ds.set_params(vec(sv, ev))
+        # the forward film on the wavefront, the adjoint on the same samples
+        rw = abi.render_params(res, res, 32, 8, kernel=abi.KERNEL_WAVEFRONT, spp_offset=it * 32)
         rp = abi.render_params(res, res, 32, 8, kernel=abi.KERNEL_MEGAKERNEL, spp_offset=it * 32)
-        img = ds.render(rp)
+        img = ds.render(rw)
         diff = img.astype(np.float64) - target
         loss = float((diff ** 2).mean())
         g = ds.adjoint(rp, (2.0 * diff / diff.size).astype(np.float32), mask)
@@ -549,7 +594,6 @@ def fit(args):
     wall = time.perf_counter() - t0
     final_s = x_s.detach().numpy()
     final_e = np.exp(x_le.detach().numpy())
-    keys = ["base_r", "base_g", "base_b", "roughness", "metallic", "specular", "sheen"]
     print(json.dumps({
         "fit": "c4", "image": f"{res}x{res}", "steps": steps, "spp_per_step": 32, "lr": 1e-2, "target_spp": 1024,
         "loss_first": hist[0], "loss_last10_mean": float(np.mean(hist[-10:])),
@@ -559,7 +603,7 @@ def fit(args):
         "radiance_rel_err_init": list(map(float, np.abs(init_e / truth_e - 1))),
         "radiance_rel_err_final": list(map(float, np.abs(final_e / truth_e - 1))),
         "seconds": wall, "adjoint_ms_per_step": adj_ms / steps,
-        "loss_curve": [float(h) for h in hist[::max(1, steps // 10)]]}), flush=True)
+        "loss_curve": [float(h) for h in hist[::max(1, steps // 10)]], "trajectory": traj}), flush=True)
     ds.close()
 
 
@@ -586,6 +630,15 @@ def main():
     ap.add_argument("--res", type=int, default=256, help="--fit: square image size")
     ap.add_argument("--gradcheck", action="store_true",
                     help="adjoint gradients against central finite differences (C4, C5) and exit")
+    ap.add_argument("--gc-params", default="",
+                    help="--gradcheck: only these parameters, e.g. c4:sphere.roughness,c5:medium.sigma_s[0]")
+    ap.add_argument("--gc-fd-spp", type=int, default=0,
+                    help="--gradcheck: samples per pixel of the finite differences over all batches (default --spp)")
+    ap.add_argument("--gc-eps", type=float, default=1.0, help="--gradcheck with --gc-params: eps multiplier")
+    ap.add_argument("--gc-no-clamps", action="store_true",
+                    help="--gradcheck: without the luminance clamps (maximum sample radiance, indirect clamp)")
+    ap.add_argument("--gc-richardson", action="store_true",
+                    help="--gradcheck: Richardson-extrapolated differences (4 D(eps) - D(2 eps)) / 3")
     ap.add_argument("--bvh-build", action="store_true",
                     help="build the bench scene's mesh BVHs on the host and twice on the device, print the timings "
                          "and exit (the command profiled by ncu for the device build)")

@@ -478,3 +478,29 @@ def test_regrouped_rays_render_like_slot_order(throughput_world_small, volume_wo
                                            rtol=1e-4, atol=1e-6)
         finally:
             s.close()
+
+
+def test_autotune_picks_a_valid_configuration_that_renders_the_same_image(cornell_world):
+    """rt_autotune times the wavefront's configurations on a slice of the
+    render and keeps the fastest for the scene. Whatever it picks is one of
+    the documented values, and the tuned render (later calls with those fields
+    left at 0 / -1 use it) traces the same samples as the untuned default: the
+    same image up to the order of the float additions."""
+    s = Scene(cornell_world)
+    try:
+        base = abi.render_params(48, 48, 64, 8, kernel=abi.KERNEL_WAVEFRONT)
+        before, _ = s.render(base)
+        best = abi.RtRenderParams()
+        abi.check(s.lib.rt_autotune(s.h, C.byref(base), C.byref(best)), "rt_autotune")
+        assert best.kernel == abi.KERNEL_WAVEFRONT
+        assert best.wavefront_size in (1 << 18, 1 << 20, 1 << 22)
+        assert best.block_size in (64, 128, 256) and best.trace_block_size in (64, 128, 256)
+        assert best.sort_materials in (0, 1) and best.node_layout in (2, 4)
+        assert best.ray_fetch in (1, 2) and best.ray_groups in (1, 2, 3, 4)
+        tuned, st = s.render(base)   # the fields at 0 / -1: the scene's tuned choice
+        explicit, _ = s.render(best)
+        np.testing.assert_allclose(tuned, before, rtol=1e-4, atol=1e-6)
+        np.testing.assert_allclose(explicit, before, rtol=1e-4, atol=1e-6)
+        assert st.samples == 48 * 48 * 64
+    finally:
+        s.close()
