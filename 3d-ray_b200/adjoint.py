@@ -18,6 +18,10 @@ import numpy as np
 
 from . import abi
 
+# Parameter vectors up to this length gather their gradients in per-thread
+# arrays inside the adjoint kernels; longer ones in shared memory.
+ADJ_LOCAL_SLOTS = 128
+
 
 class DiffScene:
     """A scene whose parameter vector can be read, written and differentiated."""

@@ -409,6 +409,35 @@ RT_D V3 clamp_lum_vjp(V3 cin, float mx, V3 g) {
     return r * keep;
 }
 
+// The adjoints of the resolve (path_resolve) for one primal end state (lp,
+// la, pre, att0, clamp_mode) and the sample's film gradient delta: the primal
+// total A, the raw la, and the adjoints of A, la and att0 through the two
+// luminance clamps and the per-frame sanitize.
+struct AdjResolve {
+    V3 tot_a, tot_la, g_a, g_la, g_att0;
+};
+RT_D AdjResolve adjoint_resolve(const RenderConst& rc, V3 lp, V3 la, V3 pre, V3 att0, int clamp_mode, V3 delta) {
+    AdjResolve r;
+    V3 A = lp, X = v3(0.0f);
+    if (clamp_mode) {
+        X = att0 * sanitize(la);
+        A = A + pre * clamp_lum(X, rc.ind_max);
+    }
+    r.tot_a = A;
+    r.tot_la = la;
+    r.g_a = clamp_lum_vjp(A, rc.max_rad, delta);
+    r.g_la = v3(0.0f);
+    r.g_att0 = v3(0.0f);
+    if (clamp_mode) {
+        V3 gx = clamp_lum_vjp(X, rc.ind_max, r.g_a * pre);
+        V3 sl = sanitize(la);
+        r.g_att0 = gx * sl;
+        V3 pos = v3(sl.x > 0.0f ? 1.0f : 0.0f, sl.y > 0.0f ? 1.0f : 0.0f, sl.z > 0.0f ? 1.0f : 0.0f);
+        r.g_la = gx * att0 * pos;
+    }
+    return r;
+}
+
 // What the out-of-line hooks read of the path state, passed by value: handing
 // them the PathState itself by reference would take its address and move the
 // whole state out of registers into local memory for the entire replay loop.
@@ -433,6 +462,13 @@ struct AdjointSink {
     V3 tot_a, tot_la;      // primal A = lp + pre * clamp(att0 * S(la)) and la
     V3 g_a, g_la, g_att0;  // their adjoints
     int abs_mat;           // material of the current interior absorption (-1: none)
+    RT_D void set_resolve(const AdjResolve& r) {
+        tot_a = r.tot_a;
+        tot_la = r.tot_la;
+        g_a = r.g_a;
+        g_la = r.g_la;
+        g_att0 = r.g_att0;
+    }
     // the last shadow ray
     int sh_added;
     V3 sh_x;               // the term it added

@@ -14,6 +14,7 @@
 #include "adjoint.cuh"
 #include "integrator.cuh"
 #include "wavefront.cuh"
+#include "wf_adjoint.cuh"
 #include "world.h"
 
 using rt::V3;
@@ -393,24 +394,7 @@ __global__ void RT_ADJ_BOUNDS k_adjoint(rt::SceneView s, rt::RenderConst rc, Adj
         adj.abs_mat = -1;
         adj.sh_added = 0;
         adj.sh_n = 0;
-        V3 A = pp.lp, X = rt::v3(0.0f), C = rt::v3(0.0f);
-        if (pp.clamp_mode) {
-            X = pp.att0 * rt::sanitize(pp.la);
-            C = rt::clamp_lum(X, rc.ind_max);
-            A = A + pp.pre * C;
-        }
-        adj.tot_a = A;
-        adj.tot_la = pp.la;
-        adj.g_a = rt::clamp_lum_vjp(A, rc.max_rad, delta);
-        adj.g_la = rt::v3(0.0f);
-        adj.g_att0 = rt::v3(0.0f);
-        if (pp.clamp_mode) {
-            V3 gx = rt::clamp_lum_vjp(X, rc.ind_max, adj.g_a * pp.pre);
-            V3 sl = rt::sanitize(pp.la);
-            adj.g_att0 = gx * sl;
-            V3 pos = rt::v3(sl.x > 0.0f ? 1.0f : 0.0f, sl.y > 0.0f ? 1.0f : 0.0f, sl.z > 0.0f ? 1.0f : 0.0f);
-            adj.g_la = gx * pp.att0 * pos;
-        }
+        adj.set_resolve(rt::adjoint_resolve(rc, pp.lp, pp.la, pp.pre, pp.att0, pp.clamp_mode, delta));
         // replay
         rt::PathState ps;
         rt::path_init(ps, rc, px, py, sidx);
@@ -765,9 +749,14 @@ int default_groups(const std::vector<RtScene*>& scenes) {
     return 4;
 }
 
-int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st) {
+// mode: rt::WF_RENDER renders the requests into their films; rt::WF_RECORD
+// and rt::WF_REPLAY are the two passes of the wavefront adjoint over the same
+// requests, with adj holding their buffers (rt_adjoint).
+int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st, int mode = rt::WF_RENDER,
+              const rt::WfAdjoint* adj = nullptr) {
     auto t0 = std::chrono::steady_clock::now();
     if (reqs.empty()) return RT_OK;
+    if (mode != rt::WF_RENDER && !adj) return fail(RT_ERR_INVALID_ARG, "adjoint pass without its buffers");
     std::lock_guard<std::mutex> lk(g_wf_mu);
     RtScene* s0 = reqs[0].scene;
     int dev = s0->device;
@@ -848,6 +837,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     for (auto& q : wreq) add((size_t)3 * q.ww * q.wh * sizeof(double));
     add(reqs.size() * sizeof(float*));
     add(reqs.size() * sizeof(int) * 2);
+    if (mode == rt::WF_REPLAY) add((size_t)nslots * 4 * sizeof(float4));
     need += 1024;
     WfWorkspace& ws = g_wf_ws[dev];
     if (ws.bytes < need) {
@@ -910,6 +900,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     }
     auto* d_films = cv.take<float*>(reqs.size());
     auto* d_fdims = cv.take<int>(2 * reqs.size());
+    if (adj) a.J = *adj;
+    if (mode == rt::WF_REPLAY) a.J.st = cv.take<float4>((size_t)nslots * 4);
     a.views = d_views;
     a.nviews = (int)views.size();
     a.reqs = d_reqs;
@@ -959,7 +951,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     const bool transmit = !a.opaque;
     a.regroup = groups == 2;
     a.raysort = groups >= 3 && !pt;
-    a.shadowsort = groups == 4 && !pt;
+    a.shadowsort = groups == 4 && !pt && mode != rt::WF_REPLAY;   // the replay queues no shadow rays
     // 8x8x8 origin cells x 8x8 direction bins: the measured best of the
     // layouts that fit 15 bits (coarser cells or octant-only directions cost
     // extend 4-13% on the icosphere field)
@@ -981,6 +973,11 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         gpt_e = (unsigned)std::max(1, nb_e * sms);
         gpt_o = (unsigned)std::max(1, nb_o * sms);
     }
+    const int adj_blk = 128;
+    unsigned gadj = (unsigned)((nslots + adj_blk - 1) / adj_blk);
+    size_t adj_shmem = 0;
+    if (mode == rt::WF_REPLAY)
+        adj_shmem = (size_t)(a.J.use_local ? a.J.nact : (a.J.use_shared ? a.J.nparams : 0)) * sizeof(float);
     unsigned gs = (unsigned)((nslots + blk - 1) / blk);
     unsigned gst = (unsigned)((nslots + tblk - 1) / tblk);
     unsigned gsh = (unsigned)((cap + tblk - 1) / tblk);
@@ -990,7 +987,9 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     auto launch_iter = [&](cudaEvent_t* ev) {
         if (ev) cudaEventRecord(ev[0], stream);
         rt::k_wf_reset<<<1, 256, 0, stream>>>(a);
-        rt::k_wf_regen<<<g256, 256, 0, stream>>>(a);
+        if (mode == rt::WF_RECORD) rt::k_wf_regen<rt::WF_RECORD><<<g256, 256, 0, stream>>>(a);
+        else if (mode == rt::WF_REPLAY) rt::k_wf_regen<rt::WF_REPLAY><<<g256, 256, 0, stream>>>(a);
+        else rt::k_wf_regen<rt::WF_RENDER><<<g256, 256, 0, stream>>>(a);
         if (ev) cudaEventRecord(ev[1], stream);
         if (l4) rt::k_wf_extend<kStack, true><<<gst, tblk, 0, stream>>>(a);
         else if (pt) rt::k_wf_extend_pt<kStack><<<gpt_e, tblk, 0, stream>>>(a);
@@ -1001,6 +1000,18 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
             rt::k_wf_scatter<<<g256, 256, 0, stream>>>(a);
         }
         if (ev) cudaEventRecord(ev[3], stream);
+        if (mode == rt::WF_REPLAY) {   // the adjoint vertex, shadow rays inline: no occlude
+            if (medium && transmit) rt::k_wf_adjoint<kStack, true, true><<<gadj, adj_blk, adj_shmem, stream>>>(a);
+            else if (medium) rt::k_wf_adjoint<kStack, true, false><<<gadj, adj_blk, adj_shmem, stream>>>(a);
+            else if (transmit) rt::k_wf_adjoint<kStack, false, true><<<gadj, adj_blk, adj_shmem, stream>>>(a);
+            else rt::k_wf_adjoint<kStack, false, false><<<gadj, adj_blk, adj_shmem, stream>>>(a);
+            if (a.raysort) rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.rhist, a.roff, &d_ctl->nbounce);
+            if (ev) {
+                cudaEventRecord(ev[4], stream);
+                cudaEventRecord(ev[5], stream);
+            }
+            return;
+        }
         if (medium && transmit) rt::k_wf_shade<true, true><<<gs, blk, 0, stream>>>(a);
         else if (medium) rt::k_wf_shade<true, false><<<gs, blk, 0, stream>>>(a);
         else if (transmit) rt::k_wf_shade<false, true><<<gs, blk, 0, stream>>>(a);
@@ -1030,8 +1041,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         // alone (everything else it reads lives in the workspace), so those
         // bytes key the cached one.
         const unsigned shape[] = {(unsigned)blk, (unsigned)tblk, (unsigned)l4, (unsigned)l4_occ, (unsigned)pt,
-                                  (unsigned)medium,
-                                  (unsigned)transmit, gpt_e, gpt_o, gs, gst, gsh, g256, gsh256};
+                                  (unsigned)medium, (unsigned)transmit, gpt_e, gpt_o, gs, gst, gsh, g256, gsh256,
+                                  (unsigned)mode, gadj, (unsigned)adj_shmem};
         std::vector<unsigned char> key(sizeof(a) + sizeof(shape));
         std::memcpy(key.data(), &a, sizeof(a));
         std::memcpy(key.data() + sizeof(a), shape, sizeof(shape));
@@ -1053,7 +1064,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
             ws.exec_key = std::move(key);
         }
     }
-    int per_iter = 5 + (sort ? 2 : 0) + (a.raysort ? 1 : 0) + (a.shadowsort ? 2 : 0);
+    int per_iter = (mode == rt::WF_REPLAY ? 4 : 5) + (sort ? 2 : 0) + (a.raysort ? 1 : 0) + (a.shadowsort ? 2 : 0);
     int max_depth = 1;
     for (auto& q : wreq) max_depth = std::max(max_depth, q.rc.max_depth);
     int64_t limit = (total / nslots + 2) * (int64_t)(max_depth + 2) + 64;
@@ -1122,7 +1133,8 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     if (rc == RT_OK) {
         dim3 g(std::max<unsigned>(1, std::min<unsigned>(4096, (unsigned)((wreq[0].ww * (int64_t)wreq[0].wh + 255) / 256))),
                (unsigned)wreq.size());
-        rt::k_wf_finalize<<<g, 256, 0, stream>>>(d_reqs, (int)wreq.size(), d_films, d_fdims, d_fdims + reqs.size());
+        if (mode == rt::WF_RENDER)
+            rt::k_wf_finalize<<<g, 256, 0, stream>>>(d_reqs, (int)wreq.size(), d_films, d_fdims, d_fdims + reqs.size());
         CUDA_TRY(cudaEventRecord(s0->ev1, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
         rc = check_err(s0);
@@ -1143,7 +1155,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         cudaEventElapsedTime(&ms, s0->ev0, s0->ev1);
         st->kernel_ms = ms;
         st->samples = (uint64_t)total;
-        st->kernel_launches = (int32_t)(iters * per_iter + 1);
+        st->kernel_launches = (int32_t)(iters * per_iter + (mode == rt::WF_RENDER ? 1 : 0));
         st->iterations = (int32_t)iters;
         st->regen_ms = t_regen;
         st->extend_ms = t_extend;
@@ -1159,19 +1171,9 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
 
 WfConfig g_wf_default;
 
-int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam, float* d_film, RtStats* st) {
-    HostReq q;
-    q.scene = sc;
-    q.rc = make_rc(sc, p, cam);
-    q.x0 = p->pixel_x0;
-    q.y0 = p->pixel_y0;
-    q.ww = p->window_w > 0 ? p->window_w : p->width;
-    q.wh = p->window_h > 0 ? p->window_h : p->height;
-    q.spp = p->spp;
-    q.spp0 = p->spp_offset;
-    q.W = p->width;
-    q.H = p->height;
-    q.d_film = d_film;
+// The wavefront configuration of one scene's request: the scene's tuned
+// values, overridden by the request's own.
+int wf_config(const RtScene* sc, const RtRenderParams* p, WfConfig& out) {
     WfConfig cfg = g_wf_default;
     if (sc->tuned) {
         cfg.slots = sc->tuned_slots;
@@ -1195,6 +1197,26 @@ int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam,
         return fail(RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
     if (cfg.tblock != 0 && cfg.tblock != 64 && cfg.tblock != 128 && cfg.tblock != 256)
         return fail(RT_ERR_INVALID_ARG, "trace_block_size must be 64, 128 or 256");
+    out = cfg;
+    return RT_OK;
+}
+
+int wf_render_one(RtScene* sc, const RtRenderParams* p, const RtCameraDesc& cam, float* d_film, RtStats* st) {
+    HostReq q;
+    q.scene = sc;
+    q.rc = make_rc(sc, p, cam);
+    q.x0 = p->pixel_x0;
+    q.y0 = p->pixel_y0;
+    q.ww = p->window_w > 0 ? p->window_w : p->width;
+    q.wh = p->window_h > 0 ? p->window_h : p->height;
+    q.spp = p->spp;
+    q.spp0 = p->spp_offset;
+    q.W = p->width;
+    q.H = p->height;
+    q.d_film = d_film;
+    WfConfig cfg;
+    int rc = wf_config(sc, p, cfg);
+    if (rc != RT_OK) return rc;
     if (p->window_w > 0 || p->window_h > 0)
         CUDA_TRY(cudaMemsetAsync(d_film, 0, (size_t)3 * p->width * p->height * sizeof(float), sc->stream));
     return wf_render({q}, cfg, st);
@@ -1938,6 +1960,50 @@ void put_params(RtScene* sc, const float* in) {
     }
 }
 
+// The wavefront adjoint (params->kernel RT_KERNEL_WAVEFRONT): the samples in
+// runs of whole spp slices of at most kAdjRecord samples, each run rendered
+// once with its end states recorded (WF_RECORD) and then replayed with the
+// gradient hooks (WF_REPLAY). base carries the parameter, mask and gradient
+// buffers; ms and launches add up the passes.
+constexpr long long kAdjRecord = 1LL << 24;   // 64 B per recorded sample: 1 GiB
+
+int wf_adjoint(RtScene* sc, const RtRenderParams* p, const rt::WfAdjoint& base, double& ms, long long& launches) {
+    WfConfig cfg;
+    int rc = wf_config(sc, p, cfg);
+    if (rc != RT_OK) return rc;
+    HostReq q;
+    q.scene = sc;
+    q.rc = make_rc(sc, p, sc->host.camera);
+    q.x0 = p->pixel_x0;
+    q.y0 = p->pixel_y0;
+    q.ww = p->window_w > 0 ? p->window_w : p->width;
+    q.wh = p->window_h > 0 ? p->window_h : p->height;
+    q.W = p->width;
+    q.H = p->height;
+    q.d_film = nullptr;
+    long long npix = (long long)q.ww * q.wh;
+    int per = (int)std::max<long long>(1, std::min<long long>(p->spp, kAdjRecord / std::max<long long>(npix, 1)));
+    rt::WfAdjoint J = base;
+    J.nrec = npix * per;
+    void* mem = nullptr;
+    if (cudaMalloc(&mem, (size_t)J.nrec * 4 * sizeof(float4)) != cudaSuccess)
+        return fail(RT_ERR_OOM, "adjoint sample record");
+    J.rec = static_cast<float4*>(mem);
+    for (int s0 = 0; s0 < p->spp && rc == RT_OK; s0 += per) {
+        q.spp = std::min(per, p->spp - s0);
+        q.spp0 = p->spp_offset + s0;
+        for (int mode : {rt::WF_RECORD, rt::WF_REPLAY}) {
+            RtStats one{};
+            rc = wf_render({q}, cfg, &one, mode, &J);
+            if (rc != RT_OK) break;
+            ms += one.kernel_ms;
+            launches += one.kernel_launches;
+        }
+    }
+    cudaFree(mem);
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2017,8 +2083,13 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
         if (i < nm * kPerMat) hm[(size_t)(i / kPerMat)] |= 1u << (i % kPerMat);
         else gm |= 1u << (i - nm * kPerMat);
     }
+    std::vector<int> act;   // the selected slots, for the wavefront replay's gather
+    for (int i = 0; i < np; i++) {
+        bool on = i < nm * kPerMat ? ((hm[(size_t)(i / kPerMat)] >> (i % kPerMat)) & 1u) : ((gm >> (i - nm * kPerMat)) & 1u);
+        if (on) act.push_back(i);
+    }
     size_t bytes = (size_t)np * sizeof(double) + (size_t)np * sizeof(float) + film * sizeof(float) +
-                   (size_t)nm * sizeof(unsigned) + 256;
+                   (size_t)nm * sizeof(unsigned) + (size_t)(act.size() + 1) * sizeof(int) + 256;
     void* mem = nullptr;
     if (cudaMalloc(&mem, bytes) != cudaSuccess) return fail(RT_ERR_OOM, "adjoint buffers");
     char* base = static_cast<char*>(mem);
@@ -2026,6 +2097,7 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
     float* d_params = reinterpret_cast<float*>(base + (size_t)np * sizeof(double));
     float* d_img = d_params + np;
     unsigned* d_mask = reinterpret_cast<unsigned*>(d_img + film);
+    int* d_act = reinterpret_cast<int*>(d_mask + nm);
     int rc = RT_OK;
     auto step = [&](cudaError_t e, const char* what) {
         if (rc == RT_OK && e != cudaSuccess) rc = fail(RT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -2035,6 +2107,9 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
          "parameter copy");
     step(cudaMemcpyAsync(d_mask, hm.data(), (size_t)nm * sizeof(unsigned), cudaMemcpyHostToDevice, sc->stream),
          "mask copy");
+    if (!act.empty())
+        step(cudaMemcpyAsync(d_act, act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, sc->stream),
+             "slot list copy");
     step(cudaMemsetAsync(d_grad, 0, (size_t)np * sizeof(double), sc->stream), "gradient clear");
     step(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream), "error clear");
     AdjArgs a;
@@ -2059,7 +2134,28 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
     a.use_local = RT_ADJ_LOCAL_ACC && np <= rt::kAdjLocal;
     long long total = (long long)ww * wh * p->spp;
     long long blocks = std::min<long long>((total + kBlock - 1) / kBlock, 148LL * 16);
-    if (rc == RT_OK) {
+    double wf_ms = 0.0;
+    long long launches = 1;
+    const bool wavefront = p->kernel == RT_KERNEL_WAVEFRONT;
+    if (rc == RT_OK && wavefront) {
+        rt::WfAdjoint J{};
+        J.dimg = d_img;
+        J.W = p->width;
+        J.H = p->height;
+        J.inv_spp = 1.0f / (float)p->spp;
+        J.params = d_params;
+        J.mmask = d_mask;
+        J.gmask = gm;
+        J.nparams = np;
+        J.medium_base = nm * kPerMat;
+        J.act = d_act;
+        J.nact = (int)act.size();
+        J.use_local = RT_ADJ_LOCAL_ACC && np <= rt::kAdjLocal;
+        J.use_shared = (size_t)np * sizeof(float) <= 48 * 1024;
+        J.grad = d_grad;
+        launches = 0;
+        if (!act.empty()) rc = wf_adjoint(sc, p, J, wf_ms, launches);
+    } else if (rc == RT_OK) {
         step(cudaEventRecord(sc->ev0, sc->stream), "event");
         k_adjoint<kStack><<<(unsigned)std::max<long long>(blocks, 1), kBlock, shmem, sc->stream>>>(sc->view, rcon, a,
                                                                                                      sc->d_err);
@@ -2074,7 +2170,8 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
     }
     if (rc == RT_OK) rc = check_err(sc);
     float ms = 0.0f;
-    if (rc == RT_OK) cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+    if (rc == RT_OK && !wavefront) cudaEventElapsedTime(&ms, sc->ev0, sc->ev1);
+    if (wavefront) ms = (float)wf_ms;
     cudaFree(mem);
     if (rc != RT_OK) return rc;
     for (int i = 0; i < np; i++) grad[i] = (float)hg[(size_t)i];
@@ -2082,7 +2179,7 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
         *st = RtStats{};
         st->kernel_ms = ms;
         st->samples = (uint64_t)total;
-        st->kernel_launches = 1;
+        st->kernel_launches = (int32_t)launches;
         st->rr_min_bounces = rcon.rr_min_bounces;
         st->rr_min_survival = rcon.rr_min_survival;
         st->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

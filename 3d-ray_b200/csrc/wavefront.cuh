@@ -17,8 +17,17 @@
 // Many requests of uneven resolution, spp and depth share the pool: a work id
 // maps to (request, sample, pixel) with a binary search over the requests'
 // prefix offsets, samples outermost so a warp shares a sample index.
+//
+// The same loop runs the path-replay adjoint (rt_adjoint) in two passes over
+// a range of samples: WF_RECORD renders them with the forward kernels and
+// regen stores each finished sample's end state (lp, la, pre, att0) by work id
+// instead of adding it to a film; WF_REPLAY traces the same samples again,
+// regen seeds each new path with the adjoints of its recorded resolve, and
+// k_wf_adjoint (wf_adjoint.cuh) replaces shade and occlude: it runs the vertex
+// with the replay's gradient hooks and its shadow rays inline.
 #pragma once
 
+#include "adjoint.cuh"
 #include "integrator.cuh"
 
 namespace rt {
@@ -89,6 +98,27 @@ struct WfCtl {
 // Buckets of the bounce-ray sort.
 constexpr int kRayKeys = 1 << 15;
 
+enum : int { WF_RENDER = 0, WF_RECORD = 1, WF_REPLAY = 2 };
+
+// The adjoint passes' buffers and parameters (zero in WF_RENDER).
+struct WfAdjoint {
+    float4* rec;            // per work id, 4 float4: {lp, clamp flag}, la, pre, att0 of the finished sample
+    long long nrec;         // work ids the record holds
+    float4* st;             // per slot, 4 float4: the replay's resolve adjoints and interior material
+    const float* dimg;      // dLoss/dfilm, 3 planes of W x H
+    int W, H;
+    float inv_spp;          // 1 / the request's spp: the film is the mean of its samples
+    const float* params;    // raw parameter vector, 16 per material, then the medium's 6
+    const unsigned* mmask;  // per material: bit k = slot k is differentiated
+    unsigned gmask;         // the medium's slots
+    int nparams, medium_base;
+    const int* act;         // the differentiated slots, nact of them
+    int nact;
+    int use_local;          // gradients gather in per-thread arrays (nparams <= kAdjLocal)
+    int use_shared;         // ... otherwise in shared memory (nparams floats), else global atomics
+    double* grad;           // nparams accumulators
+};
+
 struct WfArgs {
     const SceneView* views;
     int nviews;
@@ -114,6 +144,7 @@ struct WfArgs {
     WfShadow S;
     WfCtl* ctl;
     int* err;
+    WfAdjoint J;
 };
 
 RT_D int fbits(float f) { return __float_as_int(f); }
@@ -228,6 +259,7 @@ RT_D int find_request(const WfRequest* reqs, int n, unsigned long long id) {
     return lo;
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
     // Work ids come from the global counter with one atomic per block (a
     // ballot prefix over the block's free slots), and the live count with one
@@ -242,12 +274,36 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
     int flags = in ? fbits(a.P.d[i].w) : 0;
     bool alive = in && (flags & PF_ALIVE);
     bool need = in && !alive;
-    if (need && (flags & PF_DONE)) {   // resolve the finished sample into its film
-        int req = RT_IX(fbits(a.P.pre[i].w), a.nreq);
+    if (MODE == WF_RECORD && need && (flags & PF_DONE)) {   // keep the finished sample's end state
+        float4 lp = a.P.lp[i], la = a.P.la[i], pre = a.P.pre[i], at = a.P.att0[i];
+        const WfRequest& R = a.reqs[RT_IX(fbits(pre.w), a.nreq)];
+        int pix = fbits(la.w);
+        int lx = pix & 0xFFFF, ly = pix >> 16;
+        long long id = R.begin + (long long)(fbits(lp.w) - R.spp0) * ((long long)R.ww * R.wh) +
+                       strip_index(lx, ly, R.ww, R.wh);
+        if (id >= 0 && id < a.J.nrec) {
+            float4* r = a.J.rec + 4 * id;
+            r[0] = make_float4(lp.x, lp.y, lp.z, ibits(flags & PF_CLAMP));
+            r[1] = la;
+            r[2] = pre;
+            r[3] = at;
+        } else {
+            atomicExch(a.err, RT_ERR_BOUNDS);
+        }
+    }
+    if (MODE == WF_RENDER && need && (flags & PF_DONE)) {   // resolve the finished sample into its film
+        // path_resolve reads lp, la, pre, att0 and the clamp flag alone: load
+        // those four records, not the whole path state
+        float4 lp = a.P.lp[i], la = a.P.la[i], pre = a.P.pre[i], at = a.P.att0[i];
+        int req = RT_IX(fbits(pre.w), a.nreq);
         const WfRequest& R = a.reqs[req];
         PathState ps;
-        int fl, pix;
-        wf_load(a, i, R, ps, fl, pix);
+        ps.lp = v3(lp.x, lp.y, lp.z);
+        ps.la = v3(la.x, la.y, la.z);
+        ps.pre = v3(pre.x, pre.y, pre.z);
+        ps.att0 = v3(at.x, at.y, at.z);
+        ps.clamp_mode = (flags & PF_CLAMP) != 0;
+        int pix = fbits(la.w);
         V3 L = path_resolve(ps, R.rc);
         int lx = pix & 0xFFFF, ly = pix >> 16;
         size_t plane = (size_t)R.ww * R.wh, k = (size_t)RT_IX(strip_index(lx, ly, R.ww, R.wh), plane);
@@ -293,6 +349,24 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
             PathState ps;
             path_init(ps, R.rc, R.x0 + lx, R.y0 + ly, (uint32_t)(R.spp0 + s));
             int al = path_alive(ps);
+            if (MODE == WF_REPLAY) {   // the adjoints of the recorded resolve; no gradient, no replay
+                const WfAdjoint& J = a.J;
+                size_t plane = (size_t)J.W * J.H, fi = (size_t)(R.y0 + ly) * J.W + (R.x0 + lx);
+                V3 delta = v3(J.dimg[fi], J.dimg[plane + fi], J.dimg[2 * plane + fi]) * J.inv_spp;
+                AdjResolve ar{};
+                if (id < (unsigned long long)J.nrec && !is_zero(delta)) {
+                    const float4* r = J.rec + 4 * id;
+                    float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+                    ar = adjoint_resolve(R.rc, v3(r0.x, r0.y, r0.z), v3(r1.x, r1.y, r1.z), v3(r2.x, r2.y, r2.z),
+                                         v3(r3.x, r3.y, r3.z), fbits(r0.w) != 0, delta);
+                }
+                al = al && !is_zero(ar.g_a);
+                float4* q = J.st + 4 * (size_t)i;
+                q[0] = make_float4(ar.tot_a.x, ar.tot_a.y, ar.tot_a.z, ar.tot_la.x);
+                q[1] = make_float4(ar.tot_la.y, ar.tot_la.z, ar.g_a.x, ar.g_a.y);
+                q[2] = make_float4(ar.g_a.z, ar.g_la.x, ar.g_la.y, ar.g_la.z);
+                q[3] = make_float4(ar.g_att0.x, ar.g_att0.y, ar.g_att0.z, ibits(-1));
+            }
             wf_store(a, i, ps, wf_flags(ps, al), req, lx | (ly << 16));
             wf_store_media(a, i, R, ps);
             live = true;
@@ -573,6 +647,32 @@ struct QueueShadows : NoAdjoint {
     RT_D void skipped(V3, V3, float) {}
 };
 
+// Under the ray sort: the continued ray's sort key and its rank in the key's
+// count (one returning atomic per distinct key in the warp).
+RT_D void wf_rank_ray(const WfArgs& a, const SceneView& s, const PathState& ps, int i) {
+    int key = ray_key(s, ps.o, ps.d, a.rkey_bits, a.rdir_bits);
+    unsigned grp = __match_any_sync(__activemask(), key);
+    int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&a.rhist[key], __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    a.P.keys[i] = key;
+    a.P.rrank[i] = base + __popc(grp & ((1u << lane) - 1u));
+}
+
+// Hit record of slot i as extend wrote it.
+RT_D Hit wf_hit(const WfArgs& a, int i) {
+    float4 hh = a.P.hit[i];
+    int packed = fbits(hh.w);
+    Hit h;
+    h.t = hh.x;
+    h.u = hh.y;
+    h.v = hh.z;
+    h.kind = packed == 0 ? HIT_NONE : ((unsigned)packed >> 30);
+    h.slot = packed & 0x3FFFFFFF;
+    return h;
+}
+
 // Minimum resident blocks of 256 for shade (a register budget); a build knob.
 #ifndef RT_SHADE_MIN_BLOCKS
 #define RT_SHADE_MIN_BLOCKS 2
@@ -598,28 +698,12 @@ __global__ void __launch_bounds__(256, RT_SHADE_MIN_BLOCKS) k_wf_shade(WfArgs a)
     PathState ps;
     int fl, pix;
     wf_load(a, i, R, ps, fl, pix);
-    float4 hh = a.P.hit[i];
-    int packed = fbits(hh.w);
-    Hit h;
-    h.t = hh.x;
-    h.u = hh.y;
-    h.v = hh.z;
-    h.kind = packed == 0 ? HIT_NONE : ((unsigned)packed >> 30);
-    h.slot = packed & 0x3FFFFFFF;
+    Hit h = wf_hit(a, i);
     QueueShadows sink{{}, &a, i, R.scene};
     bool alive = shade_vertex<MEDIUM, TRANSMIT>(s, R.rc, ps, h, sink);
     wf_store(a, i, ps, wf_flags(ps, alive), req, pix);
     wf_store_media(a, i, R, ps);
-    if (a.raysort && alive) {   // the continued ray's sort key and its rank in the key's count
-        int key = ray_key(s, ps.o, ps.d, a.rkey_bits, a.rdir_bits);
-        unsigned grp = __match_any_sync(__activemask(), key);
-        int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(&a.rhist[key], __popc(grp));
-        base = __shfl_sync(grp, base, leader);
-        a.P.keys[i] = key;
-        a.P.rrank[i] = base + __popc(grp & ((1u << lane) - 1u));
-    }
+    if (a.raysort && alive) wf_rank_ray(a, s, ps, i);
 }
 
 // Exclusive scan of a ray-sort key histogram (kRayKeys counts) into off (one

@@ -789,6 +789,8 @@ def main():
             if line.startswith("l2_bytes_per_launch:"):
                 l2_bytes = float(line.split(":")[1])
     roof["traffic"] = traffic
+    roof["traffic_source"] = (f"profiles/{roof['kernel']}_icospheres.md: ncu DRAM read + write of a steady-state "
+                              "launch (all 4 M slots busy), measured on the same kernels") if traffic else None
     # L2 roofline beside the HBM one: the scene is largely L2-resident, so the
     # traversal kernels are compared against L2 bandwidth too. The peak is a
     # project micro-benchmark (L2-only float4 streams over a 32 MiB buffer).

@@ -438,8 +438,13 @@ int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* be
  * parameter-vector layout above; count is that layout's length. mask (count
  * bytes, or NULL for all) selects the slots to differentiate; unselected slots
  * come back 0 and cost nothing (a material with no selected BSDF slot skips
- * the dual-number BSDF evaluations). The megakernel form is used whatever
- * params->kernel says; count_work must be 0. */
+ * the dual-number BSDF evaluations). params->kernel selects the form:
+ * RT_KERNEL_MEGAKERNEL traces both passes of a sample in one thread;
+ * RT_KERNEL_WAVEFRONT renders runs of at most 2^24 samples with the wavefront
+ * kernels, keeping each sample's end state (64 B, device memory for one run),
+ * then replays them on the wavefront with the gradient hooks and the shadow
+ * rays inline. Both give the same gradient up to the order of the float sums.
+ * count_work must be 0. */
 int rt_adjoint(RtScene* scene, const RtRenderParams* params,
                const float* dL_dimage_planar, const uint8_t* mask,
                float* dL_dparams, int32_t count, RtStats* stats);

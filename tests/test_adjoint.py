@@ -109,6 +109,45 @@ def test_radiance_gradient_is_exact_without_clamps():
         assert g[i] == pytest.approx(fd, rel=2e-3)
 
 
+@pytest.mark.parametrize("scene", ["sphere", "volume", "sky", "many_materials"])
+def test_wavefront_adjoint_equals_megakernel(scene):
+    """The wavefront form (a recording forward pass, then the replay with the
+    shadow rays inline) computes the same per-vertex gradient terms as the
+    megakernel on the same samples; only the order of the float sums differs
+    (and the primal's shadow terms, which occlude adds in any order)."""
+    if scene == "sphere":
+        ds = rt.DiffScene(rt.scenes.cornell_sphere(SPHERE))
+        slots = [ds.slot("fit_sphere", n) for n in ("roughness", "metallic", "specular", "sheen")]
+        slots += [ds.slot("fit_sphere", "base_color", c) for c in range(3)]
+        slots += [ds.slot("light", "radiance", c) for c in range(3)]
+        res, spp, depth, kw = 48, 64, 8, {}
+    elif scene == "volume":
+        ds = rt.DiffScene(rt.scenes.cornell_volume())
+        slots = [ds.medium_slot(k, c) for k in ("sigma_a", "sigma_s") for c in range(3)]
+        slots += [ds.slot("glass", "absorption", c) for c in range(3)]
+        res, spp, depth, kw = 32, 64, 16, {}
+    elif scene == "sky":
+        ds = rt.DiffScene(rt.scenes.sky_scene())
+        slots = [ds.slot("red", "base_color", 0), ds.slot("ground", "base_color", 1)]
+        res, spp, depth, kw = 32, 64, 8, NO_CLAMP
+    else:   # more slots than the per-thread accumulators hold: the shared-memory gather
+        w = rt.scenes.cornell_spheres()
+        for k in range(2):
+            w.add_material(f"unused{k}", rt.scenes.disney((0.5, 0.5, 0.5)))
+        ds = rt.DiffScene(w)
+        slots = None
+        res, spp, depth, kw = 32, 32, 8, {}
+    if scene == "many_materials":
+        assert ds.count > rt.adjoint.ADJ_LOCAL_SLOTS
+    wimg = _weights(res, res)
+    mega = ds.adjoint(_params(res, res, spp, depth, spp_offset=7, **kw), wimg, slots)
+    wf_rp = abi.render_params(res, res, spp, depth, kernel=abi.KERNEL_WAVEFRONT, spp_offset=7, **kw)
+    wave = ds.adjoint(wf_rp, wimg, slots)
+    assert ds.last_stats.kernel_launches > 4   # the two wavefront passes ran
+    assert np.count_nonzero(mega) > 0
+    np.testing.assert_allclose(wave, mega, rtol=1e-3, atol=1e-5 * np.abs(mega).max())
+
+
 def test_unmasked_slots_come_back_zero():
     ds = rt.DiffScene(rt.scenes.cornell_sphere(SPHERE))
     rp = _params(32, 32, 16)
