@@ -13,7 +13,10 @@
 //     as in path replay backpropagation (Vicini et al. 2021).
 // Sampling decisions are detached: sampled directions, lobe choices, light
 // samples, the MIS weights and the Russian-roulette probability are held
-// fixed, so f/pdf is differentiated through f only. The local derivatives of
+// fixed, so f/pdf is differentiated through f only. That is exact for an
+// estimator linear in its terms; the luminance clamps are not, and for the
+// medium's free-flight and Russian-roulette decisions the replay adds their
+// score terms (free_flight, roulette_score). The local derivatives of
 // the Disney BSDF come from forward-mode dual numbers run once per parameter
 // direction over the material constructor and the BSDF formulas. Geometry
 // and visibility (edges) are not differentiated.
@@ -415,6 +418,8 @@ RT_D V3 clamp_lum_vjp(V3 cin, float mx, V3 g) {
 // luminance clamps and the per-frame sanitize.
 struct AdjResolve {
     V3 tot_a, tot_la, g_a, g_la, g_att0;
+    V3 delta;    // the sample's film gradient
+    float val;   // delta . the sample's clamped radiance
 };
 RT_D AdjResolve adjoint_resolve(const RenderConst& rc, V3 lp, V3 la, V3 pre, V3 att0, int clamp_mode, V3 delta) {
     AdjResolve r;
@@ -425,6 +430,8 @@ RT_D AdjResolve adjoint_resolve(const RenderConst& rc, V3 lp, V3 la, V3 pre, V3 
     }
     r.tot_a = A;
     r.tot_la = la;
+    r.delta = delta;
+    r.val = dot(delta, clamp_lum(A, rc.max_rad));
     r.g_a = clamp_lum_vjp(A, rc.max_rad, delta);
     r.g_la = v3(0.0f);
     r.g_att0 = v3(0.0f);
@@ -462,12 +469,21 @@ struct AdjointSink {
     V3 tot_a, tot_la;      // primal A = lp + pre * clamp(att0 * S(la)) and la
     V3 g_a, g_la, g_att0;  // their adjoints
     int abs_mat;           // material of the current interior absorption (-1: none)
+    V3 delta;              // the sample's film gradient
+    float val;             // delta . the sample's clamped radiance
+    float max_rad, ind_max;   // the two clamps (RenderConst)
+    // d log beta_c / d theta_k of the path throughput Russian roulette reads,
+    // for the medium's six slots (sigma_a, then sigma_s), kept while a medium
+    // slot is differentiated
+    float dlb[3][6];
     RT_D void set_resolve(const AdjResolve& r) {
         tot_a = r.tot_a;
         tot_la = r.tot_la;
         g_a = r.g_a;
         g_la = r.g_la;
         g_att0 = r.g_att0;
+        delta = r.delta;
+        val = r.val;
     }
     // the last shadow ray
     int sh_added;
@@ -611,10 +627,99 @@ struct AdjointSink {
     RT_D void skipped(V3, V3, float) {}
     RT_D void interior(int mat) { abs_mat = mat; }
 
+    // Score terms under the clamps. The clamps make the sample value a
+    // nonlinear function F of its terms, each term divided by the density of
+    // the decisions before it, so the derivative of E[F] holds, besides the
+    // detached terms, E[dlog p_j/dtheta * B_j] for every decision j whose
+    // density depends on theta, with B_j = F - sum over the terms after j of
+    // dF/dterm . term - b_j and any baseline b_j that depends on the path
+    // before j alone. b_j = F of the terms before j (the sample's value had
+    // the path ended there) makes B_j exactly 0 when F is linear (no clamp
+    // saturates), so unclamped samples gain no variance. The terms after j are
+    // the replay's suffix (target), except at the first surface vertex's
+    // roulette, after which every term goes to la through att0.
+    RT_D float score_weight(const PathView& v, V3 pre, V3 att0, bool first_surface) const {
+        V3 now = v.lp;
+        if (v.clamp_mode) now = now + pre * clamp_lum(att0 * sanitize(v.la), ind_max);
+        float after;
+        if (first_surface) {
+            after = dot(g_la, tot_la);
+        } else {
+            V3 g, S;
+            target(v, g, S);
+            after = dot(g, S);
+        }
+        return val - after - dot(delta, clamp_lum(now, max_rad));
+    }
+
+    // A free-flight decision of the medium: its score, and its factor's log
+    // derivatives in the throughput. medium_sample draws from the channel
+    // mixture (1/3) sum_c sigma_t,c exp(-sigma_t,c t) for a scattering at t,
+    // (1/3) sum_c exp(-sigma_t,c t) for passing a segment of length t, and
+    // puts tr_c sigma_s,c / p or tr_c / p into the throughput; sigma_t =
+    // sigma_a + sigma_s.
+    RT_NI void free_flight(PathView v, V3 pre, V3 att0, float t, int mode) {
+        bool sc = mode == SEG_MEDIUM_SCATTER;
+        V3 st = s->sigma_t, tr = medium_tr(*s, t);
+        V3 dens = sc ? st * tr : tr;
+        float p = (dens.x + dens.y + dens.z) / 3.0f;
+        if (!(p >= 1e-20f)) return;
+        float stc[3] = {st.x, st.y, st.z}, trc[3] = {tr.x, tr.y, tr.z};
+        float ssc[3] = {s->sigma_s.x, s->sigma_s.y, s->sigma_s.z};
+        float dl[3];   // d log p / d sigma_t,k
+        for (int k = 0; k < 3; k++) dl[k] = (sc ? trc[k] * (1.0f - stc[k] * t) : -t * trc[k]) / (3.0f * p);
+        float b = score_weight(v, pre, att0, false);
+        if (b != 0.0f && isfinite(b))
+            for (int k = 0; k < 3; k++) {
+                add(medium_base + k, b * dl[k]);
+                add(medium_base + 3 + k, b * dl[k]);
+            }
+        for (int c = 0; c < 3; c++)
+            for (int k = 0; k < 3; k++) {
+                float own = c == k ? -t : 0.0f;
+                dlb[c][k] += own - dl[k];
+                dlb[c][3 + k] += own + ((c == k && sc && ssc[c] > 0.0f) ? 1.0f / ssc[c] : 0.0f) - dl[k];
+            }
+    }
+
+    // Russian roulette: a survivor was drawn against q = clamp(max_c thr_c,
+    // min survival, 0.95), which moves with theta only strictly between the
+    // bounds, as the largest channel of the throughput (the mean over
+    // channels tied for the largest, the central derivative of the max). The
+    // survivor's throughput then carries 1/q. A path the roulette ends has no
+    // terms after the decision, so its score weight is 0.
+    RT_NI void roulette_score(PathView v, V3 pre, V3 att0, V3 thr, float q, int first_surface) {
+        float m = fmaxf(thr.x, fmaxf(thr.y, thr.z));
+        if (q != m) return;
+        float thc[3] = {thr.x, thr.y, thr.z};
+        float dq[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        int nt = 0;
+        for (int c = 0; c < 3; c++)
+            if (thc[c] == m) {
+                nt++;
+                for (int k = 0; k < 6; k++) dq[k] += dlb[c][k];
+            }
+        for (int k = 0; k < 6; k++) dq[k] /= (float)nt;
+        float b = score_weight(v, pre, att0, first_surface != 0);
+        if (b != 0.0f && isfinite(b))
+            for (int k = 0; k < 6; k++) add(medium_base + k, b * dq[k]);
+        for (int c = 0; c < 3; c++)
+            for (int k = 0; k < 6; k++) dlb[c][k] -= dq[k];
+    }
+    RT_D bool medium_scores() const { return (gmask & 0x3Fu) && medium_ok(); }
+    RT_D void roulette(const PathState& ps, V3 thr, float q, int first_surface) {
+        if (medium_scores()) roulette_score(path_view(ps), ps.pre, ps.att0, thr, q, first_surface);
+    }
+    RT_D void clear_log_beta() {
+        for (int c = 0; c < 3; c++)
+            for (int k = 0; k < 6; k++) dlb[c][k] = 0.0f;
+    }
+
     RT_D void segment(const PathState& ps, float t, int mode) {
         V3 g, S;
         target(path_view(ps), g, S);
         V3 gs = g * S;
+        if (mode != SEG_ABSORPTION && medium_scores()) free_flight(path_view(ps), ps.pre, ps.att0, t, mode);
         if (is_zero(gs)) return;
         if (mode != SEG_MEDIUM_PASS && abs_mat >= 0) {
             const Material& m = s->materials[abs_mat];

@@ -683,31 +683,28 @@ __device__ __forceinline__ bool traverse4_any(const SceneView& s, V3 o, V3 d, fl
             float4 hx = ldg_scene(q + 3), hy = ldg_scene(q + 4), hz = ldg_scene(q + 5);
             float4 cc = ldg_scene(q + 6);
             int c[4] = {__float_as_int(cc.x), __float_as_int(cc.y), __float_as_int(cc.z), __float_as_int(cc.w)};
-            float te[4];
+            float te;
             bool h[4];
-            h[0] = c[0] != kNone && box_hit_te(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, o, inv, tmin, tmax, te[0]);
-            h[1] = c[1] != kNone && box_hit_te(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, o, inv, tmin, tmax, te[1]);
-            h[2] = c[2] != kNone && box_hit_te(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, o, inv, tmin, tmax, te[2]);
-            h[3] = c[3] != kNone && box_hit_te(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, o, inv, tmin, tmax, te[3]);
-            // enter the slot the ray meets first (an occluder near the origin
-            // ends the walk sooner), stack the others
-            int nj = -1;
-            float tn = kInf;
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (h[j] && (nj < 0 || te[j] < tn)) {
-                    nj = j;
-                    tn = te[j];
-                }
-            code = nj >= 0 ? c[nj] : kNone;
+            h[0] = c[0] != kNone && box_hit_te(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, o, inv, tmin, tmax, te);
+            h[1] = c[1] != kNone && box_hit_te(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, o, inv, tmin, tmax, te);
+            h[2] = c[2] != kNone && box_hit_te(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, o, inv, tmin, tmax, te);
+            h[3] = c[3] != kNone && box_hit_te(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, o, inv, tmin, tmax, te);
+            // enter the first hit slot, stack the others (entering the slot the
+            // ray meets first instead: occlude 54.4 against 49.1 ms per 64-spp
+            // icosphere frame; the selection costs more than earlier exits win)
+            code = kNone;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                if (!h[j] || j == nj) continue;
-                if (sp >= STACK) {
-                    *err = RT_ERR_STACK;
-                    return false;
+                if (!h[j]) continue;
+                if (code == kNone) {
+                    code = c[j];
+                } else {
+                    if (sp >= STACK) {
+                        *err = RT_ERR_STACK;
+                        return false;
+                    }
+                    stc[sp++] = c[j];
                 }
-                stc[sp++] = c[j];
             }
         }
         if (code != kNone) {

@@ -264,13 +264,17 @@ RT_D void nee_medium(const SceneView& s, const RenderConst& rc, PathState& ps, V
 }
 
 // Russian roulette on the projected throughput (Renderer.cs:1283-1294).
-RT_D bool russian_roulette(const RenderConst& rc, int depth, V3& att, V3& next_beta, Sampler& rng) {
+// q_used: the survival probability a surviving path was drawn against, 0 when
+// the roulette did not run.
+RT_D bool russian_roulette(const RenderConst& rc, int depth, V3& att, V3& next_beta, Sampler& rng, float& q_used) {
     int used = rc.max_depth - depth;
+    q_used = 0.0f;
     if (used >= rc.rr_min_bounces) {
         float q = fmaxf(next_beta.x, fmaxf(next_beta.y, next_beta.z));
         q = fmaxf(q, rc.rr_min_survival);
         q = fminf(q, 0.95f);
         if (rng.next() > q) return false;
+        q_used = q;
         float inv = 1.0f / q;
         att = att * inv;
         next_beta = next_beta * inv;
@@ -298,6 +302,10 @@ struct NoAdjoint {
     RT_D void nee_surface(const PathState&, int, const Material&, const Surface&, V3, V3, float, V3, float, V3,
                           int) {}
     RT_D void nee_medium(const PathState&, int, float, int) {}
+    // A path survived Russian roulette drawn against q = clamp(max(thr)); its
+    // throughput now carries 1/q. first: the roulette of the first surface
+    // vertex (whose attenuation becomes att0).
+    RT_D void roulette(const PathState&, V3, float, int) {}
     // The vertex attenuation: att_pre before Russian roulette, att after. For
     // the legacy path, the lobe and direction of the null sample before it.
     RT_D void scatter(const PathState&, const Material&, const Surface&, V3, V3, int, int, float, V3, V3, int, V3) {}
@@ -349,6 +357,7 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
                 q = fminf(q, 0.95f);
                 if (ps.rng.next() > q) return false;
                 scale = 1.0f / q;
+                sink.roulette(ps, mthr, q, 0);
             }
             float ppdf;
             V3 wi = hg_sample(s.hg_g, ps.d, ps.rng, ppdf);
@@ -410,8 +419,10 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         }
         sink.aov_bounce(bs.is_delta, bs.f);
         next_beta = beta_s * att;
-        V3 att_pre = att;
-        if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
+        V3 att_pre = att, thr = next_beta;
+        float q_rr;
+        if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng, q_rr)) return false;
+        if (q_rr > 0.0f) sink.roulette(ps, thr, q_rr, ps.first);
         sink.scatter(ps, m, rec, view, bs.wo, bs.lobe, bs.is_delta ? SCATTER_DELTA : SCATTER_SAMPLED, bs.pdf,
                      att_pre, att, -1, bs.wo);
         V3 off = dot(bs.wo, rec.n) >= 0.0f ? rec.n : -rec.n;
@@ -432,8 +443,10 @@ __device__ __forceinline__ bool shade_vertex(const SceneView& s, const RenderCon
         att = latt;
         sink.aov_bounce(false, att);   // Disney's IsDeltaScatter is false
         next_beta = beta_s * att;
-        V3 att_pre = att;
-        if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng)) return false;
+        V3 att_pre = att, thr = next_beta;
+        float q_rr;
+        if (!russian_roulette(rc, ps.depth, att, next_beta, ps.rng, q_rr)) return false;
+        if (q_rr > 0.0f) sink.roulette(ps, thr, q_rr, ps.first);
         sink.scatter(ps, m, rec, view, sdir, lobe, SCATTER_LEGACY, 1.0f, att_pre, att, bs.lobe, bs.tried);
         next_o = rec.p;
         next_d = sdir;

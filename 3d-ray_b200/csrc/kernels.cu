@@ -392,6 +392,9 @@ __global__ void RT_ADJ_BOUNDS k_adjoint(rt::SceneView s, rt::RenderConst rc, Adj
         adj.opaque = rc.opaque;
         adj.err = err;
         adj.abs_mat = -1;
+        adj.max_rad = rc.max_rad;
+        adj.ind_max = rc.ind_max;
+        adj.clear_log_beta();
         adj.sh_added = 0;
         adj.sh_n = 0;
         adj.set_resolve(rt::adjoint_resolve(rc, pp.lp, pp.la, pp.pre, pp.att0, pp.clamp_mode, delta));
@@ -837,7 +840,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     for (auto& q : wreq) add((size_t)3 * q.ww * q.wh * sizeof(double));
     add(reqs.size() * sizeof(float*));
     add(reqs.size() * sizeof(int) * 2);
-    if (mode == rt::WF_REPLAY) add((size_t)nslots * 4 * sizeof(float4));
+    if (mode == rt::WF_REPLAY) add((size_t)nslots * rt::kAdjState * sizeof(float4));
     need += 1024;
     WfWorkspace& ws = g_wf_ws[dev];
     if (ws.bytes < need) {
@@ -901,7 +904,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     auto* d_films = cv.take<float*>(reqs.size());
     auto* d_fdims = cv.take<int>(2 * reqs.size());
     if (adj) a.J = *adj;
-    if (mode == rt::WF_REPLAY) a.J.st = cv.take<float4>((size_t)nslots * 4);
+    if (mode == rt::WF_REPLAY) a.J.st = cv.take<float4>((size_t)nslots * rt::kAdjState);
     a.views = d_views;
     a.nviews = (int)views.size();
     a.reqs = d_reqs;

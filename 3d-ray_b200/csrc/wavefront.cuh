@@ -99,12 +99,17 @@ struct WfCtl {
 constexpr int kRayKeys = 1 << 15;
 
 enum : int { WF_RENDER = 0, WF_RECORD = 1, WF_REPLAY = 2 };
+// float4s of a replayed slot's adjoint state: 5 for the resolve adjoints, the
+// interior material, the film gradient and the clamped value, then 5 for the
+// throughput's log derivatives (dlb) while a medium slot is differentiated
+constexpr int kAdjState = 10;
 
 // The adjoint passes' buffers and parameters (zero in WF_RENDER).
 struct WfAdjoint {
     float4* rec;            // per work id, 4 float4: {lp, clamp flag}, la, pre, att0 of the finished sample
     long long nrec;         // work ids the record holds
-    float4* st;             // per slot, 4 float4: the replay's resolve adjoints and interior material
+    float4* st;             // per slot, kAdjState float4: the replay's resolve adjoints, interior material,
+                            // film gradient and clamped value
     const float* dimg;      // dLoss/dfilm, 3 planes of W x H
     int W, H;
     float inv_spp;          // 1 / the request's spp: the film is the mean of its samples
@@ -361,11 +366,14 @@ __global__ void __launch_bounds__(256) k_wf_regen(WfArgs a) {
                                          v3(r3.x, r3.y, r3.z), fbits(r0.w) != 0, delta);
                 }
                 al = al && !is_zero(ar.g_a);
-                float4* q = J.st + 4 * (size_t)i;
+                float4* q = J.st + kAdjState * (size_t)i;
                 q[0] = make_float4(ar.tot_a.x, ar.tot_a.y, ar.tot_a.z, ar.tot_la.x);
                 q[1] = make_float4(ar.tot_la.y, ar.tot_la.z, ar.g_a.x, ar.g_a.y);
                 q[2] = make_float4(ar.g_a.z, ar.g_la.x, ar.g_la.y, ar.g_la.z);
                 q[3] = make_float4(ar.g_att0.x, ar.g_att0.y, ar.g_att0.z, ibits(-1));
+                q[4] = make_float4(ar.delta.x, ar.delta.y, ar.delta.z, ar.val);
+                if (J.gmask & 0x3Fu)
+                    for (int k = 5; k < kAdjState; k++) q[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             }
             wf_store(a, i, ps, wf_flags(ps, al), req, lx | (ly << 16));
             wf_store_media(a, i, R, ps);

@@ -59,15 +59,30 @@ __global__ void __launch_bounds__(128) k_wf_adjoint(WfArgs a) {
         adj.err = a.err;
         adj.sh_added = 0;
         adj.sh_n = 0;
-        float4* q = J.st + 4 * (size_t)i;
-        float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+        float4* q = J.st + kAdjState * (size_t)i;
+        float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4];
         adj.tot_a = v3(q0.x, q0.y, q0.z);
         adj.tot_la = v3(q0.w, q1.x, q1.y);
         adj.g_a = v3(q1.z, q1.w, q2.x);
         adj.g_la = v3(q2.y, q2.z, q2.w);
         adj.g_att0 = v3(q3.x, q3.y, q3.z);
         adj.abs_mat = fbits(q3.w);
+        adj.delta = v3(q4.x, q4.y, q4.z);
+        adj.val = q4.w;
+        adj.max_rad = R.rc.max_rad;
+        adj.ind_max = R.rc.ind_max;
+        const bool track = MEDIUM && (J.gmask & 0x3Fu);
+        if (track) {   // the throughput's log derivatives, 18 floats in q[5 .. 9]
+            const float* f = reinterpret_cast<const float*>(q + 5);
+            for (int c = 0; c < 3; c++)
+                for (int k = 0; k < 6; k++) adj.dlb[c][k] = f[c * 6 + k];
+        }
         bool alive = shade_vertex<MEDIUM, TRANSMIT>(s, R.rc, ps, h, adj);
+        if (track && alive) {
+            float* f = reinterpret_cast<float*>(q + 5);
+            for (int c = 0; c < 3; c++)
+                for (int k = 0; k < 6; k++) f[c * 6 + k] = adj.dlb[c][k];
+        }
         wf_store(a, i, ps, wf_flags(ps, alive), req, pix);
         wf_store_media(a, i, R, ps);
         if (adj.abs_mat != fbits(q3.w)) q[3] = make_float4(q3.x, q3.y, q3.z, ibits(adj.abs_mat));

@@ -401,6 +401,12 @@ def batched_side(rt):
     return out
 
 
+def adjoint_kernel(args):
+    """The rt_adjoint form --adjoint-kernel names."""
+    abi = load_package().abi
+    return abi.KERNEL_WAVEFRONT if args.adjoint_kernel == "wavefront" else abi.KERNEL_MEGAKERNEL
+
+
 def gradcheck(args):
     """The path-replay adjoint against central finite differences under common
     random numbers: C4 (the Cornell box with a Disney sphere: the sphere's
@@ -446,7 +452,7 @@ def gradcheck(args):
         # the finite differences may take more samples per batch than the
         # adjoint (the adjoint's are the first of them), and a larger eps
         fper = max(per, args.gc_fd_spp // nb) if args.gc_fd_spp else per
-        rp = abi.render_params(res, res, per, depth, kernel=abi.KERNEL_MEGAKERNEL, **kw)
+        rp = abi.render_params(res, res, per, depth, kernel=adjoint_kernel(args), **kw)
         rw = abi.render_params(res, res, fper, depth, kernel=abi.KERNEL_WAVEFRONT, **kw)
         pilot = abi.render_params(res, res, 2048, depth, kernel=abi.KERNEL_WAVEFRONT, spp_offset=1 << 24, **kw)
         theta = ds.get_params()
@@ -465,6 +471,11 @@ def gradcheck(args):
                     slots[f"medium.{nm}[{c}]"] = (i, 1e-2 * float(theta[i]))
                 i = ds.slot("glass", "absorption", c)
                 slots[f"glass.absorption[{c}]"] = (i, 1e-2 * float(theta[i]))
+                # the single-scattering albedo at a fixed sigma_t: sigma_s = albedo * sigma_t,
+                # sigma_a = (1 - albedo) * sigma_t, a direction in the parameter vector
+                ia, isc = ds.medium_slot("sigma_a", c), ds.medium_slot("sigma_s", c)
+                st = float(theta[ia]) + float(theta[isc])
+                slots[f"medium.albedo[{c}]"] = ([(isc, st), (ia, -st)], 1e-2 * float(theta[isc]) / st)
         else:
             slots = {f"glass.absorption[{c}]": (ds.slot("glass", "absorption", c),
                                                 1e-2 * float(theta[ds.slot("glass", "absorption", c)]))
@@ -474,30 +485,33 @@ def gradcheck(args):
             slots = {k: (i, e * args.gc_eps) for k, (i, e) in slots.items()
                      if any(o == f"{name}:{k}" for o in only)}
 
-        def film_at(i, value, p):
+        def film_at(dirs, h, p):   # the film at theta + h * (the direction dirs)
             th = theta.copy()
-            th[i] = value
+            for j, c in dirs:
+                th[j] = np.float32(float(theta[j]) + h * c)
             ds.set_params(th)
             return ds.render(p).astype(np.float64)
 
         rows = {}
         adj_ms, t0 = 0.0, time.time()
         for key, (i, eps) in slots.items():
-            d = film_at(i, theta[i] + eps, pilot) - film_at(i, theta[i] - eps, pilot)
+            dirs = i if isinstance(i, list) else [(i, 1.0)]
+            d = film_at(dirs, eps, pilot) - film_at(dirs, -eps, pilot)
             wimg = np.sign(d).astype(np.float32)
             adj = np.zeros(nb)
             fd = np.zeros(nb)
             for b in range(nb):
                 rp.spp_offset = rw.spp_offset = b * fper
                 ds.set_params(theta)
-                adj[b] = ds.adjoint(rp, wimg, [i])[i]
+                g = ds.adjoint(rp, wimg, [j for j, _ in dirs])
+                adj[b] = sum(c * float(g[j]) for j, c in dirs)
                 adj_ms += ds.last_stats.kernel_ms
-                lp = float((film_at(i, theta[i] + eps, rw) * wimg).sum())
-                lm = float((film_at(i, theta[i] - eps, rw) * wimg).sum())
+                lp = float((film_at(dirs, eps, rw) * wimg).sum())
+                lm = float((film_at(dirs, -eps, rw) * wimg).sum())
                 fd[b] = (lp - lm) / (2.0 * eps)
                 if args.gc_richardson:   # (4 D(eps) - D(2 eps)) / 3 cancels the eps^2 term
-                    lp2 = float((film_at(i, theta[i] + 2 * eps, rw) * wimg).sum())
-                    lm2 = float((film_at(i, theta[i] - 2 * eps, rw) * wimg).sum())
+                    lp2 = float((film_at(dirs, 2 * eps, rw) * wimg).sum())
+                    lm2 = float((film_at(dirs, -2 * eps, rw) * wimg).sum())
                     fd[b] = (4.0 * fd[b] - (lp2 - lm2) / (4.0 * eps)) / 3.0
             ds.set_params(theta)
             diff = adj - fd
@@ -568,7 +582,7 @@ def fit(args):
     for it in range(steps):
         if it >= steps - 10:   # the loss the ground truth gets on the same samples
             ds.set_params(vec(truth_s, truth_e))
-            rp = abi.render_params(res, res, 32, 8, kernel=abi.KERNEL_MEGAKERNEL, spp_offset=it * 32)
+            rp = abi.render_params(res, res, 32, 8, kernel=adjoint_kernel(args), spp_offset=it * 32)
             hist_truth.append(float(((ds.render(rp).astype(np.float64) - target) ** 2).mean()))
         sv = x_s.detach().numpy().astype(np.float32)
         ev = np.exp(x_le.detach().numpy()).astype(np.float32)
@@ -578,7 +592,7 @@ def fit(args):
         ds.set_params(vec(sv, ev))
         # the forward film on the wavefront, the adjoint on the same samples
         rw = abi.render_params(res, res, 32, 8, kernel=abi.KERNEL_WAVEFRONT, spp_offset=it * 32)
-        rp = abi.render_params(res, res, 32, 8, kernel=abi.KERNEL_MEGAKERNEL, spp_offset=it * 32)
+        rp = abi.render_params(res, res, 32, 8, kernel=adjoint_kernel(args), spp_offset=it * 32)
         img = ds.render(rw)
         diff = img.astype(np.float64) - target
         loss = float((diff ** 2).mean())
@@ -627,6 +641,8 @@ def main():
     ap.add_argument("--ray-groups", type=int, default=1, choices=[1, 2, 3, 4],
                     help="--profile-frame: rays in slot order (1), regrouped by kind in each block (2), bounce rays sorted by origin and direction (3), bounce and shadow rays sorted (4)")
     ap.add_argument("--fit", action="store_true", help="the C4 inverse-rendering fit (Adam on rt_adjoint) and exit")
+    ap.add_argument("--adjoint-kernel", default="megakernel", choices=["megakernel", "wavefront"],
+                    help="--fit / --gradcheck: the rt_adjoint form")
     ap.add_argument("--res", type=int, default=256, help="--fit: square image size")
     ap.add_argument("--gradcheck", action="store_true",
                     help="adjoint gradients against central finite differences (C4, C5) and exit")
