@@ -398,6 +398,37 @@ def batched_side(rt):
     out["c5_views"] = {"views": len(reqs5), "samples": n, "seconds": st.kernel_ms / 1e3,
                        "msamples_per_s": n / st.kernel_ms / 1e3,
                        "finite": bool(all(np.isfinite(f).all() for f in films))}
+    out["adjoint"] = adjoint_side(rt)
+    return out
+
+
+def adjoint_side(rt):
+    """The path-replay adjoint (rt_adjoint) in both forms, device time of
+    both passes: C4 at the fit's call (256x256, 32 spp, depth 8, the sphere's
+    seven BSDF slots) and C5 at 64x64, 256 spp, depth 16 (the medium's six
+    slots), the second of two calls each."""
+    abi = rt.abi
+    out = {}
+    sphere = dict(base_color=(0.6, 0.3, 0.2), roughness=0.4, metallic=0.2, specular=0.6, sheen=0.3)
+    for name, world, res, spp, depth in (("c4_256x256_32spp_bsdf7", rt.scenes.cornell_sphere(sphere), 256, 32, 8),
+                                         ("c5_64x64_256spp_medium6", rt.scenes.cornell_volume(), 64, 256, 16)):
+        ds = rt.DiffScene(world)
+        if name.startswith("c4"):
+            slots = [ds.slot("fit_sphere", "base_color", c) for c in range(3)]
+            slots += [ds.slot("fit_sphere", n) for n in ("roughness", "metallic", "specular", "sheen")]
+        else:
+            slots = [ds.medium_slot(k, c) for k in ("sigma_a", "sigma_s") for c in range(3)]
+        wimg = np.random.default_rng(2).uniform(0, 1, (3, res, res)).astype(np.float32)
+        row = {}
+        for kname, kern in (("megakernel", abi.KERNEL_MEGAKERNEL), ("wavefront", abi.KERNEL_WAVEFRONT)):
+            rp = abi.render_params(res, res, spp, depth, kernel=kern)
+            for _ in range(2):
+                ds.adjoint(rp, wimg, slots)
+            row[kname] = res * res * spp / ds.last_stats.kernel_ms / 1e3
+        row["unit"] = "Msamples/s"
+        row["speedup_wavefront"] = row["wavefront"] / row["megakernel"]
+        out[name] = row
+        ds.close()
     return out
 
 
