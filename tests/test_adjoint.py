@@ -148,6 +148,24 @@ def test_wavefront_adjoint_equals_megakernel(scene):
     np.testing.assert_allclose(wave, mega, rtol=1e-3, atol=1e-5 * np.abs(mega).max())
 
 
+def test_wavefront_adjoint_runs_in_chunks_of_whole_spp_slices():
+    """A request larger than the wavefront adjoint's sample record (2^24
+    samples) is done in runs of whole spp slices; the gradient is the mean over
+    all samples, so it equals the mean of the two halves rendered as separate
+    calls."""
+    ds = rt.DiffScene(rt.scenes.cornell_sphere(SPHERE))
+    slots = [ds.slot("fit_sphere", "base_color", c) for c in range(3)] + [ds.slot("fit_sphere", "roughness")]
+    res, spp = 64, 8192   # 2^25 samples: two runs
+    wimg = _weights(res, res)
+
+    def grad(n, off):
+        return ds.adjoint(abi.render_params(res, res, n, 8, kernel=abi.KERNEL_WAVEFRONT, spp_offset=off), wimg,
+                          slots).astype(np.float64)
+    whole = grad(spp, 0)
+    halves = 0.5 * (grad(spp // 2, 0) + grad(spp // 2, spp // 2))
+    np.testing.assert_allclose(whole[slots], halves[slots], rtol=1e-4)
+
+
 def test_unmasked_slots_come_back_zero():
     ds = rt.DiffScene(rt.scenes.cornell_sphere(SPHERE))
     rp = _params(32, 32, 16)
