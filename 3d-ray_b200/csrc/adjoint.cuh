@@ -684,22 +684,30 @@ struct AdjointSink {
 
     // Russian roulette: a survivor was drawn against q = clamp(max_c thr_c,
     // min survival, 0.95), which moves with theta only strictly between the
-    // bounds, as the largest channel of the throughput (the mean over
-    // channels tied for the largest, the central derivative of the max). The
-    // survivor's throughput then carries 1/q. A path the roulette ends has no
-    // terms after the decision, so its score weight is 0.
+    // bounds, as the largest channel of the throughput. Channels tied for the
+    // largest (a grey medium keeps all three equal until a coloured surface)
+    // make the max a kink: its slope is the largest of their derivatives for
+    // a rising theta and the smallest for a falling one, and the central
+    // derivative, which central differences measure, is the mean of the two.
+    // The survivor's throughput then carries 1/q. A path the roulette ends
+    // has no terms after the decision, so its score weight is 0.
     RT_NI void roulette_score(PathView v, V3 pre, V3 att0, V3 thr, float q, int first_surface) {
         float m = fmaxf(thr.x, fmaxf(thr.y, thr.z));
         if (q != m) return;
         float thc[3] = {thr.x, thr.y, thr.z};
-        float dq[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-        int nt = 0;
-        for (int c = 0; c < 3; c++)
-            if (thc[c] == m) {
-                nt++;
-                for (int k = 0; k < 6; k++) dq[k] += dlb[c][k];
+        float lo[6], hi[6];
+        int tied = 0;
+        for (int c = 0; c < 3; c++) {
+            if (thc[c] != m) continue;
+            for (int k = 0; k < 6; k++) {
+                lo[k] = tied ? fminf(lo[k], dlb[c][k]) : dlb[c][k];
+                hi[k] = tied ? fmaxf(hi[k], dlb[c][k]) : dlb[c][k];
             }
-        for (int k = 0; k < 6; k++) dq[k] /= (float)nt;
+            tied++;
+        }
+        if (!tied) return;
+        float dq[6];
+        for (int k = 0; k < 6; k++) dq[k] = 0.5f * (lo[k] + hi[k]);
         float b = score_weight(v, pre, att0, first_surface != 0);
         if (b != 0.0f && isfinite(b))
             for (int k = 0; k < 6; k++) add(medium_base + k, b * dq[k]);
