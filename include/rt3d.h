@@ -434,7 +434,8 @@ int rt_autotune(RtScene* scene, const RtRenderParams* params, RtRenderParams* be
  * held fixed, with score terms for the two discrete events whose probability
  * the reference's estimator keeps (a lobe weight divided by max(p, floor), and
  * a null Sample followed by the legacy Scatter draw) and, for the samples the
- * luminance clamps saturate, for the medium's free-flight draws; geometry and visibility
+ * luminance clamps saturate, for the medium's free-flight draws and Russian
+ * roulette (with respect to the medium's slots); geometry and visibility
  * edges are not differentiated. Writes the gradient (float, host) in the
  * parameter-vector layout above; count is that layout's length. mask (count
  * bytes, or NULL for all) selects the slots to differentiate; unselected slots
