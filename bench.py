@@ -310,6 +310,28 @@ def profile_frame(args):
     lib.rt_scene_destroy(scene)
 
 
+def profile_adjoint(args):
+    """The C4 fit's adjoint call (256x256, 32 spp, depth 8, the sphere's
+    seven BSDF slots) twice, in the --adjoint-kernel form: the workload the
+    adjoint's ncu summaries under profiles/ were captured on."""
+    rt = load_package()
+    abi = rt.abi
+    sphere = dict(base_color=(0.6, 0.3, 0.2), roughness=0.4, metallic=0.2, specular=0.6, sheen=0.3)
+    ds = rt.DiffScene(rt.scenes.cornell_sphere(sphere))
+    slots = [ds.slot("fit_sphere", "base_color", c) for c in range(3)]
+    slots += [ds.slot("fit_sphere", n) for n in ("roughness", "metallic", "specular", "sheen")]
+    res, spp = 256, 32
+    wimg = np.random.default_rng(2).uniform(0, 1, (3, res, res)).astype(np.float32)
+    rp = abi.render_params(res, res, spp, 8, kernel=adjoint_kernel(args))
+    for i in range(2):
+        g = ds.adjoint(rp, wimg, slots)
+        st = ds.last_stats
+        print(json.dumps({"call": i, "adjoint_kernel": args.adjoint_kernel, "kernel_ms": st.kernel_ms,
+                          "Msamples_per_s": res * res * spp / st.kernel_ms / 1e3, "launches": st.kernel_launches,
+                          "finite": bool(np.isfinite(g).all())}), flush=True)
+    ds.close()
+
+
 def c1_side(rt, lib, abi):
     """C1: the Cornell box at 256x256, 64 spp, depth 8: the plain megakernel
     and the autotuned wavefront (device time, third of three renders), and the
@@ -701,11 +723,15 @@ def main():
                          "and exit (the command profiled by ncu for the device build)")
     ap.add_argument("--profile-frame", action="store_true",
                     help="render the frame twice with fixed settings and exit (the command profiled by ncu)")
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="the C4 fit's adjoint call twice (--adjoint-kernel form) and exit (the command profiled by ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.profile_frame:
         return profile_frame(args)
+    if args.profile_adjoint:
+        return profile_adjoint(args)
     if args.bvh_build:
         rt, world = build_world()
         lib = rt.abi.load()
