@@ -119,3 +119,56 @@ def test_gpu_image_at_the_oracle_noise_floor(name, kernel):
     assert np.all(np.abs(cz) < Z_MAX), (name, cz)
     worst = np.unravel_index(np.argmax(np.abs(tz)), tz.shape)
     assert np.abs(tz).max() < Z_MAX_TILE, (name, worst, tz[worst])
+
+
+# --- the bench's time-to-relMSE reference ------------------------------------------
+BENCH_GOLDEN = os.path.join(ROOT, "tests", "golden", "oracle_bench_cornell.npz")
+
+
+def _bench_golden():
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_bench_reference as m
+    return m, np.load(BENCH_GOLDEN)
+
+
+def test_bench_reference_fixture_is_consistent():
+    """CPU check of the 256x256 oracle render of bench.py's reference frame:
+    its metadata match the generator's, and its halves agree in the mean and
+    differ pixel by pixel."""
+    m, g = _bench_golden()
+    assert (int(g["width"]), int(g["height"]), int(g["depth"])) == (m.WIDTH, m.HEIGHT, m.DEPTH)
+    assert (int(g["gpu_offset"]), int(g["gpu_spp"]), int(g["half_spp"])) == (m.GPU_OFFSET, m.GPU_SPP, m.HALF_SPP)
+    a, b = g["a"].astype(np.float64), g["b"].astype(np.float64)
+    assert a.shape == (3, m.HEIGHT, m.WIDTH) and np.all(np.isfinite(a)) and np.all(np.isfinite(b))
+    assert np.mean(a != b) > 0.5
+    z = (a - b).sum(axis=(1, 2)) / np.sqrt(((a - b) ** 2).sum(axis=(1, 2)))
+    assert np.all(np.abs(z) < Z_MAX), z
+
+
+@pytest.mark.gpu
+def test_bench_relmse_reference_at_the_oracle_noise_floor():
+    """bench.py measures time to relMSE 1e-3 against a 65 536-sample wavefront
+    render of the Cornell box at 256x256 (Sobol indices [2^20, 2^20 + 65536)).
+    This renders that very image and holds it to the committed 4096-sample
+    oracle render of the same frame, as the 64x64 scenes above."""
+    m, gold = _bench_golden()
+    lib = abi.load()
+    pw = abi.PackedWorld(m.world())
+    h = C.c_void_p()
+    abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
+    try:
+        p = abi.render_params(m.WIDTH, m.HEIGHT, m.GPU_SPP, m.DEPTH, kernel=abi.KERNEL_WAVEFRONT,
+                              spp_offset=m.GPU_OFFSET)
+        img = np.zeros((3, m.HEIGHT, m.WIDTH), np.float32)
+        st = abi.RtStats()
+        abi.check(lib.rt_render(h, C.byref(p), abi.ptr(img), C.byref(st)), "rt_render")
+    finally:
+        lib.rt_scene_destroy(h)
+    assert st.samples == m.WIDTH * m.HEIGHT * m.GPU_SPP and np.all(np.isfinite(img))
+    rel, floor, tz, cz = parity_stats(gold["a"], gold["b"], img, m.GPU_SPP / (2 * m.HALF_SPP))
+    assert rel <= FLOOR_MARGIN * floor, (rel, floor)
+    assert np.all(np.abs(cz) < Z_MAX), cz
+    worst = np.unravel_index(np.argmax(np.abs(tz)), tz.shape)
+    assert np.abs(tz).max() < Z_MAX_TILE, (worst, tz[worst])
+
