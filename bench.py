@@ -239,9 +239,10 @@ def time_to_relmse_on(lib, abi, h, width, height, depth, window=None, target=1e-
     """Seconds of device time until a render reaches relMSE <= target against
     a 65 536-spp wavefront reference of the same frame (or window), rendered
     from a disjoint Sobol range so that it is uncorrelated with the test
-    images; spp doubles from 16. For the Cornell frame, tests/test_image_parity.py
-    renders this reference and holds it to a committed 4096-sample oracle
-    render of the frame at the oracle's noise floor."""
+    images; spp doubles from 16. For the two frames measured here (the Cornell
+    box and the icosphere window), tests/test_image_parity.py renders this
+    reference and holds it to a committed 4096-sample oracle render of the
+    frame at the oracle's noise floor."""
     import torch
     x0, y0, ww, wh = window or (0, 0, width, height)
     win = dict(pixel_x0=x0, pixel_y0=y0, window_w=ww, window_h=wh) if window else {}

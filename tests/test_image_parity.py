@@ -121,54 +121,71 @@ def test_gpu_image_at_the_oracle_noise_floor(name, kernel):
     assert np.abs(tz).max() < Z_MAX_TILE, (name, worst, tz[worst])
 
 
-# --- the bench's time-to-relMSE reference ------------------------------------------
-BENCH_GOLDEN = os.path.join(ROOT, "tests", "golden", "oracle_bench_cornell.npz")
+# --- the bench's time-to-relMSE references ------------------------------------------
+BENCH_FRAMES = ["cornell", "icospheres"]
 
 
-def _bench_golden():
+def _bench_golden(name):
     import sys
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     import make_bench_reference as m
-    return m, np.load(BENCH_GOLDEN)
+    return m, np.load(m.path(name))
 
 
-def test_bench_reference_fixture_is_consistent():
-    """CPU check of the 256x256 oracle render of bench.py's reference frame:
-    its metadata match the generator's, and its halves agree in the mean and
+@pytest.mark.parametrize("name", BENCH_FRAMES)
+def test_bench_reference_fixture_is_consistent(name):
+    """CPU check of the oracle renders of bench.py's reference frames: their
+    metadata match the generator's, and their halves agree in the mean and
     differ pixel by pixel."""
-    m, g = _bench_golden()
-    assert (int(g["width"]), int(g["height"]), int(g["depth"])) == (m.WIDTH, m.HEIGHT, m.DEPTH)
+    m, g = _bench_golden(name)
+    W, H, win, depth = m.FRAMES[name]
+    assert (int(g["width"]), int(g["height"]), int(g["depth"])) == (W, H, depth)
+    assert tuple(int(x) for x in g["window"]) == tuple(win)
     assert (int(g["gpu_offset"]), int(g["gpu_spp"]), int(g["half_spp"])) == (m.GPU_OFFSET, m.GPU_SPP, m.HALF_SPP)
     a, b = g["a"].astype(np.float64), g["b"].astype(np.float64)
-    assert a.shape == (3, m.HEIGHT, m.WIDTH) and np.all(np.isfinite(a)) and np.all(np.isfinite(b))
-    assert np.mean(a != b) > 0.5
+    assert a.shape == (3, win[3], win[2]) and np.all(np.isfinite(a)) and np.all(np.isfinite(b))
+    lit = (a + b) > 0   # the icosphere frame's black background is zero in both halves
+    assert lit.mean() > 0.3 and np.mean(a[lit] != b[lit]) > 0.5
     z = (a - b).sum(axis=(1, 2)) / np.sqrt(((a - b) ** 2).sum(axis=(1, 2)))
     assert np.all(np.abs(z) < Z_MAX), z
 
 
 @pytest.mark.gpu
-def test_bench_relmse_reference_at_the_oracle_noise_floor():
-    """bench.py measures time to relMSE 1e-3 against a 65 536-sample wavefront
-    render of the Cornell box at 256x256 (Sobol indices [2^20, 2^20 + 65536)).
-    This renders that very image and holds it to the committed 4096-sample
-    oracle render of the same frame, as the 64x64 scenes above."""
-    m, gold = _bench_golden()
+@pytest.mark.parametrize("name", BENCH_FRAMES)
+def test_bench_relmse_reference_at_the_oracle_noise_floor(name):
+    """bench.py measures time to relMSE 1e-3 against 65 536-sample wavefront
+    renders (Sobol indices [2^20, 2^20 + 65536)) of the Cornell box at 256x256
+    and of a 256x256 window of the icosphere-field frame. This renders those
+    very images and holds them to the committed 4096-sample oracle renders of
+    the same frames, as the 64x64 scenes above."""
+    m, gold = _bench_golden(name)
+    W, H, (x0, y0, ww, wh), depth = m.FRAMES[name]
     lib = abi.load()
-    pw = abi.PackedWorld(m.world())
+    pw = abi.PackedWorld(m.world(name))
     h = C.c_void_p()
     abi.check(lib.rt_scene_create(pw.ref(), C.byref(h)), "rt_scene_create")
     try:
-        p = abi.render_params(m.WIDTH, m.HEIGHT, m.GPU_SPP, m.DEPTH, kernel=abi.KERNEL_WAVEFRONT,
-                              spp_offset=m.GPU_OFFSET)
-        img = np.zeros((3, m.HEIGHT, m.WIDTH), np.float32)
+        p = m.window_params(abi, name, m.GPU_SPP, m.GPU_OFFSET, kernel=abi.KERNEL_WAVEFRONT)
+        film = np.zeros((3, H, W), np.float32)
         st = abi.RtStats()
-        abi.check(lib.rt_render(h, C.byref(p), abi.ptr(img), C.byref(st)), "rt_render")
+        abi.check(lib.rt_render(h, C.byref(p), abi.ptr(film), C.byref(st)), "rt_render")
     finally:
         lib.rt_scene_destroy(h)
-    assert st.samples == m.WIDTH * m.HEIGHT * m.GPU_SPP and np.all(np.isfinite(img))
+    img = film[:, y0:y0 + wh, x0:x0 + ww]
+    assert st.samples == ww * wh * m.GPU_SPP and np.all(np.isfinite(img))
     rel, floor, tz, cz = parity_stats(gold["a"], gold["b"], img, m.GPU_SPP / (2 * m.HALF_SPP))
     assert rel <= FLOOR_MARGIN * floor, (rel, floor)
     assert np.all(np.abs(cz) < Z_MAX), cz
-    worst = np.unravel_index(np.argmax(np.abs(tz)), tz.shape)
-    assert np.abs(tz).max() < Z_MAX_TILE, (worst, tz[worst])
-
+    # The tile test needs the halves' variance estimate: a tile where most
+    # pixels come out identical in both halves (the icosphere frame's black
+    # background, with a lit pixel at a silhouette) hides events rarer than
+    # 1 in 2048 samples that the GPU's 65 536 catch, so its estimate is ~0.
+    # Such tiles carry no image (relMSE and the channel means cover them) and
+    # are left out; the rest must hold.
+    a, b = gold["a"], gold["b"]
+    c, hh, wd = a.shape
+    varies = (a != b).reshape(c, hh // 8, 8, wd // 8, 8).mean(axis=(2, 4)) >= 0.5
+    assert varies.mean() > 0.4, varies.mean()
+    tzv = np.where(varies, tz, 0.0)
+    worst = np.unravel_index(np.argmax(np.abs(tzv)), tzv.shape)
+    assert np.abs(tzv).max() < Z_MAX_TILE, (worst, tzv[worst])
