@@ -45,6 +45,20 @@ class DiffScene:
         base = self.num_materials * abi.ADJ_PER_MATERIAL
         return base + (abi.ADJ_MEDIUM_SIGMA_A if name == "sigma_a" else abi.ADJ_MEDIUM_SIGMA_S) + channel
 
+    def medium_albedo_direction(self, theta, channel: int = 0) -> dict:
+        """The medium's single-scattering albedo a = sigma_s / sigma_t of one
+        channel as a direction in the parameter vector at a fixed sigma_t:
+        d sigma_s / da = sigma_t, d sigma_a / da = -sigma_t. Returns {slot:
+        coefficient}; dLoss/da is the sum of coefficient * dLoss/dslot."""
+        ia, isc = self.medium_slot("sigma_a", channel), self.medium_slot("sigma_s", channel)
+        st = float(theta[ia]) + float(theta[isc])
+        return {isc: st, ia: -st}
+
+    def medium_albedo_gradient(self, theta, grad, channel: int = 0) -> float:
+        """dLoss/d(albedo) of one channel at a fixed sigma_t, from the gradient
+        rt_adjoint returns for the sigma_a and sigma_s slots."""
+        return float(sum(c * float(grad[i]) for i, c in self.medium_albedo_direction(theta, channel).items()))
+
     def get_params(self) -> np.ndarray:
         out = np.zeros(self.count, np.float32)
         abi.check(self.lib.rt_scene_get_params(self.handle, abi.ptr(out), self.count), "rt_scene_get_params")

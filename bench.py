@@ -531,9 +531,9 @@ def gradcheck(args):
                 slots[f"glass.absorption[{c}]"] = (i, 1e-2 * float(theta[i]))
                 # the single-scattering albedo at a fixed sigma_t: sigma_s = albedo * sigma_t,
                 # sigma_a = (1 - albedo) * sigma_t, a direction in the parameter vector
-                ia, isc = ds.medium_slot("sigma_a", c), ds.medium_slot("sigma_s", c)
-                st = float(theta[ia]) + float(theta[isc])
-                slots[f"medium.albedo[{c}]"] = ([(isc, st), (ia, -st)], 1e-2 * float(theta[isc]) / st)
+                dirs = ds.medium_albedo_direction(theta, c)
+                isc = ds.medium_slot("sigma_s", c)
+                slots[f"medium.albedo[{c}]"] = (list(dirs.items()), 1e-2 * float(theta[isc]) / dirs[isc])
         else:
             slots = {f"glass.absorption[{c}]": (ds.slot("glass", "absorption", c),
                                                 1e-2 * float(theta[ds.slot("glass", "absorption", c)]))

@@ -166,6 +166,36 @@ def test_wavefront_adjoint_runs_in_chunks_of_whole_spp_slices():
     np.testing.assert_allclose(whole[slots], halves[slots], rtol=1e-4)
 
 
+def test_medium_albedo_gradient_is_exact_without_roulette():
+    """The medium's albedo at a fixed sigma_t (DiffScene.medium_albedo_direction)
+    moves no free-flight density, so without Russian roulette every sample's
+    value is smooth in it and Richardson central differences on the same
+    samples match the adjoint to float rounding."""
+    ds = rt.DiffScene(rt.scenes.cornell_volume())
+    res = 32
+    kw = dict(rr_min_bounces=1000, **NO_CLAMP)
+    rp = _params(res, res, 256, 16, **kw)
+    rw = abi.render_params(res, res, 256, 16, kernel=abi.KERNEL_WAVEFRONT, **kw)
+    wimg = _weights(res, res)
+    theta = ds.get_params()
+    for c in range(3):
+        dirs = ds.medium_albedo_direction(theta, c)
+        adj = ds.medium_albedo_gradient(theta, ds.adjoint(rp, wimg, list(dirs)), c)
+        eps = 1e-2 * float(theta[ds.medium_slot("sigma_s", c)]) / dirs[ds.medium_slot("sigma_s", c)]
+
+        def loss(h):
+            th = theta.copy()
+            for i, k in dirs.items():
+                th[i] = np.float32(float(theta[i]) + h * k)
+            ds.set_params(th)
+            return float((ds.render(rw).astype(np.float64) * wimg).sum())
+        d1 = (loss(eps) - loss(-eps)) / (2 * eps)
+        d2 = (loss(2 * eps) - loss(-2 * eps)) / (4 * eps)
+        ds.set_params(theta)
+        fd = (4 * d1 - d2) / 3
+        assert adj == pytest.approx(fd, rel=2e-3), (c, adj, fd)
+
+
 def test_unmasked_slots_come_back_zero():
     ds = rt.DiffScene(rt.scenes.cornell_sphere(SPHERE))
     rp = _params(32, 32, 16)
