@@ -465,6 +465,7 @@ struct AdjointSink {
     double* gacc;          // global accumulators
     int medium_base;       // first global slot (medium sigma_a, sigma_s)
     int opaque;
+    int any4;              // opaque shadow rays walk the four-wide records in any order (stack bound fits)
     int* err;
     V3 tot_a, tot_la;      // primal A = lp + pre * clamp(att0 * S(la)) and la
     V3 g_a, g_la, g_att0;  // their adjoints
@@ -524,7 +525,8 @@ struct AdjointSink {
         sh_n = 0;
         Hit h;
         if (opaque) {
-            traverse<true, STACK>(*s, o, d, tmin, tmax, h, nullptr, err);
+            if (any4) traverse4_any<STACK>(*s, o, d, tmin, tmax, h, err);
+            else traverse<true, STACK>(*s, o, d, tmin, tmax, h, nullptr, err);
             return h.kind == HIT_NONE ? v3(1.0f) : v3(0.0f);
         }
         V3 thr = v3(1.0f);

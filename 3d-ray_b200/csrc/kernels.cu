@@ -319,6 +319,7 @@ struct AdjArgs {
     int medium_base;
     int use_shared;
     int use_local;
+    int any4;              // opaque shadow rays may walk the four-wide records
 };
 
 // Build knobs of the adjoint kernel: a register cap (0: the compiler's
@@ -390,6 +391,7 @@ __global__ void RT_ADJ_BOUNDS k_adjoint(rt::SceneView s, rt::RenderConst rc, Adj
         adj.gacc = a.grad;
         adj.medium_base = a.medium_base;
         adj.opaque = rc.opaque;
+        adj.any4 = a.any4;
         adj.err = err;
         adj.abs_mat = -1;
         adj.max_rad = rc.max_rad;
@@ -946,6 +948,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         l4_occ = true;
         for (const HostReq& q : reqs) l4_occ = l4_occ && q.scene->host.max_stack4 <= kStack;
     }
+    a.any4 = l4_occ && opaque;
     int groups = cfg.groups > 0 ? cfg.groups : default_groups(scenes);
     // shade is compiled with the volumetric branch and the transmission lobe
     // only when a scene of the batch needs them
@@ -2135,6 +2138,7 @@ int rt_adjoint(RtScene* sc, const RtRenderParams* p, const float* dimg, const ui
     a.use_shared = shmem <= 48 * 1024;
     if (!a.use_shared) shmem = 0;
     a.use_local = RT_ADJ_LOCAL_ACC && np <= rt::kAdjLocal;
+    a.any4 = rcon.opaque && sc->host.max_stack4 <= kStack;
     long long total = (long long)ww * wh * p->spp;
     long long blocks = std::min<long long>((total + kBlock - 1) / kBlock, 148LL * 16);
     double wf_ms = 0.0;

@@ -149,6 +149,7 @@ struct WfArgs {
     WfShadow S;
     WfCtl* ctl;
     int* err;
+    int any4;         // opaque shadow rays may walk the four-wide records (their stack bound fits)
     WfAdjoint J;
 };
 

@@ -56,6 +56,7 @@ __global__ void __launch_bounds__(128) k_wf_adjoint(WfArgs a) {
         adj.gacc = J.grad;
         adj.medium_base = J.medium_base;
         adj.opaque = R.rc.opaque;
+        adj.any4 = a.any4;
         adj.err = a.err;
         adj.sh_added = 0;
         adj.sh_n = 0;
