@@ -1011,10 +1011,11 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
             else if (medium) rt::k_wf_adjoint<kStack, true, false><<<gadj, adj_blk, adj_shmem, stream>>>(a);
             else if (transmit) rt::k_wf_adjoint<kStack, false, true><<<gadj, adj_blk, adj_shmem, stream>>>(a);
             else rt::k_wf_adjoint<kStack, false, false><<<gadj, adj_blk, adj_shmem, stream>>>(a);
+            if (ev) cudaEventRecord(ev[4], stream);
             if (a.raysort) rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.rhist, a.roff, &d_ctl->nbounce);
             if (ev) {
-                cudaEventRecord(ev[4], stream);
                 cudaEventRecord(ev[5], stream);
+                cudaEventRecord(ev[6], stream);
             }
             return;
         }
@@ -1022,24 +1023,26 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         else if (medium) rt::k_wf_shade<true, false><<<gs, blk, 0, stream>>>(a);
         else if (transmit) rt::k_wf_shade<false, true><<<gs, blk, 0, stream>>>(a);
         else rt::k_wf_shade<false, false><<<gs, blk, 0, stream>>>(a);
+        if (ev) cudaEventRecord(ev[4], stream);   // the ray sorts' scans and scatter count as sorting
         if (a.raysort) rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.rhist, a.roff, &d_ctl->nbounce);
         if (a.shadowsort) {
             rt::k_wf_rscan<<<1, 1024, 0, stream>>>(a.shist, a.soff, &d_ctl->nshadow);
             rt::k_wf_sscatter<<<gsh256, 256, 0, stream>>>(a);
         }
-        if (ev) cudaEventRecord(ev[4], stream);
+        if (ev) cudaEventRecord(ev[5], stream);
         if (l4_occ && a.opaque) rt::k_wf_occlude<kStack, true, true><<<gsh, tblk, 0, stream>>>(a);
         else if (l4) rt::k_wf_occlude<kStack, true, false><<<gsh, tblk, 0, stream>>>(a);
         else if (pt && a.opaque) rt::k_wf_occlude_pt<kStack><<<gpt_o, tblk, 0, stream>>>(a);
         else if (a.opaque) rt::k_wf_occlude<kStack, false, true><<<gsh, tblk, 0, stream>>>(a);
         else rt::k_wf_occlude<kStack, false, false><<<gsh, tblk, 0, stream>>>(a);
-        if (ev) cudaEventRecord(ev[5], stream);
+        if (ev) cudaEventRecord(ev[6], stream);
     };
+    constexpr int kEv = 7;   // profiling events per iteration
     const int batch = 4;
     cudaGraphExec_t exec = nullptr;
     std::vector<cudaEvent_t> pev;
     if (cfg.profile) {
-        pev.resize(batch * 6);
+        pev.resize(batch * kEv);
         for (auto& e : pev)
             if (cudaEventCreate(&e) != cudaSuccess) return fail(RT_ERR_CUDA, "event creation failed");
     } else {
@@ -1089,7 +1092,7 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
     for (;;) {
         for (int k = 0; k < batch; k++) {
             if (cfg.profile) {
-                launch_iter(&pev[k * 6]);
+                launch_iter(&pev[k * kEv]);
             } else if (cudaGraphLaunch(exec, stream) != cudaSuccess) {
                 rc = fail(RT_ERR_CUDA, "graph launch failed");
                 break;
@@ -1114,13 +1117,14 @@ int wf_render(const std::vector<HostReq>& reqs, const WfConfig& cfg, RtStats* st
         }
         if (cfg.profile) {
             for (int k = 0; k < batch; k++) {
-                float m[5];
-                for (int e = 0; e < 5; e++) cudaEventElapsedTime(&m[e], pev[k * 6 + e], pev[k * 6 + e + 1]);
+                float m[kEv - 1];
+                for (int e = 0; e < kEv - 1; e++)
+                    cudaEventElapsedTime(&m[e], pev[k * kEv + e], pev[k * kEv + e + 1]);
                 t_regen += m[0];
                 t_extend += m[1];
-                t_sort += m[2];
+                t_sort += m[2] + m[4];   // the material sort, then the ray sorts' scans and scatter
                 t_shade += m[3];
-                t_occlude += m[4];
+                t_occlude += m[5];
             }
         }
         unsigned long long next = ws.pinned[2 * check];

@@ -241,7 +241,8 @@ typedef struct RtStats {
     uint64_t shadow_node_visits;    /* the same three for shadow rays (count_work only) */
     uint64_t shadow_prim_tests;
     uint64_t shadow_other_tests;
-    double   regen_ms, extend_ms, shade_ms, occlude_ms, sort_ms;   /* profile_kernels only */
+    double   regen_ms, extend_ms, shade_ms, occlude_ms, sort_ms;   /* profile_kernels only; sort_ms holds
+                                       the material sort and the ray sorts' scans and scatter */
     int32_t  iterations;            /* wavefront iterations */
     int32_t  kernel_launches;       /* kernels launched by the call */
     int32_t  rr_min_bounces;        /* the RR knobs the call used */

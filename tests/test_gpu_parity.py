@@ -504,3 +504,22 @@ def test_autotune_picks_a_valid_configuration_that_renders_the_same_image(cornel
         assert st.samples == 48 * 48 * 64
     finally:
         s.close()
+
+
+def test_profiled_render_equals_the_graph_render(throughput_world_small):
+    """profile_kernels runs the same iteration kernel by kernel with events
+    around each group instead of the graph: the same image, and a split that
+    adds up to the call's device time."""
+    s = Scene(throughput_world_small)
+    try:
+        p = abi.render_params(96, 54, 64, 12, kernel=abi.KERNEL_WAVEFRONT, wavefront_size=1 << 15)
+        g, _ = s.render(p)
+        p.profile_kernels = 1
+        f, st = s.render(p)
+        np.testing.assert_allclose(f, g, rtol=1e-6, atol=1e-7)
+        parts = [st.regen_ms, st.extend_ms, st.shade_ms, st.occlude_ms, st.sort_ms]
+        assert all(x > 0.0 for x in parts), parts
+        assert sum(parts) <= st.kernel_ms * 1.01 + 0.05 and sum(parts) >= 0.5 * st.kernel_ms, (parts, st.kernel_ms)
+    finally:
+        s.close()
+
